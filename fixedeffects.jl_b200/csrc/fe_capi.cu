@@ -1,0 +1,432 @@
+// fe_capi.cu -- extern "C" entry points of include/fe_b200.h.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/fe_b200.h"
+#include "fe_plan.h"
+#include "fe_solve.h"
+
+using fe::set_error;
+
+namespace {
+
+int check_plan(fe_plan* p) {
+  if (!p) {
+    set_error("plan is NULL");
+    return FE_ERR_INVALID;
+  }
+  return FE_OK;
+}
+
+int create_common(fe_plan** out, int32_t nprob, const int64_t* n_obs, int32_t K,
+                  const int64_t* const* refs, const int64_t* n_levels,
+                  const double* const* interaction, const double* weights, int32_t device) {
+  if (!out) {
+    set_error("out is NULL");
+    return FE_ERR_INVALID;
+  }
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    (void)cudaGetLastError();
+    set_error("no CUDA device available");
+    return FE_ERR_CUDA;
+  }
+  if (device < 0 || device >= ndev) {
+    set_error("device ordinal out of range");
+    return FE_ERR_INVALID;
+  }
+  fe_plan* pl = new (std::nothrow) fe_plan();
+  if (!pl) {
+    set_error("host allocation failed");
+    return FE_ERR_ALLOC;
+  }
+  int st = fe::plan_build(pl, nprob, n_obs, K, refs, n_levels, interaction, weights, device);
+  if (st) {
+    fe::plan_destroy(pl);
+    return st;
+  }
+  *out = pl;
+  return FE_OK;
+}
+
+int solve_common(fe_plan* plan, void* Y, bool host, int32_t dtype, int64_t ncols, int64_t ld,
+                 int32_t precision, double tol, int64_t maxiter, int64_t* iterations,
+                 uint8_t* converged) {
+  int st = check_plan(plan);
+  if (st) return st;
+  if (dtype != FE_DTYPE_F64 && dtype != FE_DTYPE_F32) {
+    set_error("dtype must be FE_DTYPE_F64 or FE_DTYPE_F32");
+    return FE_ERR_INVALID;
+  }
+  if (precision < 0 || precision > 2) {
+    set_error("precision must be FE_PREC_FP64, FE_PREC_MIXED or FE_PREC_FP32");
+    return FE_ERR_INVALID;
+  }
+  if (ncols < 0 || (ncols > 0 && !Y && plan->N > 0)) {
+    set_error("Y is NULL or ncols < 0");
+    return FE_ERR_INVALID;
+  }
+  if (ld < plan->N) {
+    set_error("ld must be >= the number of observations");
+    return FE_ERR_INVALID;
+  }
+  if (!(tol >= 0.0) || maxiter < 1) {
+    set_error("tol must be >= 0 and maxiter >= 1");
+    return FE_ERR_INVALID;
+  }
+  if (ncols == 0) return FE_OK;
+  const size_t es = dtype == FE_DTYPE_F64 ? 8 : 4;
+  fe::SolveReq rq;
+  rq.dtype = dtype;
+  rq.ncols = ncols;
+  rq.precision = precision;
+  rq.tol = tol;
+  rq.maxiter = maxiter;
+  rq.residuals = true;
+  rq.iters = iterations;
+  rq.converged = converged;
+  plan->last_prob_iters.assign((size_t)plan->nprob * ncols, 0);
+  plan->last_prob_conv.assign((size_t)plan->nprob * ncols, 0);
+  rq.prob_iters = plan->last_prob_iters.data();
+  rq.prob_converged = plan->last_prob_conv.data();
+  if (cudaSetDevice(plan->device) != cudaSuccess) {
+    set_error("cudaSetDevice failed");
+    return FE_ERR_CUDA;
+  }
+  const int64_t N = plan->N;
+  if (host && N > 0) {
+    // stage through device memory: one 2D copy in, one out
+    st = plan->ws.ystage.ensure((size_t)N * ncols * es);
+    if (st) return st;
+    cudaError_t e = cudaMemcpy2DAsync(plan->ws.ystage.p, (size_t)N * es, Y, (size_t)ld * es,
+                                      (size_t)N * es, (size_t)ncols, cudaMemcpyHostToDevice,
+                                      plan->stream);
+    if (e != cudaSuccess) {
+      set_error(std::string("host to device copy failed: ") + cudaGetErrorString(e));
+      return FE_ERR_CUDA;
+    }
+    rq.Y = plan->ws.ystage.p;
+    rq.ld = N;
+  } else {
+    rq.Y = Y;
+    rq.ld = ld;
+  }
+  st = fe::solve(plan, rq);
+  if (st) return st;
+  if (host && N > 0) {
+    cudaError_t e = cudaMemcpy2DAsync(Y, (size_t)ld * es, plan->ws.ystage.p, (size_t)N * es,
+                                      (size_t)N * es, (size_t)ncols, cudaMemcpyDeviceToHost,
+                                      plan->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(plan->stream);
+    if (e != cudaSuccess) {
+      set_error(std::string("device to host copy failed: ") + cudaGetErrorString(e));
+      return FE_ERR_CUDA;
+    }
+  } else {
+    cudaError_t e = cudaStreamSynchronize(plan->stream);
+    if (e != cudaSuccess) {
+      set_error(std::string("stream synchronize failed: ") + cudaGetErrorString(e));
+      return FE_ERR_CUDA;
+    }
+  }
+  return FE_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int fe_version(void) { return FE_B200_VERSION; }
+
+const char* fe_last_error(void) { return fe::last_error(); }
+
+int fe_plan_create(fe_plan** out, int64_t n_obs, int32_t n_fe, const int64_t* const* refs,
+                   const int64_t* n_levels, const double* const* interaction,
+                   const double* weights, int32_t device) {
+  if (n_obs < 0) {
+    set_error("n_obs must be >= 0");
+    return FE_ERR_INVALID;
+  }
+  return create_common(out, 1, &n_obs, n_fe, refs, n_levels, interaction, weights, device);
+}
+
+int fe_plan_create_batch(fe_plan** out, int32_t n_problems, const int64_t* n_obs, int32_t n_fe,
+                         const int64_t* const* refs, const int64_t* n_levels,
+                         const double* const* interaction, const double* weights,
+                         int32_t device) {
+  return create_common(out, n_problems, n_obs, n_fe, refs, n_levels, interaction, weights, device);
+}
+
+int fe_plan_update_weights(fe_plan* plan, const double* weights) {
+  int st = check_plan(plan);
+  if (st) return st;
+  return fe::plan_update_weights(plan, weights);
+}
+
+int fe_plan_set_stream(fe_plan* plan, void* stream) {
+  int st = check_plan(plan);
+  if (st) return st;
+  if (cudaStreamSynchronize(plan->stream) != cudaSuccess) {
+    set_error("stream synchronize failed");
+    return FE_ERR_CUDA;
+  }
+  if (stream) {
+    if (plan->own_stream) cudaStreamDestroy(plan->stream);
+    plan->own_stream = false;
+    plan->stream = static_cast<cudaStream_t>(stream);
+  } else if (!plan->own_stream) {
+    cudaSetDevice(plan->device);
+    if (cudaStreamCreateWithFlags(&plan->stream, cudaStreamNonBlocking) != cudaSuccess) {
+      set_error("stream creation failed");
+      return FE_ERR_CUDA;
+    }
+    plan->own_stream = true;
+  }
+  return FE_OK;
+}
+
+int fe_plan_set_option(fe_plan* plan, int32_t option, double value) {
+  int st = check_plan(plan);
+  if (st) return st;
+  switch (option) {
+    case FE_OPT_TILE: {
+      const int v = (int)value;
+      if (v != 0 && v != 1 && v != 2 && v != 4 && v != 8 && v != 16 && v != 32) {
+        set_error("tile must be 0 or a power of two <= 32");
+        return FE_ERR_INVALID;
+      }
+      plan->opt_tile = v;
+      return FE_OK;
+    }
+    case FE_OPT_CHECK_EVERY:
+      if (value < 1) {
+        set_error("check interval must be >= 1");
+        return FE_ERR_INVALID;
+      }
+      plan->opt_check_every = (int)value;
+      return FE_OK;
+    case FE_OPT_MAX_ROUNDS:
+      if (value < 1) {
+        set_error("max rounds must be >= 1");
+        return FE_ERR_INVALID;
+      }
+      plan->opt_max_rounds = (int)value;
+      return FE_OK;
+    case FE_OPT_PROFILE:
+      plan->prof.on = value != 0;
+      return FE_OK;
+    case FE_OPT_INNER_RHO:
+      if (!(value > 0 && value < 1)) {
+        set_error("inner rho must be in (0, 1)");
+        return FE_ERR_INVALID;
+      }
+      plan->opt_inner_rho = value;
+      return FE_OK;
+    default:
+      set_error("unknown option");
+      return FE_ERR_INVALID;
+  }
+}
+
+int fe_plan_destroy(fe_plan* plan) {
+  if (!plan) return FE_OK;
+  return fe::plan_destroy(plan);
+}
+
+int fe_solve_residuals(fe_plan* plan, void* Y, int32_t dtype, int64_t ncols, int64_t ld,
+                       int32_t precision, double tol, int64_t maxiter, int64_t* iterations,
+                       uint8_t* converged) {
+  return solve_common(plan, Y, true, dtype, ncols, ld, precision, tol, maxiter, iterations,
+                      converged);
+}
+
+int fe_solve_residuals_device(fe_plan* plan, void* Y_dev, int32_t dtype, int64_t ncols,
+                              int64_t ld, int32_t precision, double tol, int64_t maxiter,
+                              int64_t* iterations, uint8_t* converged) {
+  return solve_common(plan, Y_dev, false, dtype, ncols, ld, precision, tol, maxiter, iterations,
+                      converged);
+}
+
+int fe_solve_coefficients(fe_plan* plan, const void* y, int32_t dtype, int32_t precision,
+                          double tol, int64_t maxiter, double* const* coefs,
+                          int64_t* iterations, uint8_t* converged) {
+  int st = check_plan(plan);
+  if (st) return st;
+  if (dtype != FE_DTYPE_F64 && dtype != FE_DTYPE_F32) {
+    set_error("dtype must be FE_DTYPE_F64 or FE_DTYPE_F32");
+    return FE_ERR_INVALID;
+  }
+  if (precision < 0 || precision > 2) {
+    set_error("precision must be FE_PREC_FP64, FE_PREC_MIXED or FE_PREC_FP32");
+    return FE_ERR_INVALID;
+  }
+  if ((!y && plan->N > 0) || !coefs) {
+    set_error("y and coefs are required");
+    return FE_ERR_INVALID;
+  }
+  for (int k = 0; k < plan->K; ++k)
+    if (!coefs[k] && plan->nlev[k] > 0) {
+      set_error("coefs[k] is NULL");
+      return FE_ERR_INVALID;
+    }
+  if (!(tol >= 0.0) || maxiter < 1) {
+    set_error("tol must be >= 0 and maxiter >= 1");
+    return FE_ERR_INVALID;
+  }
+  if (cudaSetDevice(plan->device) != cudaSuccess) {
+    set_error("cudaSetDevice failed");
+    return FE_ERR_CUDA;
+  }
+  const int64_t N = plan->N;
+  const size_t es = dtype == FE_DTYPE_F64 ? 8 : 4;
+  fe::SolveReq rq;
+  rq.dtype = dtype;
+  rq.ncols = 1;
+  rq.ld = N;
+  rq.precision = precision;
+  rq.tol = tol;
+  rq.maxiter = maxiter;
+  rq.residuals = false;
+  rq.iters = iterations;
+  rq.converged = converged;
+  rq.coefs = coefs;
+  plan->last_prob_iters.assign((size_t)plan->nprob, 0);
+  plan->last_prob_conv.assign((size_t)plan->nprob, 0);
+  rq.prob_iters = plan->last_prob_iters.data();
+  rq.prob_converged = plan->last_prob_conv.data();
+  if (N > 0) {
+    st = plan->ws.ystage.ensure((size_t)N * es);
+    if (st) return st;
+    cudaError_t e = cudaMemcpyAsync(plan->ws.ystage.p, y, (size_t)N * es, cudaMemcpyHostToDevice,
+                                    plan->stream);
+    if (e != cudaSuccess) {
+      set_error(std::string("host to device copy failed: ") + cudaGetErrorString(e));
+      return FE_ERR_CUDA;
+    }
+    rq.Y = plan->ws.ystage.p;
+  }
+  // solve_coefficients! always runs LSMR, even with one fixed effect
+  const int save_tile = plan->opt_tile;
+  plan->opt_tile = 1;
+  st = fe::solve(plan, rq);
+  plan->opt_tile = save_tile;
+  return st;
+}
+
+int fe_plan_problem_results(fe_plan* plan, int64_t* iterations, uint8_t* converged) {
+  int st = check_plan(plan);
+  if (st) return st;
+  if (iterations)
+    std::copy(plan->last_prob_iters.begin(), plan->last_prob_iters.end(), iterations);
+  if (converged) std::copy(plan->last_prob_conv.begin(), plan->last_prob_conv.end(), converged);
+  return FE_OK;
+}
+
+int fe_plan_last_solve_info(fe_plan* plan, int64_t ncols, double* test2, int32_t* rounds,
+                            int64_t* lsmr_iters) {
+  int st = check_plan(plan);
+  if (st) return st;
+  const int64_t n = std::min<int64_t>(ncols, (int64_t)plan->last_test2.size());
+  for (int64_t j = 0; j < n; ++j) {
+    if (test2) test2[j] = plan->last_test2[(size_t)j];
+    if (rounds) rounds[j] = plan->last_rounds[(size_t)j];
+    if (lsmr_iters) lsmr_iters[j] = plan->last_iters_raw[(size_t)j];
+  }
+  return FE_OK;
+}
+
+int fe_plan_get_integer_plan(fe_plan* plan, int32_t* perm0, int64_t* const* offsets,
+                             int32_t* const* segperm) {
+  int st = check_plan(plan);
+  if (st) return st;
+  if (plan->nprob != 1) {
+    set_error("integer plan export is defined for single-problem plans");
+    return FE_ERR_INVALID;
+  }
+  cudaSetDevice(plan->device);
+  const int64_t N = plan->N;
+  if (perm0 && N > 0) {
+    if (cudaMemcpy(perm0, plan->d_obs_src.p, (size_t)N * 4, cudaMemcpyDeviceToHost) != cudaSuccess) {
+      set_error("copy of the integer plan failed");
+      return FE_ERR_CUDA;
+    }
+  }
+  for (int k = 0; k < plan->K; ++k) {
+    if (offsets && offsets[k])
+      std::copy(plan->seg_off[k].begin(), plan->seg_off[k].begin() + plan->nlev[k] + 1, offsets[k]);
+    if (segperm && segperm[k] && plan->seg_len[k] > 0) {
+      if (plan->perm_identity[k]) {
+        for (int64_t q = 0; q < plan->seg_len[k]; ++q) segperm[k][q] = (int32_t)q;
+      } else if (cudaMemcpy(segperm[k], plan->d_perm[k].p, (size_t)plan->seg_len[k] * 4,
+                            cudaMemcpyDeviceToHost) != cudaSuccess) {
+        set_error("copy of the integer plan failed");
+        return FE_ERR_CUDA;
+      }
+    }
+  }
+  return FE_OK;
+}
+
+int fe_plan_get_scales(fe_plan* plan, double* const* scales) {
+  int st = check_plan(plan);
+  if (st) return st;
+  if (!scales) {
+    set_error("scales is NULL");
+    return FE_ERR_INVALID;
+  }
+  cudaSetDevice(plan->device);
+  cudaStreamSynchronize(plan->stream);
+  for (int k = 0; k < plan->K; ++k)
+    if (scales[k] && plan->nlev[k] > 0 &&
+        cudaMemcpy(scales[k], plan->d_scale_d[k].p, (size_t)plan->nlev[k] * 8,
+                   cudaMemcpyDeviceToHost) != cudaSuccess) {
+      set_error("copy of the scales failed");
+      return FE_ERR_CUDA;
+    }
+  return FE_OK;
+}
+
+int fe_plan_primary(fe_plan* plan, int32_t* primary) {
+  int st = check_plan(plan);
+  if (st) return st;
+  if (primary) *primary = plan->primary;
+  return FE_OK;
+}
+
+int fe_plan_kernel_stat(fe_plan* plan, int32_t index, char* name, int64_t name_len,
+                        int64_t* launches, double* total_ms, double* alg_bytes) {
+  int st = check_plan(plan);
+  if (st) return st;
+  fe::prof_flush(plan);
+  if (index < 0 || index >= (int32_t)plan->prof.stats.size()) {
+    set_error("kernel stat index out of range");
+    return FE_ERR_INVALID;
+  }
+  auto it = plan->prof.stats.begin();
+  std::advance(it, index);
+  const fe::KernelStat& s = it->second;
+  if (name && name_len > 0) {
+    std::strncpy(name, s.name.c_str(), (size_t)name_len - 1);
+    name[name_len - 1] = '\0';
+  }
+  if (launches) *launches = s.launches;
+  if (total_ms) *total_ms = s.ms;
+  if (alg_bytes) *alg_bytes = s.bytes;
+  return FE_OK;
+}
+
+int fe_plan_reset_stats(fe_plan* plan) {
+  int st = check_plan(plan);
+  if (st) return st;
+  fe::prof_flush(plan);
+  plan->prof.stats.clear();
+  return FE_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,524 @@
+// fe_plan.cu -- plan construction: validation, the integer plan (stable
+// counting sorts), work items, and the Jacobi preconditioner on the device.
+//
+// Replaces the solver constructor and update_weights! of the reference's CUDA
+// backend (ext/CUDAExt.jl:99-121) and of the CPU backend
+// (src/SolverCPU.jl:55-95).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "fe_kernels.cuh"
+#include "fe_plan.h"
+
+namespace fe {
+
+namespace {
+thread_local std::string g_err;
+}
+void set_error(const std::string& msg) { g_err = msg; }
+const char* last_error() { return g_err.c_str(); }
+
+DevBuf::~DevBuf() {
+  if (p) cudaFree(p);
+}
+int DevBuf::ensure(size_t n) {
+  if (n <= bytes && p) return 0;
+  if (p) {
+    cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+  }
+  if (n == 0) n = 16;
+  cudaError_t e = cudaMalloc(&p, n);
+  if (e != cudaSuccess) {
+    p = nullptr;
+    set_error(std::string("cudaMalloc of ") + std::to_string(n) + " bytes failed: " +
+              cudaGetErrorString(e));
+    (void)cudaGetLastError();
+    return 3;  // FE_ERR_ALLOC
+  }
+  bytes = n;
+  return 0;
+}
+
+template <typename T>
+static int upload(DevBuf& b, const T* src, size_t n, cudaStream_t s) {
+  int st = b.ensure(n * sizeof(T));
+  if (st) return st;
+  if (n) FE_CK(cudaMemcpyAsync(b.p, src, n * sizeof(T), cudaMemcpyHostToDevice, s));
+  return 0;
+}
+
+// ---------------------------------------------------------------------------
+// setup kernels
+// ---------------------------------------------------------------------------
+__global__ void k_sqrt_w(const double* __restrict__ w, double* __restrict__ sw, int64_t n) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) sw[i] = sqrt(w[i]);
+}
+__global__ void k_gather_d(const double* __restrict__ src, const int32_t* __restrict__ idx,
+                           double* __restrict__ dst, int64_t n) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) dst[i] = src[idx[i]];
+}
+// cw = interaction * sqrt(w) in sorted observation order (the per-observation
+// part of the reference's cache!, src/SolverCPU.jl:91-95).
+__global__ void k_cw(const double* __restrict__ inter, const double* __restrict__ sw,
+                     double* __restrict__ cw_d, float* __restrict__ cw_f, int64_t n) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) {
+    double c = 1.0;
+    if (inter) c = inter[i];
+    if (sw) c *= sw[i];
+    cw_d[i] = c;
+    cw_f[i] = (float)c;
+  }
+}
+__global__ void k_cwp(const double* __restrict__ cw_d, const int32_t* __restrict__ perm,
+                      double* __restrict__ cwp_d, float* __restrict__ cwp_f, int64_t n) {
+  const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q < n) {
+    const double c = cw_d[perm ? perm[q] : q];
+    cwp_d[q] = c;
+    cwp_f[q] = (float)c;
+  }
+}
+
+static inline unsigned grid1(int64_t n, int b = 256) { return (unsigned)((n + b - 1) / b); }
+
+// ---------------------------------------------------------------------------
+// integer plan
+// ---------------------------------------------------------------------------
+// Stable counting sort of keys[0..n) with values in [0, nb): the restatement
+// of bucketize_refs (ext/MetalExt.jl:40-64) with 0-based positions.
+static void counting_sort(const int32_t* key, int64_t n, int64_t nb, std::vector<int64_t>& off,
+                          int32_t* perm, int64_t base_pos) {
+  off.assign((size_t)nb + 1, 0);
+  for (int64_t i = 0; i < n; ++i) off[(size_t)key[i] + 1] += 1;
+  for (int64_t l = 0; l < nb; ++l) off[(size_t)l + 1] += off[(size_t)l];
+  std::vector<int64_t> next(off.begin(), off.end() - 1);
+  for (int64_t i = 0; i < n; ++i) perm[next[(size_t)key[i]]++] = (int32_t)(base_pos + i);
+}
+
+int plan_build(fe_plan* pl, int32_t nprob, const int64_t* n_obs, int32_t K,
+               const int64_t* const* refs, const int64_t* n_levels,
+               const double* const* interaction, const double* weights, int32_t device) {
+  if (nprob < 1 || !n_obs) {
+    set_error("plan: need at least one problem");
+    return 1;
+  }
+  if (K < 1 || K > kMaxFE) {
+    set_error("plan: number of fixed effects must be in 1.." + std::to_string(kMaxFE));
+    return 1;
+  }
+  if (!refs || !n_levels) {
+    set_error("plan: refs and n_levels are required");
+    return 1;
+  }
+  pl->K = K;
+  pl->nprob = nprob;
+  pl->device = device;
+  pl->prob_obs_off.assign((size_t)nprob + 1, 0);
+  for (int p = 0; p < nprob; ++p) {
+    if (n_obs[p] < 0) {
+      set_error("plan: negative observation count");
+      return 1;
+    }
+    pl->prob_obs_off[p + 1] = pl->prob_obs_off[p] + n_obs[p];
+  }
+  const int64_t N = pl->prob_obs_off[nprob];
+  if (N >= (int64_t)INT32_MAX) {
+    set_error("plan: more than 2^31-1 observations is not supported");
+    return 1;
+  }
+  pl->N = N;
+  for (int k = 0; k < K; ++k)
+    if (N > 0 && !refs[k]) {
+      set_error("plan: refs[" + std::to_string(k) + "] is null");
+      return 1;
+    }
+  // per-problem level offsets and validation (refs are 1-based; 0 marks an FE
+  // absent from a problem, which requires n_levels == 0 there)
+  pl->prob_lev_off.assign((size_t)(nprob + 1) * K, 0);
+  pl->prob_nfe.assign(nprob, 0);
+  pl->nlev.assign(K, 0);
+  for (int p = 0; p < nprob; ++p)
+    for (int k = 0; k < K; ++k) {
+      const int64_t nl = n_levels[(int64_t)p * K + k];
+      if (nl < 0) {
+        set_error("plan: negative level count");
+        return 1;
+      }
+      pl->prob_lev_off[(size_t)(p + 1) * K + k] = pl->prob_lev_off[(size_t)p * K + k] + nl;
+      if (nl > 0) pl->prob_nfe[p] += 1;
+    }
+  for (int k = 0; k < K; ++k) {
+    pl->nlev[k] = pl->prob_lev_off[(size_t)nprob * K + k];
+    if (pl->nlev[k] >= (int64_t)INT32_MAX - 1) {
+      set_error("plan: too many levels");
+      return 1;
+    }
+  }
+  for (int p = 0; p < nprob; ++p) {
+    const int64_t o0 = pl->prob_obs_off[p], o1 = pl->prob_obs_off[p + 1];
+    for (int k = 0; k < K; ++k) {
+      const int64_t nl = n_levels[(int64_t)p * K + k];
+      const int64_t* r = refs[k];
+      for (int64_t i = o0; i < o1; ++i) {
+        const int64_t v = r[i];
+        if (nl == 0 ? (v != 0) : (v < 1 || v > nl)) {
+          set_error("plan: refs[" + std::to_string(k) + "][" + std::to_string(i) + "] = " +
+                    std::to_string(v) + " is outside 1.." + std::to_string(nl));
+          return 1;
+        }
+      }
+    }
+  }
+  // primary FE: the one with the most levels (its observations become
+  // contiguous, so its expand and reduce stream through memory)
+  pl->primary = 0;
+  for (int k = 1; k < K; ++k)
+    if (pl->nlev[k] > pl->nlev[pl->primary]) pl->primary = k;
+
+  FE_CK(cudaSetDevice(device));
+  if (!pl->stream) {
+    FE_CK(cudaStreamCreateWithFlags(&pl->stream, cudaStreamNonBlocking));
+    pl->own_stream = true;
+  }
+  cudaStream_t s = pl->stream;
+
+  // sorted observation order: stable sort of each problem by its primary level
+  std::vector<int32_t> obs_src((size_t)N), obs_dst((size_t)N);
+  {
+    std::vector<int32_t> key;
+    std::vector<int64_t> off;
+    const int kp = pl->primary;
+    for (int p = 0; p < nprob; ++p) {
+      const int64_t o0 = pl->prob_obs_off[p], o1 = pl->prob_obs_off[p + 1], n = o1 - o0;
+      const int64_t nl = n_levels[(int64_t)p * K + kp];
+      if (nl == 0) {
+        for (int64_t i = 0; i < n; ++i) obs_src[(size_t)(o0 + i)] = (int32_t)(o0 + i);
+        continue;
+      }
+      key.resize((size_t)n);
+      for (int64_t i = 0; i < n; ++i) key[(size_t)i] = (int32_t)(refs[kp][o0 + i] - 1);
+      counting_sort(key.data(), n, nl, off, obs_src.data() + o0, o0);
+    }
+    for (int64_t q = 0; q < N; ++q) obs_dst[(size_t)obs_src[(size_t)q]] = (int32_t)q;
+  }
+  int st = upload(pl->d_obs_src, obs_src.data(), (size_t)N, s);
+  if (!st) st = upload(pl->d_obs_dst, obs_dst.data(), (size_t)N, s);
+  if (st) return st;
+
+  // per-FE sorted refs (global level ids; the null level nlev[k] for problems
+  // without that FE) and the level order over sorted positions
+  pl->lev_base.assign(K, 0);
+  pl->P = 0;
+  for (int k = 0; k < K; ++k) {
+    pl->lev_base[k] = pl->P;
+    pl->P += pl->nlev[k] + 1;
+  }
+  pl->d_refs.resize(K);
+  pl->d_perm.resize(K);
+  pl->d_key.resize(K);
+  pl->perm_identity.assign(K, false);
+  pl->seg_off.assign(K, {});
+  pl->seg_len.assign(K, 0);
+  std::vector<int32_t> rs((size_t)N), perm((size_t)N), keyv((size_t)N);
+  for (int k = 0; k < K; ++k) {
+    for (int p = 0; p < nprob; ++p) {
+      const int64_t o0 = pl->prob_obs_off[p], o1 = pl->prob_obs_off[p + 1];
+      const int64_t nl = n_levels[(int64_t)p * K + k];
+      const int64_t lb = pl->prob_lev_off[(size_t)p * K + k];
+      for (int64_t q = o0; q < o1; ++q) {
+        const int64_t orig = obs_src[(size_t)q];
+        rs[(size_t)q] = nl == 0 ? (int32_t)pl->nlev[k] : (int32_t)(lb + refs[k][orig] - 1);
+      }
+    }
+    // counting sort over nlev+1 buckets; the null bucket comes last and is
+    // excluded from the level order
+    std::vector<int64_t>& off = pl->seg_off[k];
+    counting_sort(rs.data(), N, pl->nlev[k] + 1, off, perm.data(), 0);
+    const int64_t npos = off[(size_t)pl->nlev[k]];
+    pl->seg_len[k] = npos;
+    bool ident = (npos == N);
+    for (int64_t q = 0; q < npos && ident; ++q) ident = (perm[(size_t)q] == (int32_t)q);
+    pl->perm_identity[k] = ident;
+    for (int64_t l = 0; l < pl->nlev[k]; ++l)
+      for (int64_t q = off[(size_t)l]; q < off[(size_t)l + 1]; ++q) keyv[(size_t)q] = (int32_t)l;
+    st = upload(pl->d_refs[k], rs.data(), (size_t)N, s);
+    if (!st) st = upload(pl->d_key[k], keyv.data(), (size_t)std::max<int64_t>(npos, 1), s);
+    if (!st && !ident) st = upload(pl->d_perm[k], perm.data(), (size_t)std::max<int64_t>(npos, 1), s);
+    if (st) return st;
+    FE_CK(cudaStreamSynchronize(s));  // host vectors are reused
+  }
+
+  // interactions in sorted order
+  pl->interacted.assign(K, false);
+  pl->d_inter_sorted.resize(K);
+  {
+    std::vector<double> tmp((size_t)N);
+    for (int k = 0; k < K; ++k) {
+      if (!interaction || !interaction[k]) continue;
+      pl->interacted[k] = true;
+      for (int64_t q = 0; q < N; ++q) tmp[(size_t)q] = interaction[k][obs_src[(size_t)q]];
+      st = upload(pl->d_inter_sorted[k], tmp.data(), (size_t)N, s);
+      if (st) return st;
+      FE_CK(cudaStreamSynchronize(s));
+    }
+  }
+  pl->d_scale_d.resize(K);
+  pl->d_scale_f.resize(K);
+  pl->d_cw_d.resize(K);
+  pl->d_cw_f.resize(K);
+  pl->d_cwp_d.resize(K);
+  pl->d_cwp_f.resize(K);
+
+  // device view
+  FeDev& d = pl->dev;
+  memset(&d, 0, sizeof(d));
+  d.K = K;
+  d.N = N;
+  d.P = pl->P;
+  for (int k = 0; k < K; ++k) {
+    d.refs[k] = pl->d_refs[k].as<int32_t>();
+    d.perm[k] = pl->perm_identity[k] ? nullptr : pl->d_perm[k].as<int32_t>();
+    d.key[k] = pl->d_key[k].as<int32_t>();
+    d.lev_base[k] = pl->lev_base[k];
+  }
+  return plan_update_weights(pl, weights);
+}
+
+// update_weights!: src/SolverCPU.jl:67-76, ext/CUDAExt.jl:112-121.
+int plan_update_weights(fe_plan* pl, const double* weights) {
+  const int64_t N = pl->N;
+  const int K = pl->K;
+  cudaStream_t s = pl->stream;
+  FE_CK(cudaSetDevice(pl->device));
+  pl->weighted = weights != nullptr;
+  if (weights) {
+    DevBuf w;
+    int st = upload(w, weights, (size_t)N, s);
+    if (!st) st = pl->d_sw_orig.ensure((size_t)std::max<int64_t>(N, 1) * 8);
+    if (!st) st = pl->d_sw_sorted.ensure((size_t)std::max<int64_t>(N, 1) * 8);
+    if (st) return st;
+    if (N) {
+      k_sqrt_w<<<grid1(N), 256, 0, s>>>(w.as<double>(), pl->d_sw_orig.as<double>(), N);
+      k_gather_d<<<grid1(N), 256, 0, s>>>(pl->d_sw_orig.as<double>(), pl->d_obs_src.as<int32_t>(),
+                                          pl->d_sw_sorted.as<double>(), N);
+      FE_CK(cudaGetLastError());
+    }
+    FE_CK(cudaStreamSynchronize(s));
+  }
+  FeDev& d = pl->dev;
+  for (int k = 0; k < K; ++k) {
+    const int64_t nl = pl->nlev[k] + 1;
+    int st = pl->d_scale_d[k].ensure((size_t)nl * 8);
+    if (!st) st = pl->d_scale_f[k].ensure((size_t)nl * 4);
+    if (st) return st;
+    FE_CK(cudaMemsetAsync(pl->d_scale_d[k].p, 0, (size_t)nl * 8, s));
+    FE_CK(cudaMemsetAsync(pl->d_scale_f[k].p, 0, (size_t)nl * 4, s));
+    d.scale_d[k] = pl->d_scale_d[k].as<double>();
+    d.scale_f[k] = pl->d_scale_f[k].as<float>();
+    const bool has_cw = pl->weighted || pl->interacted[k];
+    if (has_cw) {
+      const int64_t np = std::max<int64_t>(pl->seg_len[k], 1);
+      st = pl->d_cw_d[k].ensure((size_t)std::max<int64_t>(N, 1) * 8);
+      if (!st) st = pl->d_cw_f[k].ensure((size_t)std::max<int64_t>(N, 1) * 4);
+      if (!st) st = pl->d_cwp_d[k].ensure((size_t)np * 8);
+      if (!st) st = pl->d_cwp_f[k].ensure((size_t)np * 4);
+      if (st) return st;
+      if (N) {
+        k_cw<<<grid1(N), 256, 0, s>>>(pl->interacted[k] ? pl->d_inter_sorted[k].as<double>() : nullptr,
+                                      pl->weighted ? pl->d_sw_sorted.as<double>() : nullptr,
+                                      pl->d_cw_d[k].as<double>(), pl->d_cw_f[k].as<float>(), N);
+        if (pl->seg_len[k])
+          k_cwp<<<grid1(pl->seg_len[k]), 256, 0, s>>>(pl->d_cw_d[k].as<double>(), d.perm[k],
+                                                       pl->d_cwp_d[k].as<double>(),
+                                                       pl->d_cwp_f[k].as<float>(), pl->seg_len[k]);
+        FE_CK(cudaGetLastError());
+      }
+      d.cw_d[k] = pl->d_cw_d[k].as<double>();
+      d.cw_f[k] = pl->d_cw_f[k].as<float>();
+      d.cwp_d[k] = pl->d_cwp_d[k].as<double>();
+      d.cwp_f[k] = pl->d_cwp_f[k].as<float>();
+    } else {
+      d.cw_d[k] = nullptr;
+      d.cw_f[k] = nullptr;
+      d.cwp_d[k] = nullptr;
+      d.cwp_f[k] = nullptr;
+    }
+  }
+  // Jacobi scales as a deterministic segmented reduction (C = 1 items)
+  ItemSet* its = nullptr;
+  int st = plan_items(pl, 1, &its);
+  if (st) return st;
+  if (!its->rd.empty()) {
+    EpiScale epi;
+    for (int k = 0; k < kMaxFE; ++k) {
+      epi.sd[k] = k < K ? pl->d_scale_d[k].as<double>() : nullptr;
+      epi.sf[k] = k < K ? pl->d_scale_f[k].as<float>() : nullptr;
+    }
+    DevBuf piece;
+    st = piece.ensure((size_t)std::max<int64_t>(its->n_pieces, 1) * 8);
+    if (st) return st;
+    FeDev dd = d;
+    dd.C = 1;
+    const unsigned grid = (unsigned)((its->rd.size() + kWarps - 1) / kWarps);
+    k_reduce<double, 1, 4, LoadScaleSq, EpiScale><<<grid, kThreads, 0, s>>>(
+        dd, its->d_rd.as<ReduceItem>(), (int64_t)its->rd.size(), LoadScaleSq{}, epi,
+        its->d_splits.as<SplitLevel>(), piece.as<double>(), its->d_split_cnt.as<int32_t>(), nullptr,
+        nullptr, 0, nullptr);
+    FE_CK(cudaGetLastError());
+    FE_CK(cudaStreamSynchronize(s));
+  }
+  return 0;
+}
+
+// ---------------------------------------------------------------------------
+// work items for a column tile width C
+// ---------------------------------------------------------------------------
+static int64_t round_up(int64_t a, int64_t b) { return (a + b - 1) / b * b; }
+
+int plan_items(fe_plan* pl, int C, ItemSet** out) {
+  auto itf = pl->items.find(C);
+  if (itf != pl->items.end()) {
+    *out = itf->second.get();
+    return 0;
+  }
+  std::unique_ptr<ItemSet> its(new ItemSet());
+  its->C = C;
+  const int G = 32 / C;
+  const int U = 4;
+  const int64_t batch = (int64_t)G * U;
+  int sms = 148;
+  {
+    int dev = pl->device, v = 0;
+    if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess && v > 0) sms = v;
+  }
+  const int64_t warps_target = (int64_t)sms * 64 * 4;
+  const int64_t cap = std::max<int64_t>(batch, 16384 / C);
+  const int64_t Te = std::min(cap, std::max(batch, round_up((pl->N + warps_target - 1) / warps_target, batch)));
+  int64_t total_pos = 0;
+  for (int k = 0; k < pl->K; ++k) total_pos += pl->seg_len[k];
+  const int64_t Tr = std::min(cap, std::max(batch, round_up((total_pos + warps_target - 1) / warps_target, batch)));
+
+  const int nprob = pl->nprob;
+  const int K = pl->K;
+  its->ex_slot_off.assign((size_t)nprob + 1, 0);
+  its->rd_slot_off.assign((size_t)nprob + 1, 0);
+  int64_t slot = 0;
+  for (int p = 0; p < nprob; ++p) {
+    // expand items: chunks of the problem's sorted observation range
+    const int64_t o0 = pl->prob_obs_off[p], o1 = pl->prob_obs_off[p + 1];
+    const size_t e0 = its->ex.size();
+    for (int64_t b = o0; b < o1; b += Te) its->ex.push_back({b, std::min(o1, b + Te), p, 0});
+    while ((its->ex.size() - e0) % kWarps) its->ex.push_back({o1, o1, p, 0});
+    if (its->ex.size() == e0)
+      for (int w = 0; w < kWarps; ++w) its->ex.push_back({o1, o1, p, 0});
+    its->ex_slot_off[p + 1] = (int64_t)(its->ex.size() / kWarps);
+  }
+  // reduce items, CTA slots and split levels (slots of a problem contiguous)
+  std::vector<int32_t> split_of_problem_count(nprob, 0);
+  for (int p = 0; p < nprob; ++p) {
+    const size_t r0 = its->rd.size();
+    std::vector<int32_t> splits_here;
+    for (int k = 0; k < K; ++k) {
+      const int64_t lb = pl->prob_lev_off[(size_t)p * K + k];
+      const int64_t le = pl->prob_lev_off[(size_t)(p + 1) * K + k];
+      if (le == lb) continue;
+      const std::vector<int64_t>& off = pl->seg_off[k];
+      int64_t cur_b = -1, cur_e = -1;
+      for (int64_t l = lb; l < le; ++l) {
+        const int64_t b = off[(size_t)l], e = off[(size_t)l + 1], cnt = e - b;
+        if (cnt == 0) continue;
+        if (cnt > Tr) {
+          if (cur_b >= 0) {
+            its->rd.push_back({cur_b, cur_e, k, p, -1, 0});
+            cur_b = -1;
+          }
+          const int64_t npieces = (cnt + Tr - 1) / Tr;
+          const int64_t psz = (cnt + npieces - 1) / npieces;
+          SplitLevel sl;
+          sl.first_piece = (int32_t)its->n_pieces;
+          sl.npieces = (int32_t)npieces;
+          sl.fe = k;
+          sl.level = (int32_t)l;
+          sl.norm_slot = -1;
+          sl.pad = 0;
+          const int32_t sid = (int32_t)its->splits.size();
+          its->splits.push_back(sl);
+          splits_here.push_back(sid);
+          for (int64_t q = 0; q < npieces; ++q) {
+            const int64_t pb = b + q * psz, pe = std::min(e, pb + psz);
+            its->rd.push_back({pb, pe, k, p, sid, (int32_t)q});
+          }
+          its->n_pieces += npieces;
+          continue;
+        }
+        if (cur_b < 0) {
+          cur_b = b;
+          cur_e = e;
+        } else {
+          cur_e = e;
+        }
+        if (cur_e - cur_b >= Tr) {
+          its->rd.push_back({cur_b, cur_e, k, p, -1, 0});
+          cur_b = -1;
+        }
+      }
+      if (cur_b >= 0) its->rd.push_back({cur_b, cur_e, k, p, -1, 0});
+    }
+    while ((its->rd.size() - r0) % kWarps) its->rd.push_back({0, 0, 0, p, -1, 0});
+    if (its->rd.size() == r0)
+      for (int w = 0; w < kWarps; ++w) its->rd.push_back({0, 0, 0, p, -1, 0});
+    its->rd_slot_off[p] = slot;
+    const int64_t ncta = (int64_t)((its->rd.size() - r0) / kWarps);
+    for (int64_t c = 0; c < ncta; ++c) its->rd_cta_slot.push_back((int32_t)(slot + c));
+    slot += ncta;
+    for (int32_t sid : splits_here) its->splits[(size_t)sid].norm_slot = (int32_t)(slot++);
+    its->rd_slot_off[p + 1] = slot;
+  }
+  its->Se = its->ex_slot_off[nprob];
+  its->Sr = slot;
+
+  cudaStream_t s = pl->stream;
+  int st = upload(its->d_ex, its->ex.data(), its->ex.size(), s);
+  if (!st) st = upload(its->d_rd, its->rd.data(), its->rd.size(), s);
+  if (!st) st = upload(its->d_splits, its->splits.data(), std::max<size_t>(its->splits.size(), 1), s);
+  if (!st) st = upload(its->d_cta_slot, its->rd_cta_slot.data(), its->rd_cta_slot.size(), s);
+  if (!st) st = upload(its->d_ex_off, its->ex_slot_off.data(), its->ex_slot_off.size(), s);
+  if (!st) st = upload(its->d_rd_off, its->rd_slot_off.data(), its->rd_slot_off.size(), s);
+  if (!st) st = its->d_split_cnt.ensure(std::max<size_t>(its->splits.size(), 1) * 4);
+  if (st) return st;
+  FE_CK(cudaMemsetAsync(its->d_split_cnt.p, 0, std::max<size_t>(its->splits.size(), 1) * 4, s));
+  FE_CK(cudaStreamSynchronize(s));
+  *out = its.get();
+  pl->items[C] = std::move(its);
+  return 0;
+}
+
+int plan_destroy(fe_plan* pl) {
+  if (!pl) return 0;
+  cudaSetDevice(pl->device);
+  if (pl->stream) cudaStreamSynchronize(pl->stream);
+  for (auto& e : pl->prof.pool) cudaEventDestroy(e);
+  for (auto& pr : pl->prof.pending) {
+    cudaEventDestroy(pr.second.first);
+    cudaEventDestroy(pr.second.second);
+  }
+  if (pl->host_pinned) cudaFreeHost(pl->host_pinned);
+  cudaStream_t s = pl->stream;
+  bool own = pl->own_stream;
+  delete pl;
+  if (own && s) cudaStreamDestroy(s);
+  return 0;
+}
+
+}  // namespace fe

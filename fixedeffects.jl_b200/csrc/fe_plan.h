@@ -1,0 +1,132 @@
+// fe_plan.h -- the solver plan: the device-resident replacement of the
+// reference's AbstractFixedEffectSolver{T}(fes, w, Val{:CUDA}) object
+// (ext/CUDAExt.jl:86-121).  Internal; the C ABI is include/fe_b200.h.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "fe_internal.h"
+
+namespace fe {
+
+// thread-local last error (fe_last_error)
+void set_error(const std::string& msg);
+const char* last_error();
+
+#define FE_CK(call)                                                                     \
+  do {                                                                                  \
+    cudaError_t e_ = (call);                                                            \
+    if (e_ != cudaSuccess) {                                                            \
+      ::fe::set_error(std::string("CUDA error ") + cudaGetErrorString(e_) + " at " +    \
+                      __FILE__ + ":" + std::to_string(__LINE__) + " (" #call ")");      \
+      return 2; /* FE_ERR_CUDA */                                                       \
+    }                                                                                   \
+  } while (0)
+
+// A device allocation owned by the plan.
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  ~DevBuf();
+  int ensure(size_t n);  // grows (contents not preserved)
+  template <typename T> T* as() const { return static_cast<T*>(p); }
+};
+
+// Work items for one column-tile width C.
+struct ItemSet {
+  int C = 0;
+  std::vector<ExpandItem> ex;
+  std::vector<ReduceItem> rd;
+  std::vector<SplitLevel> splits;
+  std::vector<int32_t> rd_cta_slot;       // per reduce CTA
+  std::vector<int64_t> ex_slot_off;       // per problem, expand slots
+  std::vector<int64_t> rd_slot_off;       // per problem, reduce slots
+  int64_t n_pieces = 0;
+  int64_t Se = 0, Sr = 0;                 // slot counts
+  DevBuf d_ex, d_rd, d_splits, d_cta_slot, d_ex_off, d_rd_off, d_split_cnt;
+};
+
+struct Workspace {
+  int C = 0;
+  DevBuf B64, R64, U, V, H, Hb, X, X64;
+  DevBuf part_e, part_a, part_b, piece_part, inst, counters;
+  DevBuf coef;
+  DevBuf ystage;  // device copy of host Y for host-buffer solves
+};
+
+struct Profile {
+  bool on = false;
+  std::map<std::string, KernelStat> stats;
+  std::vector<std::pair<std::string, std::pair<cudaEvent_t, cudaEvent_t>>> pending;
+  std::vector<cudaEvent_t> pool;
+  std::map<std::string, double> bytes_per_launch;
+};
+
+}  // namespace fe
+
+struct fe_plan {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+
+  int64_t N = 0;
+  int32_t K = 0;
+  int32_t nprob = 1;
+  int32_t primary = 0;
+  bool weighted = false;
+  std::vector<bool> interacted;
+  std::vector<int64_t> nlev;           // per FE: total levels over problems
+  std::vector<int64_t> prob_obs_off;   // nprob+1
+  std::vector<int64_t> prob_lev_off;   // [(nprob+1) * K]: first global level of problem p in FE k
+  std::vector<int32_t> prob_nfe;       // FEs present in each problem
+  std::vector<int64_t> lev_base;       // per FE, row base in [P][C] slabs
+  int64_t P = 0;                       // slab rows (levels + one null level per FE)
+  std::vector<std::vector<int64_t>> seg_off;  // per FE: level-order offsets (host)
+  std::vector<int64_t> seg_len;        // per FE: positions in level order
+
+  // device integer plan
+  fe::DevBuf d_obs_src, d_obs_dst;     // sorted -> original, original -> sorted
+  std::vector<fe::DevBuf> d_refs, d_perm, d_key;
+  std::vector<bool> perm_identity;
+  // device weights/interaction/preconditioner
+  fe::DevBuf d_sw_orig, d_sw_sorted;
+  std::vector<fe::DevBuf> d_inter_sorted;
+  std::vector<fe::DevBuf> d_scale_d, d_scale_f, d_cw_d, d_cw_f, d_cwp_d, d_cwp_f;
+
+  fe::FeDev dev{};                     // device view (C patched per launch)
+
+  // options
+  int32_t opt_tile = 0;        // 0 = automatic
+  int32_t opt_check_every = 4; // iterations between host convergence checks
+  int32_t opt_max_rounds = 8;  // mixed-precision refinement rounds
+  int32_t opt_unroll = 0;      // reserved
+  double opt_inner_rho = 1e-6;
+  double opt_inner_theta = 0.5;
+
+  std::map<int, std::unique_ptr<fe::ItemSet>> items;  // by C
+  fe::Workspace ws;
+  fe::Profile prof;
+  void* host_pinned = nullptr;  // small pinned staging for counters
+
+  // results of the last solve (per column)
+  std::vector<double> last_test2;
+  std::vector<int32_t> last_rounds;
+  std::vector<int64_t> last_iters_raw;
+  std::vector<int64_t> last_prob_iters;
+  std::vector<uint8_t> last_prob_conv;
+};
+
+namespace fe {
+int plan_build(fe_plan* pl, int32_t nprob, const int64_t* n_obs, int32_t K,
+               const int64_t* const* refs, const int64_t* n_levels,
+               const double* const* interaction, const double* weights, int32_t device);
+int plan_update_weights(fe_plan* pl, const double* weights);
+int plan_items(fe_plan* pl, int C, ItemSet** out);
+int plan_destroy(fe_plan* pl);
+}  // namespace fe

@@ -1,0 +1,29 @@
+// fe_solve.h -- internal entry of the solve drivers (fe_solve.cu).
+#pragma once
+
+#include <stdint.h>
+
+#include "fe_plan.h"
+
+namespace fe {
+
+struct SolveReq {
+  void* Y = nullptr;       // device, column-major N x ncols, leading dimension ld
+  int32_t dtype = 0;       // 0: float64, 1: float32
+  int64_t ncols = 0;
+  int64_t ld = 0;
+  int32_t precision = 0;   // 0 FP64, 1 MIXED, 2 FP32
+  double tol = 1e-8;
+  int64_t maxiter = 10000;
+  bool residuals = true;   // false: solve_coefficients!
+  int64_t* iters = nullptr;          // per column
+  uint8_t* converged = nullptr;      // per column
+  int64_t* prob_iters = nullptr;     // optional [nprob][ncols]
+  uint8_t* prob_converged = nullptr; // optional [nprob][ncols]
+  double* const* coefs = nullptr;    // host, per FE (coefficients mode)
+};
+
+int solve(fe_plan* pl, const SolveReq& rq);
+int prof_flush(fe_plan* pl);
+
+}  // namespace fe

@@ -1,0 +1,176 @@
+/*
+ * fe_b200.h -- C ABI of the B200-native fixed-effects LSMR library
+ * (libfe_b200.so, built for sm_100a).
+ *
+ * This is the drop-in boundary for FixedEffects.jl's GPU solver path.  A host
+ * binding (a Julia ccall extension, Python ctypes, ...) calls these functions
+ * with plain pointers and sizes; no CUDA, torch or Julia types appear here.
+ * Each declaration names the reference interface it replaces (paths are
+ * relative to the FixedEffects.jl project root).
+ *
+ * Conventions
+ *   - Every function returns a status: FE_OK (0) or an FE_ERR_* code; the
+ *     message of the last error of the calling thread is fe_last_error().
+ *     Input errors are reported, never thrown; non-convergence is not an
+ *     error (it is returned in `converged`, as the reference does).
+ *   - refs are 1-based level ids, as FixedEffect.refs in the reference
+ *     (src/FixedEffect.jl:7-21).  interaction[k] == NULL means
+ *     UnitWeights; weights == NULL means UnitWeights.
+ *   - Y is column-major (Julia layout): column j starts at Y + j*ld.
+ *   - A plan is not thread-safe; different plans may be used concurrently.
+ *     The plan owns all device memory; host buffers are borrowed for the
+ *     duration of a call.  For host-buffer calls, pinned (page-locked)
+ *     memory gives full PCIe bandwidth.
+ */
+#ifndef FE_B200_H
+#define FE_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FE_B200_VERSION 1
+
+/* status codes */
+#define FE_OK 0
+#define FE_ERR_INVALID 1 /* bad argument (lengths, level ids, null pointers) */
+#define FE_ERR_CUDA 2    /* CUDA runtime error (message in fe_last_error) */
+#define FE_ERR_ALLOC 3   /* device allocation failed */
+#define FE_ERR_TIMEOUT 4 /* a bounded device wait gave up */
+
+/* precision modes (the reference's `double_precision` keyword,
+ * src/AbstractFixedEffectSolver.jl:37-43) */
+#define FE_PREC_FP64 0  /* FP64 bulk + FP64 scalars: double_precision = true  */
+#define FE_PREC_MIXED 1 /* FP32 bulk + FP64 scalars + FP64 refinement to tol  */
+#define FE_PREC_FP32 2  /* FP32 bulk + FP64 scalars, no refinement            */
+
+/* element types of Y */
+#define FE_DTYPE_F64 0
+#define FE_DTYPE_F32 1
+
+/* plan options (fe_plan_set_option) */
+#define FE_OPT_TILE 1        /* column-tile width cap: 0 auto (<=32), 1,2,4,..,32 */
+#define FE_OPT_CHECK_EVERY 2 /* LSMR iterations between host convergence checks */
+#define FE_OPT_MAX_ROUNDS 3  /* FP64 refinement rounds (FE_PREC_MIXED) */
+#define FE_OPT_PROFILE 4     /* 1: time every launch with CUDA events */
+#define FE_OPT_INNER_RHO 5   /* FP32 inner-solve floor (relative ||A'r|| drop) */
+
+typedef struct fe_plan fe_plan;
+
+/* Library version (FE_B200_VERSION). */
+int fe_version(void);
+
+/* Message of the last failed call on this thread ("" if none). */
+const char* fe_last_error(void);
+
+/*
+ * Builds a solver plan on `device`: validates refs, builds the integer plan
+ * (stable counting sorts by level), uploads it, and computes the Jacobi
+ * preconditioner on the GPU.
+ * Replaces AbstractFixedEffectSolver{T}(fes, w, Val{:CUDA})
+ * (ext/CUDAExt.jl:99-110) and its update_weights! (ext/CUDAExt.jl:112-121);
+ * CPU counterpart src/SolverCPU.jl:55-95.
+ *   refs[k]        n_obs level ids in 1..n_levels[k]
+ *   interaction[k] n_obs values or NULL; `interaction` itself may be NULL
+ *   weights        n_obs non-negative weights or NULL
+ */
+int fe_plan_create(fe_plan** out, int64_t n_obs, int32_t n_fe, const int64_t* const* refs,
+                   const int64_t* n_levels, const double* const* interaction,
+                   const double* weights, int32_t device);
+
+/*
+ * A plan over many independent problems solved together (one batched LSMR
+ * with per-problem scalars and stopping tests).  Observations of all problems
+ * are concatenated (problem p has n_obs[p] rows); refs[k] holds the
+ * problem-local 1-based level ids, and n_levels is [n_problems][n_fe].  A
+ * problem without FE k has n_levels[p*n_fe+k] == 0 and refs entries 0.
+ * No reference counterpart as a single call: it batches many
+ * AbstractFixedEffectSolver objects (ext/CUDAExt.jl:99-110).
+ */
+int fe_plan_create_batch(fe_plan** out, int32_t n_problems, const int64_t* n_obs, int32_t n_fe,
+                         const int64_t* const* refs, const int64_t* n_levels,
+                         const double* const* interaction, const double* weights,
+                         int32_t device);
+
+/* update_weights!(feM, w): src/SolverCPU.jl:67-76, ext/CUDAExt.jl:112-121. */
+int fe_plan_update_weights(fe_plan* plan, const double* weights);
+
+/* Runs the plan's work on a caller stream (a cudaStream_t passed as void*);
+ * NULL restores the plan's own stream. */
+int fe_plan_set_stream(fe_plan* plan, void* stream);
+
+/* Sets an FE_OPT_* option. */
+int fe_plan_set_option(fe_plan* plan, int32_t option, double value);
+
+/* Frees the plan and all its device memory. */
+int fe_plan_destroy(fe_plan* plan);
+
+/*
+ * solve_residuals!(Y, feM; tol, maxiter) for every column of Y, in place
+ * (host memory).  Replaces src/AbstractFixedEffectSolver.jl:49-68 and the
+ * column loop of :74-97 (columns are batched, up to 32 per LSMR tile).
+ * iterations[j] = LSMR iterations + 1 (the reference's ch.mvps + 1);
+ * converged[j] = the reference's ch.isconverged (FE_PREC_MIXED: the FP64
+ * tests passed).  With several problems a column reports the maximum
+ * iterations and the conjunction of convergence flags over problems
+ * (fe_plan_problem_results gives them per problem).
+ */
+int fe_solve_residuals(fe_plan* plan, void* Y, int32_t dtype, int64_t ncols, int64_t ld,
+                       int32_t precision, double tol, int64_t maxiter, int64_t* iterations,
+                       uint8_t* converged);
+
+/* As fe_solve_residuals with Y in device memory (no host copies). */
+int fe_solve_residuals_device(fe_plan* plan, void* Y_dev, int32_t dtype, int64_t ncols,
+                              int64_t ld, int32_t precision, double tol, int64_t maxiter,
+                              int64_t* iterations, uint8_t* converged);
+
+/*
+ * solve_coefficients!(y, feM; tol, maxiter) up to, not including, the
+ * normalisation: LSMR from x = 0 (src/AbstractFixedEffectSolver.jl:147-157)
+ * and coefs[k][l] = x_k[l] * scale_k[l] for l < n_levels[k] (host memory).
+ * normalize!/full (src/FixedEffect.jl:106-140) stay in the host binding.
+ * iterations = div(ch.mvps, 2) as the reference returns.
+ */
+int fe_solve_coefficients(fe_plan* plan, const void* y, int32_t dtype, int32_t precision,
+                          double tol, int64_t maxiter, double* const* coefs,
+                          int64_t* iterations, uint8_t* converged);
+
+/* Per-problem iterations/convergence of the last solve: [n_problems][ncols]. */
+int fe_plan_problem_results(fe_plan* plan, int64_t* iterations, uint8_t* converged);
+
+/* Diagnostics of the last solve per column: the FP64 test2 of the last
+ * refinement round, the number of rounds, and the raw LSMR iteration count. */
+int fe_plan_last_solve_info(fe_plan* plan, int64_t ncols, double* test2, int32_t* rounds,
+                            int64_t* lsmr_iters);
+
+/*
+ * The integer plan (single-problem plans), for bit-exact checks against the
+ * stable counting sort of ext/MetalExt.jl:40-64 (bucketize_refs):
+ *   perm0[p]      original observation (0-based) at sorted position p
+ *   offsets[k]    n_levels[k]+1 level offsets into FE k's level order
+ *   segperm[k][q] sorted position of entry q of FE k's level order
+ * Any output pointer may be NULL.
+ */
+int fe_plan_get_integer_plan(fe_plan* plan, int32_t* perm0, int64_t* const* offsets,
+                             int32_t* const* segperm);
+
+/* Jacobi scales scale_k (src/SolverCPU.jl:78-89), n_levels[k] values per FE. */
+int fe_plan_get_scales(fe_plan* plan, double* const* scales);
+
+/* Index of the FE whose levels order the observations. */
+int fe_plan_primary(fe_plan* plan, int32_t* primary);
+
+/* Launch statistics collected with FE_OPT_PROFILE: kernel `index`'s name,
+ * launches, total CUDA-event milliseconds and algorithmic bytes.  Returns
+ * FE_ERR_INVALID past the last kernel. */
+int fe_plan_kernel_stat(fe_plan* plan, int32_t index, char* name, int64_t name_len,
+                        int64_t* launches, double* total_ms, double* alg_bytes);
+int fe_plan_reset_stats(fe_plan* plan);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FE_B200_H */

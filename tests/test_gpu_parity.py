@@ -1,0 +1,270 @@
+"""GPU parity: the CUDA path through the C ABI against the oracle and the
+reference's golden vectors (test/solve.jl)."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+REL = 1e-6  # residual / fitted-value bar (relative, 2-norm per column)
+
+
+def rel_err(a, b):
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def julia_isapprox(a, b, rtol):
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    return np.linalg.norm(a - b) <= rtol * max(np.linalg.norm(a), np.linalg.norm(b))
+
+
+@pytest.fixture(scope="module")
+def g(golden):
+    return {k: np.asarray(v) for k, v in golden.items() if isinstance(v, list)}
+
+
+# --- test/solve.jl golden cases --------------------------------------------
+def test_golden_residuals_fp64(fe, g, oracle):
+    fes = [fe.FixedEffect(g["p1"]), fe.FixedEffect(g["p2"])]
+    r, it, cv = fe.solve_residuals(g["x"].copy(), fes, double_precision=True)
+    assert cv
+    assert julia_isapprox(r, g["r_ols"], np.sqrt(np.finfo(np.float64).eps))
+    _, it_o, _ = oracle.solve_residuals(g["x"], [g["p1"], g["p2"]])
+    assert it == it_o
+
+
+def test_golden_residuals_float32(fe, g):
+    fes = [fe.FixedEffect(g["p1"]), fe.FixedEffect(g["p2"])]
+    for prec in ("mixed", "fp32"):
+        r, it, cv = fe.solve_residuals(g["x"].copy(), fes, double_precision=False, precision=prec)
+        assert julia_isapprox(np.float32(r), np.float32(g["r_ols"]), np.sqrt(np.finfo(np.float32).eps))
+
+
+def test_golden_coefficients(fe, g):
+    fes = [fe.FixedEffect(g["p1"]), fe.FixedEffect(g["p2"])]
+    for dp in (True, False):
+        coefs, it, cv = fe.solve_coefficients(g["x"].copy(), fes, double_precision=dp)
+        assert cv
+        rtol = np.sqrt(np.finfo(np.float64 if dp else np.float32).eps)
+        assert julia_isapprox(g["x"] - coefs[0] - coefs[1], g["r_ols"], rtol)
+
+
+def test_golden_pooled_and_categorical_equivalents(fe, g):
+    # PooledArray / CategoricalArray refs relabel levels; residuals must not move
+    p1s = np.array([f"a{v}" for v in g["p1"]])
+    p2s = (g["p2"] * 7 + 100)
+    fes = [fe.FixedEffect(p1s), fe.FixedEffect(p2s)]
+    r, _, _ = fe.solve_residuals(g["x"].copy(), fes, double_precision=True)
+    assert julia_isapprox(r, g["r_ols"], np.sqrt(np.finfo(np.float64).eps))
+
+
+def test_length_mismatch_message(fe):
+    with pytest.raises(ValueError, match="FixedEffects must have the same length as y"):
+        fe.solve_residuals(np.ones(100), [fe.FixedEffect([1, 2])])
+
+
+def test_update_weights_round_trip(fe, g, oracle):
+    fes = [fe.FixedEffect(g["p1"])]
+    feM = fe.AbstractFixedEffectSolver(fes, np.ones(10), "CUDA", np.float64)
+    for w in (np.arange(1, 11, dtype=float), np.arange(10, 0, -1, dtype=float)):
+        fe.update_weights(feM, w)
+        r1 = feM.solve_residuals(g["x"].copy())[0]
+        r2 = fe.solve_residuals(g["x"].copy(), fes, w, double_precision=True)[0]
+        ro = oracle.solve_residuals(g["x"], [g["p1"]], weights=w)[0]
+        assert rel_err(r1, r2) < 1e-12
+        assert rel_err(r1, ro) < 1e-12
+
+
+def test_interacted_converges(fe, g):
+    inter = g["interaction"]
+    r, it, cv = fe.solve_residuals(g["x"].copy(), [fe.FixedEffect(g["p1"], interaction=inter)],
+                                   double_precision=True)
+    assert cv
+    r, it, cv = fe.solve_residuals(
+        g["x"].copy(), [fe.FixedEffect(g["p1"]), fe.FixedEffect(g["p1"], interaction=inter)],
+        double_precision=True)
+    assert cv
+
+
+# --- seeded workloads at oracle-sized scales ---------------------------------
+def _problem(synth, cfg, scale, ncols=None):
+    kw = {}
+    if ncols is not None:
+        kw["ncols"] = ncols
+    return synth.make(cfg, scale=scale, **kw)
+
+
+@pytest.mark.parametrize("cfg,scale,ncols", [(0, 0.02, None), (1, 0.002, None), (2, 0.002, 5),
+                                             (4, 0.0002, 3)])
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_configs_vs_oracle(fe, oracle, synth, cfg, scale, ncols, prec):
+    pb = _problem(synth, cfg, scale, ncols)
+    Y = np.asfortranarray(pb.Y.astype(np.float64))
+    fes = [fe.FixedEffect.from_refs(r, n, a) for r, n, a in zip(pb.refs, pb.nlev, pb.interaction)]
+    R_o, it_o, cv_o = oracle.solve_residuals_cols(Y, pb.refs, pb.nlev, pb.interaction, pb.weights,
+                                                 tol=1e-8, maxiter=10000)
+    assert cv_o.all()
+    for tile in (1, 0):
+        feM = fe.AbstractFixedEffectSolver(fes, pb.weights, "CUDA", np.float64, precision=prec)
+        feM.set_option(fe._lib.FE_OPT_TILE, tile)
+        R, its, cvs = feM.solve_residuals(Y.copy(), tol=1e-8, maxiter=10000)
+        feM.close()
+        assert cvs.all()
+        for j in range(Y.shape[1]):
+            assert rel_err(R[:, j], R_o[:, j]) < REL
+            assert rel_err(Y[:, j] - R[:, j], Y[:, j] - R_o[:, j]) < REL
+        if prec == "fp64":
+            assert np.all(np.abs(its - it_o) <= 1), (its, it_o)
+
+
+def test_integer_plan_bit_exact(fe, oracle, synth):
+    pb = synth.make(2, scale=0.002, ncols=1)
+    fes = [fe.FixedEffect.from_refs(r, n) for r, n in zip(pb.refs, pb.nlev)]
+    feM = fe.AbstractFixedEffectSolver(fes, None, "CUDA", np.float64)
+    perm0, offs, segs = feM.integer_plan()
+    p0, o_offs, o_segs = oracle.integer_plan(pb.refs, pb.nlev, feM.primary())
+    assert np.array_equal(perm0, p0)
+    for k in range(len(fes)):
+        assert np.array_equal(offs[k], o_offs[k])
+        assert np.array_equal(segs[k], o_segs[k])
+    feM.close()
+
+
+def test_scales_match_oracle(fe, oracle, synth):
+    pb = synth.make(1, scale=0.002)
+    fes = [fe.FixedEffect.from_refs(r, n, a) for r, n, a in zip(pb.refs, pb.nlev, pb.interaction)]
+    feM = fe.AbstractFixedEffectSolver(fes, pb.weights, "CUDA", np.float64)
+    sc = feM.scales()
+    for k in range(len(fes)):
+        so = oracle.scale(pb.refs[k], pb.nlev[k], pb.interaction[k], pb.weights)
+        assert np.allclose(sc[k], so, rtol=1e-13, atol=0)
+    feM.close()
+
+
+def test_deterministic_bitwise(fe, synth):
+    pb = synth.make(2, scale=0.003, ncols=4)
+    fes = [fe.FixedEffect.from_refs(r, n) for r, n in zip(pb.refs, pb.nlev)]
+    outs = []
+    for _ in range(2):
+        feM = fe.AbstractFixedEffectSolver(fes, None, "CUDA", np.float32)
+        R, its, cvs = feM.solve_residuals(np.asfortranarray(pb.Y.copy()), tol=1e-8)
+        feM.close()
+        outs.append((R, its))
+    assert np.array_equal(outs[0][0], outs[1][0])
+    assert np.array_equal(outs[0][1], outs[1][1])
+
+
+def test_batch_problems_vs_oracle(fe, oracle, synth):
+    probs = synth.make(3, scale=0.01, nproblems=12)
+    fes_list = [[fe.FixedEffect.from_refs(r, n, a) for r, n, a in zip(p.refs, p.nlev, p.interaction)]
+                for p in probs]
+    for prec in ("fp64", "mixed"):
+        bs = fe.BatchSolver(fes_list, [p.weights for p in probs], precision=prec)
+        outs, its, cvs = bs.solve_residuals([p.Y[:, 0] for p in probs], tol=1e-8, maxiter=10000)
+        bs.close()
+        assert cvs.all()
+        for p, r in zip(probs, outs):
+            ro, it_o, cv_o = oracle.solve_residuals(p.Y[:, 0].astype(np.float64), p.refs, p.nlev,
+                                                    p.interaction, p.weights, tol=1e-8)
+            assert rel_err(r, ro) < 1e-5  # inputs are Float32 columns
+
+
+def test_device_tensor_path(fe, synth, oracle):
+    import torch
+    pb = synth.make(0, scale=0.01)
+    fes = [fe.FixedEffect.from_refs(r, n) for r, n in zip(pb.refs, pb.nlev)]
+    y = pb.Y[:, 0].astype(np.float64)
+    ro = oracle.solve_residuals(y, pb.refs, pb.nlev, tol=1e-8)[0]
+    feM = fe.AbstractFixedEffectSolver(fes, None, "CUDA", np.float32)
+    t = torch.tensor(y, device="cuda")
+    t, it, cv = feM.solve_residuals(t, tol=1e-8)
+    torch.cuda.synchronize()
+    feM.close()
+    assert cv
+    assert rel_err(t.cpu().numpy(), ro) < REL
+
+
+def test_coefficients_vs_oracle(fe, oracle, synth):
+    pb = synth.make(1, scale=0.001)
+    fes = [fe.FixedEffect.from_refs(r, n, a) for r, n, a in zip(pb.refs, pb.nlev, pb.interaction)]
+    y = pb.Y[:, 0]
+    lv_o, full_o, it_o, cv_o = oracle.solve_coefficients(y, pb.refs, pb.nlev, pb.interaction,
+                                                          pb.weights, tol=1e-8)
+    for dp in (True, False):
+        full_g, it, cv = fe.solve_coefficients(y.copy(), fes, pb.weights, double_precision=dp,
+                                               tol=1e-8)
+        assert cv
+        fit_g = sum(c * (1 if a is None else a) for c, a in zip(full_g, pb.interaction))
+        fit_o = sum(c * (1 if a is None else a) for c, a in zip(full_o, pb.interaction))
+        assert rel_err(fit_g, fit_o) < REL
+        if dp:
+            assert abs(it - it_o) <= 1
+
+
+# --- edge cases --------------------------------------------------------------
+def test_single_fe_is_projection(fe, oracle):
+    rng = np.random.default_rng(5)
+    r = rng.integers(1, 30, 500)
+    y = rng.standard_normal(500)
+    ro, it_o, cv_o = oracle.solve_residuals(y, [r])
+    for dp in (True, False):
+        out, it, cv = fe.solve_residuals(y.copy(), [fe.FixedEffect(r)], double_precision=dp)
+        assert it == 1 and it_o == 1 and cv
+        assert rel_err(out, ro) < 1e-12
+
+
+def test_unobserved_levels_and_zero_weights(fe, oracle):
+    rng = np.random.default_rng(6)
+    N = 3000
+    r1 = rng.integers(1, 200, N)
+    r2 = rng.integers(1, 20, N)
+    w = rng.uniform(0.5, 1.5, N)
+    w[r2 == 3] = 0.0  # a level whose weights are all zero gets scale 0 (issue #97)
+    y = rng.standard_normal(N)
+    fes = [fe.FixedEffect.from_refs(r1, 250), fe.FixedEffect.from_refs(r2, 25)]
+    w_pos = w.copy()
+    w_pos[w_pos == 0] = 1.0  # residuals are divided by sqrt(w): compare where w > 0
+    ro = oracle.solve_residuals(y, [r1, r2], [250, 25], weights=w)[0]
+    out, it, cv = fe.solve_residuals(y.copy(), fes, w, double_precision=True)
+    m = w > 0
+    assert rel_err(out[m], ro[m]) < 1e-9
+
+
+def test_maxiter_one_quirk(fe, oracle, g):
+    fes = [fe.FixedEffect(g["p1"]), fe.FixedEffect(g["p2"])]
+    r, it, cv = fe.solve_residuals(g["x"].copy(), fes, double_precision=True, maxiter=1)
+    ro, it_o, cv_o = oracle.solve_residuals(g["x"], [g["p1"], g["p2"]], maxiter=1)
+    assert (it, cv) == (it_o, cv_o)
+    assert rel_err(r, ro) < 1e-12
+
+
+def test_many_columns_tiles(fe, oracle, synth):
+    pb = synth.make(0, scale=0.005)
+    rng = np.random.default_rng(9)
+    Y = np.asfortranarray(rng.standard_normal((pb.N, 43)))
+    fes = [fe.FixedEffect.from_refs(r, n) for r, n in zip(pb.refs, pb.nlev)]
+    R_o, _, _ = oracle.solve_residuals_cols(Y, pb.refs, pb.nlev, tol=1e-8)
+    feM = fe.AbstractFixedEffectSolver(fes, None, "CUDA", np.float32)
+    R, its, cvs = feM.solve_residuals(Y.copy(), tol=1e-8)
+    feM.close()
+    assert cvs.all()
+    assert max(rel_err(R[:, j], R_o[:, j]) for j in range(43)) < REL
+
+
+def test_zipf_split_levels(fe, oracle):
+    # one level holding most observations forces multi-piece (split) levels
+    rng = np.random.default_rng(11)
+    N = 200_000
+    r1 = rng.integers(1, 20_000, N)
+    r2 = np.where(rng.random(N) < 0.7, 1, rng.integers(2, 50, N))
+    Y = np.asfortranarray(rng.standard_normal((N, 2)))
+    R_o, it_o, _ = oracle.solve_residuals_cols(Y, [r1, r2], tol=1e-8)
+    fes = [fe.FixedEffect(r1), fe.FixedEffect(r2)]
+    for prec in ("fp64", "mixed"):
+        feM = fe.AbstractFixedEffectSolver(fes, None, "CUDA", np.float64, precision=prec)
+        R, its, cvs = feM.solve_residuals(Y.copy(), tol=1e-8)
+        feM.close()
+        assert cvs.all()
+        assert max(rel_err(R[:, j], R_o[:, j]) for j in range(2)) < REL
