@@ -42,6 +42,14 @@ struct ReduceItem {
   int32_t pad;
 };
 
+// A contiguous range of [P][C] slab rows (levels of one FE and one problem)
+// streamed by one warp in the per-level epilogue.
+struct PItem {
+  int64_t rb, re;
+  int32_t fe;
+  int32_t prob;
+};
+
 // A level cut into pieces.  The last piece to finish sums all piece partials
 // in piece order (deterministic) and finalizes the level.
 struct SplitLevel {
@@ -49,8 +57,6 @@ struct SplitLevel {
   int32_t npieces;
   int32_t fe;
   int32_t level;     // FE-local level id
-  int32_t norm_slot; // slot of its norm contributions
-  int32_t pad;
 };
 
 // Device-side view of a plan (passed by value to kernels).
@@ -120,8 +126,8 @@ struct ScalarArgs {
   const double* part0;  // expand slots
   const int64_t* off0;
   int64_t S0;
-  const double* part1;  // reduce slots (||v||^2 or ||g||^2)
-  const double* part2;  // reduce slots (||x||^2)
+  const double* part1;  // P-side slots (||v||^2 or ||g||^2)
+  const double* part2;  // P-side slots (||x||^2)
   const int64_t* off1;
   int64_t S1;
   int32_t* counters;    // [0] LSMR-active instances, [1] refinement-active

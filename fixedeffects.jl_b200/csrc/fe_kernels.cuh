@@ -1,21 +1,29 @@
 // fe_kernels.cuh -- sm_100a kernels of the fixed-effects LSMR hot path.
 //
-// Every kernel here is HBM-bound integer-indexed gather/segmented-reduction
+// Every kernel here is HBM-bound integer-indexed gather / segmented-reduction
 // work; nothing is a dense contraction, so there are no tensor-core paths.
 //
 // Layout: a column tile of C right-hand sides is stored observation-major
 // ([N][C], one row per observation) and level-major ([P][C]) on the
-// coefficient side, so one warp-wide access touches C contiguous values of a
-// row.  A warp is split into G = 32/C groups of C lanes: group g handles one
-// observation (or one level-order position) at a time and lane j of the group
-// handles column j.
+// coefficient side.  Each lane owns VEC consecutive columns of a row (16-byte
+// vectors: 4 floats or 2 doubles), a row is CL = C/VEC lanes wide, and a warp
+// instruction covers G = 32/CL rows.  Lane (g, jl) handles row slot g and
+// columns jl*VEC .. jl*VEC+VEC-1.
 //
-// Determinism: no floating-point atomics anywhere.  The reduce (A'u, the
-// reference's gather!, src/SolverCPU.jl:21-27) is a segmented reduction over
-// a once-computed stable level order; each work item is summed by one warp in
-// a fixed order, long levels are cut into pieces whose partials are summed in
-// piece order by the last piece to finish, and norms are reduced per CTA into
-// fixed slots that a scalar kernel sums in slot order.
+// Three kernels make one matvec pair:
+//   k_expand  u <- f(A v, u)             (the reference's scatter!, per FE)
+//   k_segsum  S[l] = sum_{i in l} c_i u_i (the reference's gather!, per FE)
+//   k_pupdate the per-level epilogue: v <- S*scale/beta - beta v, the deferred
+//             LSMR h/hbar/x update, and the norms, streamed over levels.
+// Index vectors (refs, level-order perms and keys, interaction*sqrt(w)) are
+// read with coalesced warp-wide loads and broadcast with shuffles.
+//
+// Determinism: no floating-point atomics anywhere.  Each segsum work item is
+// summed by one warp in a fixed order; long levels are cut into pieces whose
+// partials are summed in piece order by the last piece to finish (an integer
+// atomic counter decides who is last; the sum order does not depend on it);
+// norms are reduced per CTA into fixed slots that a scalar kernel sums in
+// slot order.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -27,6 +35,67 @@ namespace fe {
 
 #define FE_FULL 0xffffffffu
 
+// ---------------------------------------------------------------------------
+// small vectors
+// ---------------------------------------------------------------------------
+template <typename T, int V>
+struct VA {
+  T v[V];
+};
+
+// Loads/stores of V contiguous elements as 16-, 8- or 4-byte accesses.  The
+// offsets used below are multiples of V, and slabs are 256-byte aligned, so
+// every access is naturally aligned.
+template <int B> struct Carrier { };
+template <> struct Carrier<16> { using type = float4; };
+template <> struct Carrier<8> { using type = float2; };
+template <> struct Carrier<4> { using type = float; };
+
+template <typename T, int V>
+struct VecIO {
+  static constexpr int kBytes = (int)sizeof(T) * V;
+  static constexpr int kChunk = kBytes >= 16 ? 16 : kBytes;
+  static constexpr int kN = kBytes / kChunk;
+  using Cr = typename Carrier<kChunk>::type;
+};
+
+template <typename T, int V>
+__device__ __forceinline__ VA<T, V> vld(const T* p) {
+  using IO = VecIO<T, V>;
+  typename IO::Cr c[IO::kN];
+#pragma unroll
+  for (int q = 0; q < IO::kN; ++q) c[q] = reinterpret_cast<const typename IO::Cr*>(p)[q];
+  VA<T, V> a;
+  memcpy(&a, c, sizeof(a));
+  return a;
+}
+template <typename T, int V>
+__device__ __forceinline__ VA<T, V> vldg(const T* p) {
+  using IO = VecIO<T, V>;
+  typename IO::Cr c[IO::kN];
+#pragma unroll
+  for (int q = 0; q < IO::kN; ++q) c[q] = __ldg(reinterpret_cast<const typename IO::Cr*>(p) + q);
+  VA<T, V> a;
+  memcpy(&a, c, sizeof(a));
+  return a;
+}
+template <typename T, int V>
+__device__ __forceinline__ void vst(T* p, const VA<T, V>& a) {
+  using IO = VecIO<T, V>;
+  typename IO::Cr c[IO::kN];
+  memcpy(c, &a, sizeof(a));
+#pragma unroll
+  for (int q = 0; q < IO::kN; ++q) reinterpret_cast<typename IO::Cr*>(p)[q] = c[q];
+}
+
+// lane shape for accumulation type TA and tile width C
+template <typename TA, int C>
+struct Shape {
+  static constexpr int VEC = sizeof(TA) == 4 ? (C >= 4 ? 4 : C) : (C >= 2 ? 2 : 1);
+  static constexpr int CL = C / VEC;  // lanes per row
+  static constexpr int G = 32 / CL;   // rows per warp instruction
+};
+
 template <typename T> __device__ __forceinline__ const T* scale_of(const FeDev& d, int k);
 template <> __device__ __forceinline__ const float* scale_of<float>(const FeDev& d, int k) { return d.scale_f[k]; }
 template <> __device__ __forceinline__ const double* scale_of<double>(const FeDev& d, int k) { return d.scale_d[k]; }
@@ -37,14 +106,20 @@ template <typename T> __device__ __forceinline__ const T* cwp_of(const FeDev& d,
 template <> __device__ __forceinline__ const float* cwp_of<float>(const FeDev& d, int k) { return d.cwp_f[k]; }
 template <> __device__ __forceinline__ const double* cwp_of<double>(const FeDev& d, int k) { return d.cwp_d[k]; }
 
-// Norm accumulators of the warps of one CTA -> one slot per CTA (fixed order).
-template <int C>
-__device__ __forceinline__ void cta_norm_to_slot(double na, double* __restrict__ part,
+// Per-column norm accumulators of one CTA -> one slot per CTA (fixed order).
+// nrm[v] is column jl*VEC+v of this lane.
+template <int C, int VEC>
+__device__ __forceinline__ void cta_norm_to_slot(const double (&nrm)[VEC], double* __restrict__ part,
                                                  int64_t S, int64_t slot, double (*sm)[32]) {
-#pragma unroll
-  for (int o = C; o < 32; o <<= 1) na += __shfl_xor_sync(FE_FULL, na, o);
+  constexpr int CL = C / VEC;
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  if (lane < C) sm[wib][lane] = na;
+#pragma unroll
+  for (int v = 0; v < VEC; ++v) {
+    double a = nrm[v];
+#pragma unroll
+    for (int o = CL; o < 32; o <<= 1) a += __shfl_xor_sync(FE_FULL, a, o);
+    if (lane < CL) sm[wib][lane * VEC + v] = a;
+  }
   __syncthreads();
   if (threadIdx.x < C && part != nullptr && slot >= 0) {
     double t = 0.0;
@@ -57,367 +132,590 @@ __device__ __forceinline__ void cta_norm_to_slot(double na, double* __restrict__
 // ---------------------------------------------------------------------------
 // Coefficient tables gathered by the expand.
 // ---------------------------------------------------------------------------
-template <typename T, typename TA>
+template <typename T, typename TA, int VEC>
 struct TabOne {
   const T* __restrict__ tab;
-  __device__ __forceinline__ TA load(int64_t off) const { return (TA)__ldg(tab + off); }
+  __device__ __forceinline__ VA<TA, VEC> load(int64_t off) const {
+    const VA<T, VEC> a = vldg<T, VEC>(tab + off);
+    VA<TA, VEC> r;
+#pragma unroll
+    for (int v = 0; v < VEC; ++v) r.v[v] = (TA)a.v[v];
+    return r;
+  }
 };
 // x64 + x32: the FP64 accumulated solution plus the FP32 correction of the
 // inner solve that just finished (the mixed-precision residual).
+template <int VEC>
 struct TabSum64 {
   const double* __restrict__ hi;
   const float* __restrict__ lo;
-  __device__ __forceinline__ double load(int64_t off) const {
-    return __ldg(hi + off) + (double)__ldg(lo + off);
+  __device__ __forceinline__ VA<double, VEC> load(int64_t off) const {
+    VA<double, VEC> a = vldg<double, VEC>(hi + off);
+    const VA<float, VEC> b = vldg<float, VEC>(lo + off);
+#pragma unroll
+    for (int v = 0; v < VEC; ++v) a.v[v] += (double)b.v[v];
+    return a;
   }
 };
 
 // ---------------------------------------------------------------------------
-// Expand epilogues: given s = (A x)[i, j] for observation i, column j.
+// Expand epilogues.  begin() loads the per-column coefficients of the lane's
+// VEC columns; pre(o) loads the observation's old values; apply() gets
+// s = (A x)[i, cols] and adds the squared new values to nrm.
 // ---------------------------------------------------------------------------
 // LSMR u-update: U <- av * (A v) + au * U   (src/utils/lsmr.jl:104 with the
-// normalisations of u and v folded into av, au).
-template <typename T>
+// normalisations of u and v folded into av, au).  Columns whose LSMR has
+// stopped keep their U.
+template <typename T, int VEC>
 struct EpiExpandLsmr {
+  using TP = T;
   T* __restrict__ U;
   const Inst* __restrict__ inst;
-  T av, au;
+  T av[VEC], au[VEC];
+  bool actv[VEC];
   bool act;
-  __device__ __forceinline__ void begin(int prob, int j, int C) {
-    const Inst& s = inst[(int64_t)prob * C + j];
-    act = s.active != 0;
-    av = (T)s.ex_av;
-    au = (T)s.ex_au;
+  __device__ __forceinline__ void begin(int prob, int jl, int C) {
+    act = false;
+#pragma unroll
+    for (int v = 0; v < VEC; ++v) {
+      const Inst& s = inst[(int64_t)prob * C + jl * VEC + v];
+      actv[v] = s.active != 0;
+      av[v] = (T)s.ex_av;
+      au[v] = (T)s.ex_au;
+      act = act || actv[v];
+    }
   }
-  __device__ __forceinline__ double apply(int64_t i, int j, int C, T s) {
-    T* p = U + i * C + j;
-    const T u = av * s + au * (*p);
-    *p = u;
-    return (double)u * (double)u;
+  __device__ __forceinline__ VA<T, VEC> pre(int64_t o) const { return vld<T, VEC>(U + o); }
+  __device__ __forceinline__ void apply(int64_t o, const VA<T, VEC>& s, const VA<T, VEC>& old,
+                                        double (&nrm)[VEC]) {
+    VA<T, VEC> u;
+#pragma unroll
+    for (int v = 0; v < VEC; ++v) {
+      u.v[v] = actv[v] ? av[v] * s.v[v] + au[v] * old.v[v] : old.v[v];
+      if (actv[v]) nrm[v] += (double)u.v[v] * (double)u.v[v];
+    }
+    vst<T, VEC>(U + o, u);
   }
 };
 
 // out <- B - (A x): initial u of LSMR and the final residual
 // (src/utils/lsmr.jl:63, src/AbstractFixedEffectSolver.jl:62).  mask: 0 all
-// instances, 2 only instances whose refinement is still running.
-template <typename TOut, typename TA>
+// instances, 2 only instances whose refinement is still running (the others
+// keep their stored residual).
+template <typename TOut, typename TA, int VEC>
 struct EpiBminusAx {
+  using TP = double;
   const double* __restrict__ B;
   TOut* __restrict__ out;
   float* __restrict__ out32;  // optional FP32 copy (mixed-precision u)
   const Inst* __restrict__ inst;
   int mask;
-  bool act;
-  __device__ __forceinline__ void begin(int prob, int j, int C) {
-    act = true;
-    if (mask == 2) act = inst[(int64_t)prob * C + j].outer_active != 0;
+  bool actv[VEC];
+  bool act, all;
+  __device__ __forceinline__ void begin(int prob, int jl, int C) {
+    act = false;
+    all = true;
+#pragma unroll
+    for (int v = 0; v < VEC; ++v) {
+      actv[v] = mask == 2 ? inst[(int64_t)prob * C + jl * VEC + v].outer_active != 0 : true;
+      act = act || actv[v];
+      all = all && actv[v];
+    }
   }
-  __device__ __forceinline__ double apply(int64_t i, int j, int C, TA s) {
-    const int64_t o = i * C + j;
-    const double r = __ldg(B + o) - (double)s;
-    out[o] = (TOut)r;
-    if (out32) out32[o] = (float)r;
-    return r * r;
+  __device__ __forceinline__ VA<double, VEC> pre(int64_t o) const { return vldg<double, VEC>(B + o); }
+  __device__ __forceinline__ void apply(int64_t o, const VA<TA, VEC>& s, const VA<double, VEC>& b,
+                                        double (&nrm)[VEC]) {
+    VA<TOut, VEC> r;
+    VA<float, VEC> r32;
+#pragma unroll
+    for (int v = 0; v < VEC; ++v) {
+      const double x = b.v[v] - (double)s.v[v];
+      r.v[v] = (TOut)x;
+      r32.v[v] = (float)x;
+      if (actv[v]) nrm[v] += x * x;
+    }
+    if (all) {
+      vst<TOut, VEC>(out + o, r);
+      if (out32) vst<float, VEC>(out32 + o, r32);
+    } else {
+#pragma unroll
+      for (int v = 0; v < VEC; ++v)
+        if (actv[v]) {
+          out[o + v] = r.v[v];
+          if (out32) out32[o + v] = r32.v[v];
+        }
+    }
   }
 };
 
 // ---------------------------------------------------------------------------
-// expand kernel: one warp per ExpandItem (a range of sorted observations).
+// k_expand: one warp per ExpandItem (a range of sorted observations); U row
+// slots per lane group per step, KB >= number of FEs (compile-time bound so
+// that every index and row load of a step can be issued before the first is
+// consumed).  The next step's refs and weights are prefetched while the
+// current step's rows are in flight.
 // ---------------------------------------------------------------------------
-template <typename TA, int C, int U, class Tab, class Epi>
+template <typename TA, int C, int U, int KB, class Tab, class Epi>
 __global__ void __launch_bounds__(kThreads)
 k_expand(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_items, Tab tab, Epi epi,
          double* __restrict__ part, int64_t S) {
-  constexpr int G = 32 / C;
+  using Sh = Shape<TA, C>;
+  constexpr int VEC = Sh::VEC, CL = Sh::CL, G = Sh::G;
+  constexpr int STEP = G * U;                     // observations per step
+  constexpr int NI = STEP >= 32 ? STEP / 32 : 1;  // index registers per lane
+  using TP = typename Epi::TP;
   __shared__ double sm[kWarps][32];
   const int lane = threadIdx.x & 31;
-  const int g = lane / C, j = lane - g * C;
+  const int g = lane / CL, jl = lane - g * CL;
   const int64_t w = (int64_t)blockIdx.x * kWarps + (threadIdx.x >> 5);
-  double nrm = 0.0;
+  double nrm[VEC];
+#pragma unroll
+  for (int v = 0; v < VEC; ++v) nrm[v] = 0.0;
   if (w < n_items) {
     const ExpandItem it = items[w];
-    epi.begin(it.prob, j, C);
-    const bool any = __any_sync(FE_FULL, epi.act);
-    if (any) {
-      for (int64_t base = it.ib; base < it.ie; base += (int64_t)G * U) {
-        TA s[U];
-        int64_t ii[U];
+    epi.begin(it.prob, jl, C);
+    if (__any_sync(FE_FULL, epi.act)) {
+      const int K = d.K;
+      int rl[KB][NI];
+      TA cl[KB][NI];
+      auto fetch = [&](int64_t base) {
+#pragma unroll
+        for (int k = 0; k < KB; ++k) {
+#pragma unroll
+          for (int r = 0; r < NI; ++r) {
+            const int64_t p = base + r * 32 + lane;
+            const bool ok = k < K && p < it.ie && (r * 32 + lane) < STEP;
+            rl[k][r] = ok ? __ldg(d.refs[k] + p) : 0;
+            const TA* __restrict__ cw = cw_of<TA>(d, k < K ? k : 0);
+            cl[k][r] = (ok && cw) ? __ldg(cw + p) : TA(1);
+          }
+        }
+      };
+      fetch(it.ib);
+      for (int64_t base = it.ib; base < it.ie; base += STEP) {
+        int rc[KB][NI];
+        TA cc[KB][NI];
+#pragma unroll
+        for (int k = 0; k < KB; ++k)
+#pragma unroll
+          for (int r = 0; r < NI; ++r) {
+            rc[k][r] = rl[k][r];
+            cc[k][r] = cl[k][r];
+          }
+        if (base + STEP < it.ie) fetch(base + STEP);
+        VA<TP, VEC> old[U];
+        VA<TA, VEC> s[U];
 #pragma unroll
         for (int u = 0; u < U; ++u) {
-          ii[u] = base + u * G + g;
-          s[u] = TA(0);
+          const int64_t i = base + u * G + g;
+#pragma unroll
+          for (int v = 0; v < VEC; ++v) s[u].v[v] = TA(0);
+          if (i < it.ie && epi.act) old[u] = epi.pre(i * C + jl * VEC);
         }
 #pragma unroll
-        for (int k = 0; k < kMaxFE; ++k) {
-          if (k >= d.K) break;
-          const int32_t* __restrict__ refs = d.refs[k];
-          const TA* __restrict__ sc = scale_of<TA>(d, k);
-          const TA* __restrict__ cw = cw_of<TA>(d, k);
-          const int64_t lb = d.lev_base[k];
+        for (int k = 0; k < KB; ++k) {
+          if (k < K) {
+            const TA* __restrict__ sc = scale_of<TA>(d, k);
+            const int64_t lb = d.lev_base[k];
 #pragma unroll
-          for (int u = 0; u < U; ++u) {
-            if (ii[u] < it.ie && epi.act) {
-              const int r = __ldg(refs + ii[u]);
-              TA c = __ldg(sc + r);
-              if (cw) c *= __ldg(cw + ii[u]);
-              s[u] += c * tab.load((lb + r) * C + j);
+            for (int u = 0; u < U; ++u) {
+              const int q = u * G;  // + g: the same index register (G divides 32)
+              const int ref = __shfl_sync(FE_FULL, rc[k][q >> 5], (q & 31) + g);
+              const TA c = __shfl_sync(FE_FULL, cc[k][q >> 5], (q & 31) + g);
+              const int64_t i = base + u * G + g;
+              if (i < it.ie && epi.act) {
+                const TA cs = c * __ldg(sc + ref);
+                const VA<TA, VEC> t = tab.load((lb + ref) * C + jl * VEC);
+#pragma unroll
+                for (int v = 0; v < VEC; ++v) s[u].v[v] += cs * t.v[v];
+              }
             }
           }
         }
 #pragma unroll
-        for (int u = 0; u < U; ++u)
-          if (ii[u] < it.ie && epi.act) nrm += epi.apply(ii[u], j, C, s[u]);
+        for (int u = 0; u < U; ++u) {
+          const int64_t i = base + u * G + g;
+          if (i < it.ie && epi.act) epi.apply(i * C + jl * VEC, s[u], old[u], nrm);
+        }
       }
     }
   }
-  cta_norm_to_slot<C>(nrm, part, S, (int64_t)blockIdx.x, sm);
+  cta_norm_to_slot<C, VEC>(nrm, part, S, (int64_t)blockIdx.x, sm);
 }
 
 // ---------------------------------------------------------------------------
-// Reduce value loaders: the per-position term summed into a level.
+// Segmented-sum value loaders: the per-position vector summed into a level.
 // ---------------------------------------------------------------------------
-template <typename TIn, typename TA>
+template <typename TIn, typename TA, int VEC>
 struct LoadIn {
   const TIn* __restrict__ in;
-  __device__ __forceinline__ TA load(int64_t p, int64_t i, int j, int C,
-                                     const TA* __restrict__ cwp) const {
-    const TA v = (TA)in[i * C + j];
-    return cwp ? __ldg(cwp + p) * v : v;
+  static constexpr bool kSquareWeight = false;
+  __device__ __forceinline__ VA<TA, VEC> load(int64_t off) const {
+    const VA<TIn, VEC> a = vld<TIn, VEC>(in + off);
+    VA<TA, VEC> r;
+#pragma unroll
+    for (int v = 0; v < VEC; ++v) r.v[v] = (TA)a.v[v];
+    return r;
   }
 };
-// sum of interaction^2 * w for the Jacobi scale (src/SolverCPU.jl:78-89)
+// sum of interaction^2 * w for the Jacobi scale (src/SolverCPU.jl:78-89):
+// the per-position weight cw = interaction*sqrt(w) enters squared, the value
+// is 1.  C = 1.
 struct LoadScaleSq {
-  __device__ __forceinline__ double load(int64_t p, int64_t, int, int,
-                                         const double* __restrict__ cwp) const {
-    if (cwp) {
-      const double c = __ldg(cwp + p);
-      return c * c;
-    }
-    return 1.0;
+  static constexpr bool kSquareWeight = true;
+  __device__ __forceinline__ VA<double, 1> load(int64_t) const {
+    VA<double, 1> r;
+    r.v[0] = 1.0;
+    return r;
   }
 };
 
 // ---------------------------------------------------------------------------
-// Reduce epilogues: finalize(level l of FE k, column j, acc = sum over level).
+// k_segsum: one warp per ReduceItem.  Positions are visited in level order,
+// G per warp instruction (one per lane group); an inclusive segmented scan
+// over the groups (keys are sorted inside an item, so equal keys are
+// contiguous) plus a carry across steps yields each level's sum, stored to
+// Sout[level] by the group holding the level's last position.  Split pieces
+// hand their partial to the last piece of the level.
 // ---------------------------------------------------------------------------
-// LSMR v-update fused with the deferred h/hbar/x update of the previous
-// iteration (src/utils/lsmr.jl:108-110 and :138-142) and the norms ||v||^2,
-// ||x||^2.
-template <typename T>
-struct EpiReduceLsmr {
+template <typename TA, int C, int U, class Load>
+__global__ void __launch_bounds__(kThreads)
+k_segsum(const FeDev d, const ReduceItem* __restrict__ items, int64_t n_items, Load ld,
+         TA* __restrict__ Sout, const SplitLevel* __restrict__ splits,
+         double* __restrict__ piece_part, int64_t n_pieces, int32_t* __restrict__ split_cnt) {
+  using Sh = Shape<TA, C>;
+  constexpr int VEC = Sh::VEC, CL = Sh::CL, G = Sh::G;
+  constexpr int STEP = G * U;
+  constexpr int NI = STEP >= 32 ? STEP / 32 : 1;
+  __shared__ double smt[kWarps][32];
+  const int lane = threadIdx.x & 31;
+  const int g = lane / CL, jl = lane - g * CL;
+  const int64_t w = (int64_t)blockIdx.x * kWarps + (threadIdx.x >> 5);
+  if (w >= n_items) return;
+  const ReduceItem it = items[w];
+  if (it.pe <= it.pb) return;
+  const int k = it.fe;
+  const int32_t* __restrict__ perm = d.perm[k];
+  const int32_t* __restrict__ key = d.key[k];
+  const TA* __restrict__ cwp = cwp_of<TA>(d, k);
+  TA* __restrict__ Sk = Sout + d.lev_base[k] * C + jl * VEC;
+  int ckey = -1;
+  VA<TA, VEC> carry;
+#pragma unroll
+  for (int v = 0; v < VEC; ++v) carry.v[v] = TA(0);
+  for (int64_t base = it.pb; base < it.pe; base += STEP) {
+    int kl[NI];
+    int il[NI];
+    TA cl[NI];
+#pragma unroll
+    for (int r = 0; r < NI; ++r) {
+      const int64_t p = base + r * 32 + lane;
+      const bool ok = p < it.pe && (r * 32 + lane) < STEP;
+      kl[r] = ok ? __ldg(key + p) : kSentinel;
+      il[r] = ok ? (perm ? __ldg(perm + p) : (int)p) : 0;
+      TA c = TA(1);
+      if (ok && cwp) c = __ldg(cwp + p);
+      if (Load::kSquareWeight) c = c * c;
+      cl[r] = c;
+    }
+    VA<TA, VEC> val[U];
+    int kk[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int q = u * G;
+      const int src = (q & 31) + g;
+      kk[u] = __shfl_sync(FE_FULL, kl[q >> 5], src);
+      const int i = __shfl_sync(FE_FULL, il[q >> 5], src);
+      const TA c = __shfl_sync(FE_FULL, cl[q >> 5], src);
+      if (kk[u] != kSentinel) {
+        val[u] = ld.load((int64_t)i * C + jl * VEC);
+#pragma unroll
+        for (int v = 0; v < VEC; ++v) val[u].v[v] *= c;
+      } else {
+#pragma unroll
+        for (int v = 0; v < VEC; ++v) val[u].v[v] = TA(0);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int64_t b0 = base + (int64_t)u * G;
+      if (b0 >= it.pe) break;  // warp-uniform
+      const int nvalid = (int)((it.pe - b0) < G ? (it.pe - b0) : G);
+      const int k0 = __shfl_sync(FE_FULL, kk[u], jl);
+      if (ckey >= 0 && ckey != k0) {
+        if (g == 0) vst<TA, VEC>(Sk + (int64_t)ckey * C, carry);
+        ckey = -1;
+#pragma unroll
+        for (int v = 0; v < VEC; ++v) carry.v[v] = TA(0);
+      }
+      VA<TA, VEC> x = val[u];
+      const int km = kk[u];
+#pragma unroll
+      for (int dd = 1; dd < G; dd <<= 1) {
+        const int ko = __shfl_up_sync(FE_FULL, km, dd * CL);
+        const bool take = g >= dd && ko == km;
+#pragma unroll
+        for (int v = 0; v < VEC; ++v) {
+          const TA xo = __shfl_up_sync(FE_FULL, x.v[v], dd * CL);
+          if (take) x.v[v] += xo;
+        }
+      }
+      if (km == ckey) {
+#pragma unroll
+        for (int v = 0; v < VEC; ++v) x.v[v] += carry.v[v];
+      }
+      const int kn = __shfl_down_sync(FE_FULL, km, CL);
+      if (g < nvalid - 1 && kn != km) vst<TA, VEC>(Sk + (int64_t)km * C, x);
+      const int srcl = (nvalid - 1) * CL + jl;
+      ckey = __shfl_sync(FE_FULL, km, srcl);
+#pragma unroll
+      for (int v = 0; v < VEC; ++v) carry.v[v] = __shfl_sync(FE_FULL, x.v[v], srcl);
+    }
+  }
+  if (ckey < 0) return;
+  if (it.split < 0) {
+    if (g == 0) vst<TA, VEC>(Sk + (int64_t)ckey * C, carry);
+    return;
+  }
+  // split level: piece partials are stored column-major [C][n_pieces]
+  const SplitLevel sl = splits[it.split];
+  if (g == 0) {
+#pragma unroll
+    for (int v = 0; v < VEC; ++v)
+      piece_part[(int64_t)(jl * VEC + v) * n_pieces + sl.first_piece + it.pad] = (double)carry.v[v];
+  }
+  __threadfence();
+  __syncwarp();
+  int last = 0;
+  if (lane == 0) last = (atomicAdd(split_cnt + it.split, 1) == sl.npieces - 1) ? 1 : 0;
+  last = __shfl_sync(FE_FULL, last, 0);
+  if (!last) return;
+  __threadfence();
+  // all 32 lanes sum the pieces of each column in a fixed order
+  const int wib = threadIdx.x >> 5;
+  for (int jj = 0; jj < C; ++jj) {
+    const double* pp = piece_part + (int64_t)jj * n_pieces + sl.first_piece;
+    double acc = 0.0;
+    for (int q = lane; q < sl.npieces; q += 32) acc += __ldcg(pp + q);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(FE_FULL, acc, o);
+    if (lane == 0) smt[wib][jj] = acc;
+  }
+  __syncwarp();
+  if (g == 0) {
+    VA<TA, VEC> tot;
+#pragma unroll
+    for (int v = 0; v < VEC; ++v) tot.v[v] = (TA)smt[wib][jl * VEC + v];
+    vst<TA, VEC>(Sk + (int64_t)ckey * C, tot);
+  }
+  if (lane == 0) split_cnt[it.split] = 0;
+}
+
+// ---------------------------------------------------------------------------
+// P-side epilogues: update(k, lrow, o, sum, na, nb) for level lrow of FE k;
+// o is the element offset of the lane's first column.
+// ---------------------------------------------------------------------------
+// LSMR v-update (src/utils/lsmr.jl:108-110) fused with the deferred h/hbar/x
+// update of the previous iteration (lsmr.jl:138-142) and the norms ||v||^2,
+// ||x||^2.  Columns whose LSMR has stopped are left untouched.  The
+// elementwise arithmetic runs in T (the coefficients come from the FP64
+// scalar recurrences, rounded once); the norms accumulate in FP64.
+template <typename T, int VEC>
+struct PEpiLsmr {
+  using TS = T;
   T* __restrict__ V;
   T* __restrict__ H;
   T* __restrict__ Hb;
   T* __restrict__ X;
   const Inst* __restrict__ inst;
-  double rd_acc, rd_v, s_v, c1, c2, c3;
-  int upd_mode;
-  bool do_v, act;
-  __device__ __forceinline__ void begin(int prob, int j, int C) {
-    const Inst& s = inst[(int64_t)prob * C + j];
-    act = s.active != 0;
-    rd_acc = s.rd_acc;
-    rd_v = s.rd_v;
-    s_v = s.s_v;
-    c1 = s.c1;
-    c2 = s.c2;
-    c3 = s.c3;
-    upd_mode = s.upd_mode;
-    do_v = s.do_v != 0;
+  T rd_acc[VEC], rd_v[VEC], s_v[VEC], c1[VEC], c2[VEC], c3[VEC];
+  uint32_t upd_bits;  // 2 bits per column: deferred update mode
+  uint32_t v_bits;    // 1 bit per column: v is updated this iteration
+  bool act;
+  __device__ __forceinline__ void begin(int prob, int jl, int C) {
+    act = false;
+    upd_bits = 0;
+    v_bits = 0;
+#pragma unroll
+    for (int v = 0; v < VEC; ++v) {
+      const Inst& s = inst[(int64_t)prob * C + jl * VEC + v];
+      const bool a = s.active != 0;
+      rd_acc[v] = (T)s.rd_acc;
+      rd_v[v] = (T)s.rd_v;
+      s_v[v] = (T)s.s_v;
+      c1[v] = (T)s.c1;
+      c2[v] = (T)s.c2;
+      c3[v] = (T)s.c3;
+      if (a) upd_bits |= (uint32_t)(s.upd_mode & 3) << (2 * v);
+      if (a && s.do_v) v_bits |= 1u << v;
+      act = act || a;
+    }
   }
-  __device__ __forceinline__ void finalize(const FeDev& d, int k, int l, int j, int C, double acc,
-                                           double& na, double& nb) {
-    if (!act) return;
-    const int64_t idx = (d.lev_base[k] + l) * C + j;
-    const double vold = (double)V[idx];
-    if (upd_mode != 0) {
-      const double vo = s_v * vold;
-      double x;
-      if (upd_mode == 2) {
-        const double h = (double)H[idx];
-        const double hb = h + c1 * (double)Hb[idx];
-        x = (double)X[idx] + c2 * hb;
-        Hb[idx] = (T)hb;
-        X[idx] = (T)x;
-        H[idx] = (T)(vo + c3 * h);
-      } else {
-        H[idx] = (T)vo;
-        Hb[idx] = (T)0;
-        if (upd_mode == 3) {
-          X[idx] = (T)0;
-          x = 0.0;
-        } else {
-          x = (double)X[idx];
+  __device__ __forceinline__ void update(const FeDev& d, int k, int64_t l, int64_t o,
+                                         const VA<T, VEC>& sum, double (&na)[VEC],
+                                         double (&nb)[VEC]) {
+    VA<T, VEC> vv = vld<T, VEC>(V + o);
+    if (upd_bits) {
+      VA<T, VEC> hh = vld<T, VEC>(H + o);
+      VA<T, VEC> hb = vld<T, VEC>(Hb + o);
+      VA<T, VEC> xx = vld<T, VEC>(X + o);
+#pragma unroll
+      for (int v = 0; v < VEC; ++v) {
+        const uint32_t m = (upd_bits >> (2 * v)) & 3u;
+        const T vo = s_v[v] * vv.v[v];
+        if (m == 2) {
+          const T h = hh.v[v];
+          const T hbn = h + c1[v] * hb.v[v];
+          hb.v[v] = hbn;
+          xx.v[v] = xx.v[v] + c2[v] * hbn;
+          hh.v[v] = vo + c3[v] * h;
+        } else if (m != 0) {
+          hh.v[v] = vo;
+          hb.v[v] = T(0);
+          if (m == 3) xx.v[v] = T(0);
+        }
+        if (m != 0) nb[v] += (double)xx.v[v] * (double)xx.v[v];
+      }
+      vst<T, VEC>(H + o, hh);
+      vst<T, VEC>(Hb + o, hb);
+      vst<T, VEC>(X + o, xx);
+    }
+    if (v_bits) {
+      const T sc = __ldg(scale_of<T>(d, k) + l);
+#pragma unroll
+      for (int v = 0; v < VEC; ++v) {
+        if ((v_bits >> v) & 1u) {
+          const T vn = sum.v[v] * sc * rd_acc[v] - rd_v[v] * vv.v[v];
+          vv.v[v] = vn;
+          na[v] += (double)vn * (double)vn;
         }
       }
-      const double xr = (double)(T)x;
-      nb += xr * xr;
-    }
-    if (do_v) {
-      const double sc = (double)__ldg(scale_of<T>(d, k) + l);
-      const T vn = (T)(acc * sc * rd_acc - rd_v * vold);
-      V[idx] = vn;
-      na += (double)vn * (double)vn;
+      vst<T, VEC>(V + o, vv);
     }
   }
 };
 
 // x <- A'b (the warm start of src/AbstractFixedEffectSolver.jl:56).
-template <typename TOut>
-struct EpiStoreX {
+template <typename TOut, int VEC>
+struct PEpiStoreX {
+  using TS = double;
   TOut* __restrict__ X;
   bool act;
   __device__ __forceinline__ void begin(int, int, int) { act = true; }
-  __device__ __forceinline__ void finalize(const FeDev& d, int k, int l, int j, int C, double acc,
-                                           double&, double&) {
-    const int64_t idx = (d.lev_base[k] + l) * C + j;
-    X[idx] = (TOut)(acc * __ldg(d.scale_d[k] + l));
+  __device__ __forceinline__ void update(const FeDev& d, int k, int64_t l, int64_t o,
+                                         const VA<double, VEC>& sum, double (&)[VEC],
+                                         double (&)[VEC]) {
+    const double sc = __ldg(d.scale_d[k] + l);
+    VA<TOut, VEC> x;
+#pragma unroll
+    for (int v = 0; v < VEC; ++v) x.v[v] = (TOut)(sum.v[v] * sc);
+    vst<TOut, VEC>(X + o, x);
   }
 };
 
 // Mixed precision: g = A'r computed in FP64 from the FP64 residual, stored as
 // the FP32 starting v of the next inner solve; x64 += x32 and ||x64||^2.
-struct EpiGrad64 {
+template <int VEC>
+struct PEpiGrad64 {
+  using TS = double;
   float* __restrict__ V32;
   double* __restrict__ X64;
   const float* __restrict__ X32;
   const Inst* __restrict__ inst;
+  bool actv[VEC];
   bool act;
-  __device__ __forceinline__ void begin(int prob, int j, int C) {
-    act = inst[(int64_t)prob * C + j].outer_active != 0;
+  __device__ __forceinline__ void begin(int prob, int jl, int C) {
+    act = false;
+#pragma unroll
+    for (int v = 0; v < VEC; ++v) {
+      actv[v] = inst[(int64_t)prob * C + jl * VEC + v].outer_active != 0;
+      act = act || actv[v];
+    }
   }
-  __device__ __forceinline__ void finalize(const FeDev& d, int k, int l, int j, int C, double acc,
-                                           double& na, double& nb) {
-    if (!act) return;
-    const int64_t idx = (d.lev_base[k] + l) * C + j;
-    const double g = acc * __ldg(d.scale_d[k] + l);
-    V32[idx] = (float)g;
-    na += g * g;
-    const double x = X64[idx] + (double)X32[idx];
-    X64[idx] = x;
-    nb += x * x;
+  __device__ __forceinline__ void update(const FeDev& d, int k, int64_t l, int64_t o,
+                                         const VA<double, VEC>& sum, double (&na)[VEC],
+                                         double (&nb)[VEC]) {
+    const double sc = __ldg(d.scale_d[k] + l);
+    VA<float, VEC> g32 = vld<float, VEC>(V32 + o);
+    VA<double, VEC> x64 = vld<double, VEC>(X64 + o);
+    const VA<float, VEC> x32 = vld<float, VEC>(X32 + o);
+#pragma unroll
+    for (int v = 0; v < VEC; ++v) {
+      if (!actv[v]) continue;
+      const double gv = sum.v[v] * sc;
+      g32.v[v] = (float)gv;
+      na[v] += gv * gv;
+      const double x = x64.v[v] + (double)x32.v[v];
+      x64.v[v] = x;
+      nb[v] += x * x;
+    }
+    vst<float, VEC>(V32 + o, g32);
+    vst<double, VEC>(X64 + o, x64);
   }
 };
 
 // Jacobi scale: 1/sqrt(sum interaction^2 w), or 0 for an empty sum
-// (src/SolverCPU.jl:84-88, issue #97 of the reference).
-struct EpiScale {
+// (src/SolverCPU.jl:84-88, issue #97 of the reference).  C = 1.
+struct PEpiScale {
+  using TS = double;
   double* sd[kMaxFE];
   float* sf[kMaxFE];
   bool act;
   __device__ __forceinline__ void begin(int, int, int) { act = true; }
-  __device__ __forceinline__ void finalize(const FeDev&, int k, int l, int, int, double acc,
-                                           double&, double&) {
-    const double s = acc > 0 ? 1.0 / sqrt(acc) : 0.0;
+  __device__ __forceinline__ void update(const FeDev&, int k, int64_t l, int64_t,
+                                         const VA<double, 1>& sum, double (&)[1], double (&)[1]) {
+    const double s = sum.v[0] > 0 ? 1.0 / sqrt(sum.v[0]) : 0.0;
     sd[k][l] = s;
     sf[k][l] = (float)s;
   }
 };
 
 // ---------------------------------------------------------------------------
-// reduce kernel: one warp per ReduceItem.  Positions are visited in level
-// order in batches of G (one per lane group); an inclusive segmented scan over
-// the groups (keys are sorted inside an item, so equal keys are contiguous)
-// plus a carry across batches yields each level's sum; the group holding a
-// level's last position finalizes it.
+// k_pupdate: one warp per PItem (a range of slab rows of one FE and problem),
+// streaming.  Norms go to one slot per CTA.
 // ---------------------------------------------------------------------------
-template <typename TA, int C, int U, class Load, class Epi>
+template <int C, int U, class Epi>
 __global__ void __launch_bounds__(kThreads)
-k_reduce(const FeDev d, const ReduceItem* __restrict__ items, int64_t n_items, Load ld, Epi epi,
-         const SplitLevel* __restrict__ splits, double* __restrict__ piece_part,
-         int32_t* __restrict__ split_cnt, double* __restrict__ part_a, double* __restrict__ part_b,
-         int64_t S, const int32_t* __restrict__ cta_slot) {
-  constexpr int G = 32 / C;
+k_pupdate(const FeDev d, const PItem* __restrict__ items, int64_t n_items,
+          const typename Epi::TS* __restrict__ Sin, Epi epi, double* __restrict__ part_a,
+          double* __restrict__ part_b, int64_t S) {
+  using TS = typename Epi::TS;
+  using Sh = Shape<TS, C>;
+  constexpr int VEC = Sh::VEC, CL = Sh::CL, G = Sh::G;
   __shared__ double sm[kWarps][32];
   const int lane = threadIdx.x & 31;
-  const int g = lane / C, j = lane - g * C;
+  const int g = lane / CL, jl = lane - g * CL;
   const int64_t w = (int64_t)blockIdx.x * kWarps + (threadIdx.x >> 5);
-  double na = 0.0, nb = 0.0;
+  double na[VEC], nb[VEC];
+#pragma unroll
+  for (int v = 0; v < VEC; ++v) {
+    na[v] = 0.0;
+    nb[v] = 0.0;
+  }
   if (w < n_items) {
-    const ReduceItem it = items[w];
-    epi.begin(it.prob, j, C);
-    const bool any = __any_sync(FE_FULL, epi.act);
-    if (any && it.pe > it.pb) {
+    const PItem it = items[w];
+    epi.begin(it.prob, jl, C);
+    if (__any_sync(FE_FULL, epi.act)) {
       const int k = it.fe;
-      const int32_t* __restrict__ perm = d.perm[k];
-      const int32_t* __restrict__ key = d.key[k];
-      const TA* __restrict__ cwp = cwp_of<TA>(d, k);
-      int ckey = -1;
-      TA carry = TA(0);
-      for (int64_t base = it.pb; base < it.pe; base += (int64_t)G * U) {
-        int kk[U];
-        TA val[U];
+      const int64_t lb = d.lev_base[k];
+      for (int64_t base = it.rb; base < it.re; base += (int64_t)G * U) {
+        VA<TS, VEC> sv[U];
 #pragma unroll
         for (int u = 0; u < U; ++u) {
-          const int64_t p = base + u * G + g;
-          if (p < it.pe) {
-            kk[u] = __ldg(key + p);
-            const int64_t i = perm ? (int64_t)__ldg(perm + p) : p;
-            val[u] = epi.act ? ld.load(p, i, j, C, cwp) : TA(0);
-          } else {
-            kk[u] = kSentinel;
-            val[u] = TA(0);
-          }
+          const int64_t row = base + u * G + g;
+          if (row < it.re) sv[u] = vld<TS, VEC>(Sin + row * C + jl * VEC);
         }
 #pragma unroll
         for (int u = 0; u < U; ++u) {
-          const int64_t b0 = base + (int64_t)u * G;
-          if (b0 >= it.pe) break;  // warp-uniform
-          const int nvalid = (int)((it.pe - b0) < G ? (it.pe - b0) : G);
-          const int k0 = __shfl_sync(FE_FULL, kk[u], j);
-          if (ckey >= 0 && ckey != k0) {
-            if (g == 0) epi.finalize(d, k, ckey, j, C, (double)carry, na, nb);
-            ckey = -1;
-            carry = TA(0);
-          }
-          TA v = val[u];
-          const int km = kk[u];
-#pragma unroll
-          for (int dd = 1; dd < G; dd <<= 1) {
-            const TA vo = __shfl_up_sync(FE_FULL, v, dd * C);
-            const int ko = __shfl_up_sync(FE_FULL, km, dd * C);
-            if (g >= dd && ko == km) v += vo;
-          }
-          if (km == ckey) v += carry;
-          const int kn = __shfl_down_sync(FE_FULL, km, C);
-          if (g < nvalid - 1 && kn != km) epi.finalize(d, k, km, j, C, (double)v, na, nb);
-          const int src = (nvalid - 1) * C + j;
-          ckey = __shfl_sync(FE_FULL, km, src);
-          carry = __shfl_sync(FE_FULL, v, src);
-        }
-      }
-      if (ckey >= 0) {
-        if (it.split < 0) {
-          if (g == 0) epi.finalize(d, k, ckey, j, C, (double)carry, na, nb);
-        } else {
-          const SplitLevel sl = splits[it.split];
-          if (g == 0) piece_part[(int64_t)(sl.first_piece + it.pad) * C + j] = (double)carry;
-          __threadfence();
-          __syncwarp();
-          int last = 0;
-          if (lane == 0) last = (atomicAdd(split_cnt + it.split, 1) == sl.npieces - 1) ? 1 : 0;
-          last = __shfl_sync(FE_FULL, last, 0);
-          if (last) {
-            __threadfence();
-            if (g == 0) {
-              double tot = 0.0;
-              for (int q = 0; q < sl.npieces; ++q)
-                tot += __ldcg(piece_part + (int64_t)(sl.first_piece + q) * C + j);
-              double sa = 0.0, sb = 0.0;
-              epi.finalize(d, k, ckey, j, C, tot, sa, sb);
-              if (part_a) part_a[(int64_t)j * S + sl.norm_slot] = sa;
-              if (part_b) part_b[(int64_t)j * S + sl.norm_slot] = sb;
-            }
-            if (lane == 0) split_cnt[it.split] = 0;
-          }
+          const int64_t row = base + u * G + g;
+          if (row < it.re && epi.act) epi.update(d, k, row - lb, row * C + jl * VEC, sv[u], na, nb);
         }
       }
     }
   }
-  const int64_t slot = cta_slot ? (int64_t)cta_slot[blockIdx.x] : -1;
-  cta_norm_to_slot<C>(na, part_a, S, slot, sm);
+  cta_norm_to_slot<C, VEC>(na, part_a, S, (int64_t)blockIdx.x, sm);
   __syncthreads();
-  cta_norm_to_slot<C>(nb, part_b, S, slot, sm);
+  cta_norm_to_slot<C, VEC>(nb, part_b, S, (int64_t)blockIdx.x, sm);
 }
 
 }  // namespace fe

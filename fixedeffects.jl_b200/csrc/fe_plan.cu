@@ -49,9 +49,9 @@ int DevBuf::ensure(size_t n) {
 
 template <typename T>
 static int upload(DevBuf& b, const T* src, size_t n, cudaStream_t s) {
-  int st = b.ensure(n * sizeof(T));
+  int st = b.ensure((n > 0 ? n : 1) * sizeof(T));
   if (st) return st;
-  if (n) FE_CK(cudaMemcpyAsync(b.p, src, n * sizeof(T), cudaMemcpyHostToDevice, s));
+  if (n > 0 && src) FE_CK(cudaMemcpyAsync(b.p, src, n * sizeof(T), cudaMemcpyHostToDevice, s));
   return 0;
 }
 
@@ -253,8 +253,8 @@ int plan_build(fe_plan* pl, int32_t nprob, const int64_t* n_obs, int32_t K,
     for (int64_t l = 0; l < pl->nlev[k]; ++l)
       for (int64_t q = off[(size_t)l]; q < off[(size_t)l + 1]; ++q) keyv[(size_t)q] = (int32_t)l;
     st = upload(pl->d_refs[k], rs.data(), (size_t)N, s);
-    if (!st) st = upload(pl->d_key[k], keyv.data(), (size_t)std::max<int64_t>(npos, 1), s);
-    if (!st && !ident) st = upload(pl->d_perm[k], perm.data(), (size_t)std::max<int64_t>(npos, 1), s);
+    if (!st) st = upload(pl->d_key[k], keyv.data(), (size_t)npos, s);
+    if (!st && !ident) st = upload(pl->d_perm[k], perm.data(), (size_t)npos, s);
     if (st) return st;
     FE_CK(cudaStreamSynchronize(s));  // host vectors are reused
   }
@@ -359,25 +359,34 @@ int plan_update_weights(fe_plan* pl, const double* weights) {
   ItemSet* its = nullptr;
   int st = plan_items(pl, 1, &its);
   if (st) return st;
+  FeDev dd = d;
+  dd.C = 1;
+  DevBuf sums, piece;
+  st = sums.ensure((size_t)std::max<int64_t>(pl->P, 1) * 8);
+  if (!st) st = piece.ensure((size_t)std::max<int64_t>(its->n_pieces, 1) * 8);
+  if (st) return st;
+  FE_CK(cudaMemsetAsync(sums.p, 0, (size_t)std::max<int64_t>(pl->P, 1) * 8, s));
   if (!its->rd.empty()) {
-    EpiScale epi;
+    const unsigned grid = (unsigned)((its->rd.size() + kWarps - 1) / kWarps);
+    k_segsum<double, 1, 8, LoadScaleSq><<<grid, kThreads, 0, s>>>(
+        dd, its->d_rd.as<ReduceItem>(), (int64_t)its->rd.size(), LoadScaleSq{}, sums.as<double>(),
+        its->d_splits.as<SplitLevel>(), piece.as<double>(), its->n_pieces,
+        its->d_split_cnt.as<int32_t>());
+    FE_CK(cudaGetLastError());
+  }
+  if (!its->pu.empty()) {
+    PEpiScale epi;
     for (int k = 0; k < kMaxFE; ++k) {
       epi.sd[k] = k < K ? pl->d_scale_d[k].as<double>() : nullptr;
       epi.sf[k] = k < K ? pl->d_scale_f[k].as<float>() : nullptr;
     }
-    DevBuf piece;
-    st = piece.ensure((size_t)std::max<int64_t>(its->n_pieces, 1) * 8);
-    if (st) return st;
-    FeDev dd = d;
-    dd.C = 1;
-    const unsigned grid = (unsigned)((its->rd.size() + kWarps - 1) / kWarps);
-    k_reduce<double, 1, 4, LoadScaleSq, EpiScale><<<grid, kThreads, 0, s>>>(
-        dd, its->d_rd.as<ReduceItem>(), (int64_t)its->rd.size(), LoadScaleSq{}, epi,
-        its->d_splits.as<SplitLevel>(), piece.as<double>(), its->d_split_cnt.as<int32_t>(), nullptr,
-        nullptr, 0, nullptr);
+    const unsigned grid = (unsigned)(its->pu.size() / kWarps);
+    k_pupdate<1, 4, PEpiScale><<<grid, kThreads, 0, s>>>(dd, its->d_pu.as<PItem>(),
+                                                           (int64_t)its->pu.size(), sums.as<double>(),
+                                                           epi, nullptr, nullptr, 0);
     FE_CK(cudaGetLastError());
-    FE_CK(cudaStreamSynchronize(s));
   }
+  FE_CK(cudaStreamSynchronize(s));
   return 0;
 }
 
@@ -394,28 +403,33 @@ int plan_items(fe_plan* pl, int C, ItemSet** out) {
   }
   std::unique_ptr<ItemSet> its(new ItemSet());
   its->C = C;
-  const int G = 32 / C;
-  const int U = 4;
-  const int64_t batch = (int64_t)G * U;
   int sms = 148;
   {
-    int dev = pl->device, v = 0;
-    if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess && v > 0) sms = v;
+    int v = 0;
+    if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, pl->device) == cudaSuccess && v > 0)
+      sms = v;
   }
+  // about 4 waves of resident warps; rows per item a multiple of 32
   const int64_t warps_target = (int64_t)sms * 64 * 4;
-  const int64_t cap = std::max<int64_t>(batch, 16384 / C);
-  const int64_t Te = std::min(cap, std::max(batch, round_up((pl->N + warps_target - 1) / warps_target, batch)));
+  const int64_t cap = std::max<int64_t>(32, 16384 / C);
+  auto item_size = [&](int64_t total) {
+    return std::min(cap, std::max<int64_t>(32, round_up((total + warps_target - 1) / warps_target, 32)));
+  };
+  const int64_t Te = item_size(pl->N);
   int64_t total_pos = 0;
   for (int k = 0; k < pl->K; ++k) total_pos += pl->seg_len[k];
-  const int64_t Tr = std::min(cap, std::max(batch, round_up((total_pos + warps_target - 1) / warps_target, batch)));
+  const int64_t Tr = item_size(total_pos);
+  int64_t total_rows = 0;
+  for (int k = 0; k < pl->K; ++k) total_rows += pl->nlev[k];
+  const int64_t Tp = item_size(total_rows);
 
   const int nprob = pl->nprob;
   const int K = pl->K;
   its->ex_slot_off.assign((size_t)nprob + 1, 0);
-  its->rd_slot_off.assign((size_t)nprob + 1, 0);
-  int64_t slot = 0;
+  its->pu_slot_off.assign((size_t)nprob + 1, 0);
   for (int p = 0; p < nprob; ++p) {
-    // expand items: chunks of the problem's sorted observation range
+    // expand items: chunks of the problem's sorted observation range, padded
+    // so that every CTA belongs to one problem (its norm slot is per problem)
     const int64_t o0 = pl->prob_obs_off[p], o1 = pl->prob_obs_off[p + 1];
     const size_t e0 = its->ex.size();
     for (int64_t b = o0; b < o1; b += Te) its->ex.push_back({b, std::min(o1, b + Te), p, 0});
@@ -423,12 +437,19 @@ int plan_items(fe_plan* pl, int C, ItemSet** out) {
     if (its->ex.size() == e0)
       for (int w = 0; w < kWarps; ++w) its->ex.push_back({o1, o1, p, 0});
     its->ex_slot_off[p + 1] = (int64_t)(its->ex.size() / kWarps);
-  }
-  // reduce items, CTA slots and split levels (slots of a problem contiguous)
-  std::vector<int32_t> split_of_problem_count(nprob, 0);
-  for (int p = 0; p < nprob; ++p) {
-    const size_t r0 = its->rd.size();
-    std::vector<int32_t> splits_here;
+    // P-side items: chunks of the problem's slab rows, per FE, padded likewise
+    const size_t q0 = its->pu.size();
+    for (int k = 0; k < K; ++k) {
+      const int64_t rb = pl->lev_base[k] + pl->prob_lev_off[(size_t)p * K + k];
+      const int64_t re = pl->lev_base[k] + pl->prob_lev_off[(size_t)(p + 1) * K + k];
+      for (int64_t b = rb; b < re; b += Tp) its->pu.push_back({b, std::min(re, b + Tp), k, p});
+    }
+    while ((its->pu.size() - q0) % kWarps) its->pu.push_back({0, 0, 0, p});
+    if (its->pu.size() == q0)
+      for (int w = 0; w < kWarps; ++w) its->pu.push_back({0, 0, 0, p});
+    its->pu_slot_off[p + 1] = (int64_t)(its->pu.size() / kWarps);
+    // segmented-sum items: whole levels packed up to Tr positions; a longer
+    // level is cut into pieces
     for (int k = 0; k < K; ++k) {
       const int64_t lb = pl->prob_lev_off[(size_t)p * K + k];
       const int64_t le = pl->prob_lev_off[(size_t)(p + 1) * K + k];
@@ -450,11 +471,8 @@ int plan_items(fe_plan* pl, int C, ItemSet** out) {
           sl.npieces = (int32_t)npieces;
           sl.fe = k;
           sl.level = (int32_t)l;
-          sl.norm_slot = -1;
-          sl.pad = 0;
           const int32_t sid = (int32_t)its->splits.size();
           its->splits.push_back(sl);
-          splits_here.push_back(sid);
           for (int64_t q = 0; q < npieces; ++q) {
             const int64_t pb = b + q * psz, pe = std::min(e, pb + psz);
             its->rd.push_back({pb, pe, k, p, sid, (int32_t)q});
@@ -475,26 +493,21 @@ int plan_items(fe_plan* pl, int C, ItemSet** out) {
       }
       if (cur_b >= 0) its->rd.push_back({cur_b, cur_e, k, p, -1, 0});
     }
-    while ((its->rd.size() - r0) % kWarps) its->rd.push_back({0, 0, 0, p, -1, 0});
-    if (its->rd.size() == r0)
-      for (int w = 0; w < kWarps; ++w) its->rd.push_back({0, 0, 0, p, -1, 0});
-    its->rd_slot_off[p] = slot;
-    const int64_t ncta = (int64_t)((its->rd.size() - r0) / kWarps);
-    for (int64_t c = 0; c < ncta; ++c) its->rd_cta_slot.push_back((int32_t)(slot + c));
-    slot += ncta;
-    for (int32_t sid : splits_here) its->splits[(size_t)sid].norm_slot = (int32_t)(slot++);
-    its->rd_slot_off[p + 1] = slot;
+  }
+  for (int p = 0; p < nprob; ++p) {
+    its->ex_slot_off[p + 1] = std::max(its->ex_slot_off[p + 1], its->ex_slot_off[p]);
+    its->pu_slot_off[p + 1] = std::max(its->pu_slot_off[p + 1], its->pu_slot_off[p]);
   }
   its->Se = its->ex_slot_off[nprob];
-  its->Sr = slot;
+  its->Sp = its->pu_slot_off[nprob];
 
   cudaStream_t s = pl->stream;
   int st = upload(its->d_ex, its->ex.data(), its->ex.size(), s);
   if (!st) st = upload(its->d_rd, its->rd.data(), its->rd.size(), s);
-  if (!st) st = upload(its->d_splits, its->splits.data(), std::max<size_t>(its->splits.size(), 1), s);
-  if (!st) st = upload(its->d_cta_slot, its->rd_cta_slot.data(), its->rd_cta_slot.size(), s);
+  if (!st) st = upload(its->d_splits, its->splits.data(), its->splits.size(), s);
+  if (!st) st = upload(its->d_pu, its->pu.data(), its->pu.size(), s);
   if (!st) st = upload(its->d_ex_off, its->ex_slot_off.data(), its->ex_slot_off.size(), s);
-  if (!st) st = upload(its->d_rd_off, its->rd_slot_off.data(), its->rd_slot_off.size(), s);
+  if (!st) st = upload(its->d_pu_off, its->pu_slot_off.data(), its->pu_slot_off.size(), s);
   if (!st) st = its->d_split_cnt.ensure(std::max<size_t>(its->splits.size(), 1) * 4);
   if (st) return st;
   FE_CK(cudaMemsetAsync(its->d_split_cnt.p, 0, std::max<size_t>(its->splits.size(), 1) * 4, s));

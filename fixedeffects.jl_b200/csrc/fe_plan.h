@@ -23,6 +23,7 @@ const char* last_error();
   do {                                                                                  \
     cudaError_t e_ = (call);                                                            \
     if (e_ != cudaSuccess) {                                                            \
+      (void)cudaGetLastError();                                                         \
       ::fe::set_error(std::string("CUDA error ") + cudaGetErrorString(e_) + " at " +    \
                       __FILE__ + ":" + std::to_string(__LINE__) + " (" #call ")");      \
       return 2; /* FE_ERR_CUDA */                                                       \
@@ -44,17 +45,17 @@ struct ItemSet {
   std::vector<ExpandItem> ex;
   std::vector<ReduceItem> rd;
   std::vector<SplitLevel> splits;
-  std::vector<int32_t> rd_cta_slot;       // per reduce CTA
-  std::vector<int64_t> ex_slot_off;       // per problem, expand slots
-  std::vector<int64_t> rd_slot_off;       // per problem, reduce slots
+  std::vector<PItem> pu;
+  std::vector<int64_t> ex_slot_off;       // per problem, expand norm slots (CTAs)
+  std::vector<int64_t> pu_slot_off;       // per problem, P-side norm slots (CTAs)
   int64_t n_pieces = 0;
-  int64_t Se = 0, Sr = 0;                 // slot counts
-  DevBuf d_ex, d_rd, d_splits, d_cta_slot, d_ex_off, d_rd_off, d_split_cnt;
+  int64_t Se = 0, Sp = 0;                 // slot counts
+  DevBuf d_ex, d_rd, d_splits, d_pu, d_ex_off, d_pu_off, d_split_cnt;
 };
 
 struct Workspace {
   int C = 0;
-  DevBuf B64, R64, U, V, H, Hb, X, X64;
+  DevBuf B64, R64, U, V, H, Hb, X, X64, S;
   DevBuf part_e, part_a, part_b, piece_part, inst, counters;
   DevBuf coef;
   DevBuf ystage;  // device copy of host Y for host-buffer solves

@@ -135,27 +135,53 @@ struct Ctx {
   double* part_a;
   double* part_b;
   double* piece;
+  void* S;
 };
+
+// unroll depths (row slots per lane group per step)
+template <int C> struct Tune {
+  static constexpr int kExpandU = 4;
+  static constexpr int kSegU = 8;
+  static constexpr int kPU = 4;
+};
+template <typename T, int C> constexpr int vec_of() { return Shape<T, C>::VEC; }
 
 template <typename TA, int C, class Tab, class Epi>
 static int launch_expand(Ctx& c, Tab tab, Epi epi, double* part, const char* name, double bytes) {
   ProfScope ps(c.pl, name, bytes);
   const unsigned grid = (unsigned)(c.its->ex.size() / kWarps);
-  k_expand<TA, C, 4, Tab, Epi><<<grid, kThreads, 0, c.s>>>(
-      c.d, c.its->d_ex.as<ExpandItem>(), (int64_t)c.its->ex.size(), tab, epi, part, c.its->Se);
+  const ExpandItem* items = c.its->d_ex.as<ExpandItem>();
+  const int64_t n = (int64_t)c.its->ex.size();
+  constexpr int U = Tune<C>::kExpandU;
+  if (c.d.K <= 2)
+    k_expand<TA, C, U, 2, Tab, Epi><<<grid, kThreads, 0, c.s>>>(c.d, items, n, tab, epi, part, c.its->Se);
+  else if (c.d.K <= 4)
+    k_expand<TA, C, U, 4, Tab, Epi><<<grid, kThreads, 0, c.s>>>(c.d, items, n, tab, epi, part, c.its->Se);
+  else
+    k_expand<TA, C, U, kMaxFE, Tab, Epi><<<grid, kThreads, 0, c.s>>>(c.d, items, n, tab, epi, part, c.its->Se);
   FE_CK(cudaGetLastError());
   return 0;
 }
 
-template <typename TA, int C, class Load, class Epi>
-static int launch_reduce(Ctx& c, Load ld, Epi epi, double* pa, double* pb, const char* name,
-                         double bytes) {
+template <typename TA, int C, class Load>
+static int launch_segsum(Ctx& c, Load ld, TA* out, const char* name, double bytes) {
+  if (c.its->rd.empty()) return 0;
   ProfScope ps(c.pl, name, bytes);
-  const unsigned grid = (unsigned)(c.its->rd.size() / kWarps);
-  k_reduce<TA, C, 4, Load, Epi><<<grid, kThreads, 0, c.s>>>(
-      c.d, c.its->d_rd.as<ReduceItem>(), (int64_t)c.its->rd.size(), ld, epi,
-      c.its->d_splits.as<SplitLevel>(), c.piece, c.its->d_split_cnt.as<int32_t>(), pa, pb,
-      c.its->Sr, c.its->d_cta_slot.as<int32_t>());
+  const unsigned grid = (unsigned)((c.its->rd.size() + kWarps - 1) / kWarps);
+  k_segsum<TA, C, Tune<C>::kSegU, Load><<<grid, kThreads, 0, c.s>>>(
+      c.d, c.its->d_rd.as<ReduceItem>(), (int64_t)c.its->rd.size(), ld, out,
+      c.its->d_splits.as<SplitLevel>(), c.piece, c.its->n_pieces, c.its->d_split_cnt.as<int32_t>());
+  FE_CK(cudaGetLastError());
+  return 0;
+}
+
+template <int C, class Epi>
+static int launch_pupdate(Ctx& c, const typename Epi::TS* S, Epi epi, double* pa, double* pb,
+                          const char* name, double bytes) {
+  ProfScope ps(c.pl, name, bytes);
+  const unsigned grid = (unsigned)(c.its->pu.size() / kWarps);
+  k_pupdate<C, Tune<C>::kPU, Epi><<<grid, kThreads, 0, c.s>>>(
+      c.d, c.its->d_pu.as<PItem>(), (int64_t)c.its->pu.size(), S, epi, pa, pb, c.its->Sp);
   FE_CK(cudaGetLastError());
   return 0;
 }
@@ -171,8 +197,8 @@ static int launch_scalar_phase(Ctx& c, int phase, int init_mode) {
   a.counters = c.counters;
   a.off0 = c.its->d_ex_off.as<int64_t>();
   a.S0 = c.its->Se;
-  a.off1 = c.its->d_rd_off.as<int64_t>();
-  a.S1 = c.its->Sr;
+  a.off1 = c.its->d_pu_off.as<int64_t>();
+  a.S1 = c.its->Sp;
   switch (phase) {
     case PH_INIT_BETA:
     case PH_BETA:
@@ -204,9 +230,10 @@ static int read_counter(Ctx& c, int idx, int32_t* out) {
   return 0;
 }
 
-// algorithmic bytes per launch (the roofline numerators)
+// algorithmic bytes per launch (the roofline numerators): every index vector
+// and observation row once, every coefficient-table row once
 struct Bytes {
-  double expand, reduce, resid64, grad64;
+  double expand, segsum, pupdate, resid64, segsum64, grad64;
 };
 static Bytes alg_bytes(const fe_plan* pl, int C, int sT) {
   Bytes b{};
@@ -226,9 +253,11 @@ static Bytes alg_bytes(const fe_plan* pl, int C, int sT) {
   }
   const double refs = N * 4.0 * pl->K;
   b.expand = refs + cw + 2.0 * N * C * sT + P * C * sT;
-  b.reduce = posmeta + cwp + pos * C * sT + 8.0 * P * C * sT;
+  b.segsum = posmeta + cwp + pos * C * sT + P * C * sT;
+  b.pupdate = 9.0 * P * C * sT;
   b.resid64 = refs + cw64 + N * C * (8.0 + 8.0 + 4.0) + P * C * 12.0;
-  b.grad64 = posmeta + cwp64 + pos * C * 8.0 + P * C * 24.0;
+  b.segsum64 = posmeta + cwp64 + pos * C * 8.0 + P * C * 8.0;
+  b.grad64 = P * C * (8.0 + 4.0 + 8.0 + 4.0 + 8.0);
   return b;
 }
 
@@ -248,8 +277,9 @@ static int prepare(fe_plan* pl, int C, int sT, bool mixed, Ctx& c) {
   if ((st = w.X.ensure(P * nC * (size_t)sT))) return st;
   if (mixed && (st = w.X64.ensure(P * nC * 8))) return st;
   if ((st = w.part_e.ensure((size_t)std::max<int64_t>(its->Se, 1) * nC * 8))) return st;
-  if ((st = w.part_a.ensure((size_t)std::max<int64_t>(its->Sr, 1) * nC * 8))) return st;
-  if ((st = w.part_b.ensure((size_t)std::max<int64_t>(its->Sr, 1) * nC * 8))) return st;
+  if ((st = w.part_a.ensure((size_t)std::max<int64_t>(its->Sp, 1) * nC * 8))) return st;
+  if ((st = w.part_b.ensure((size_t)std::max<int64_t>(its->Sp, 1) * nC * 8))) return st;
+  if ((st = w.S.ensure(P * nC * 8))) return st;
   if ((st = w.piece_part.ensure((size_t)std::max<int64_t>(its->n_pieces, 1) * nC * 8))) return st;
   if ((st = w.inst.ensure((size_t)pl->nprob * nC * sizeof(Inst)))) return st;
   if ((st = w.counters.ensure(64))) return st;
@@ -268,6 +298,7 @@ static int prepare(fe_plan* pl, int C, int sT, bool mixed, Ctx& c) {
   c.part_a = w.part_a.as<double>();
   c.part_b = w.part_b.as<double>();
   c.piece = w.piece_part.as<double>();
+  c.S = w.S.p;
   // coefficient-side slabs start at zero (levels without observations and
   // the null levels are never written afterwards)
   FE_CK(cudaMemsetAsync(w.V.p, 0, P * nC * (size_t)sT, c.s));
@@ -275,6 +306,7 @@ static int prepare(fe_plan* pl, int C, int sT, bool mixed, Ctx& c) {
   FE_CK(cudaMemsetAsync(w.Hb.p, 0, P * nC * (size_t)sT, c.s));
   FE_CK(cudaMemsetAsync(w.X.p, 0, P * nC * (size_t)sT, c.s));
   if (mixed) FE_CK(cudaMemsetAsync(w.X64.p, 0, P * nC * 8, c.s));
+  FE_CK(cudaMemsetAsync(w.S.p, 0, P * nC * 8, c.s));
   FE_CK(cudaMemsetAsync(c.counters, 0, 64, c.s));
   return 0;
 }
@@ -342,6 +374,26 @@ static void init_insts(fe_plan* pl, const SolveReq& rq, int C, int ncols, std::v
 }
 
 // ---------------------------------------------------------------------------
+// coefficient download (solve_coefficients!)
+// ---------------------------------------------------------------------------
+template <typename TX>
+static int download_coefs(fe_plan* pl, Ctx& c, const TX* X, const SolveReq& rq) {
+  Workspace& w = pl->ws;
+  for (int k = 0; k < pl->K; ++k) {
+    const int64_t n = pl->nlev[k];
+    if (!n) continue;
+    int st = w.coef.ensure((size_t)n * 8);
+    if (st) return st;
+    k_coefs<TX><<<grid1(n), 256, 0, c.s>>>(X, c.C, 0, pl->lev_base[k], n,
+                                             pl->d_scale_d[k].as<double>(), w.coef.as<double>());
+    FE_CK(cudaGetLastError());
+    FE_CK(cudaMemcpyAsync(rq.coefs[k], w.coef.p, (size_t)n * 8, cudaMemcpyDeviceToHost, c.s));
+    FE_CK(cudaStreamSynchronize(c.s));
+  }
+  return 0;
+}
+
+// ---------------------------------------------------------------------------
 // plain LSMR (bulk type T) on one tile
 // ---------------------------------------------------------------------------
 template <typename T, int C>
@@ -360,38 +412,41 @@ static int solve_plain_tile(fe_plan* pl, const SolveReq& rq, int64_t col0, int n
   T* V = w.V.as<T>();
   T* X = w.X.as<T>();
   double* B64 = w.B64.as<double>();
+  double* S64 = static_cast<double*>(c.S);
+  T* ST = static_cast<T*>(c.S);
   // warm start x = A'b (src/AbstractFixedEffectSolver.jl:56); solve_coefficients! starts at 0
   if (rq.residuals) {
-    if ((st = launch_reduce<double, C>(c, LoadIn<double, double>{B64}, EpiStoreX<T>{X, true},
-                                       nullptr, nullptr, "reduce_warm", 0.0)))
+    if ((st = launch_segsum<double, C>(c, LoadIn<double, double, vec_of<double, C>()>{B64}, S64, "segsum_warm", 0.0)))
+      return st;
+    if ((st = launch_pupdate<C>(c, S64, PEpiStoreX<T, vec_of<double, C>()>{X, true}, nullptr, nullptr, "pupdate_warm", 0.0)))
       return st;
   }
   // u = b - A x, beta (lsmr.jl:63-64)
-  if ((st = launch_expand<T, C>(c, TabOne<T, T>{X},
-                                EpiBminusAx<T, T>{B64, U, nullptr, c.inst, 0, true}, c.part_e,
+  if ((st = launch_expand<T, C>(c, TabOne<T, T, vec_of<T, C>()>{X},
+                                EpiBminusAx<T, T, vec_of<T, C>()>{B64, U, nullptr, c.inst, 0}, c.part_e,
                                 "expand_init", by.expand)))
     return st;
   if ((st = launch_scalar_phase(c, PH_INIT_BETA, 0))) return st;
-  EpiReduceLsmr<T> er{};
-  er.V = V;
-  er.H = w.H.as<T>();
-  er.Hb = w.Hb.as<T>();
-  er.X = X;
-  er.inst = c.inst;
-  if ((st = launch_reduce<T, C>(c, LoadIn<T, T>{U}, er, c.part_a, c.part_b, "reduce", by.reduce)))
-    return st;
+  PEpiLsmr<T, vec_of<T, C>()> pe{};
+  pe.V = V;
+  pe.H = w.H.as<T>();
+  pe.Hb = w.Hb.as<T>();
+  pe.X = X;
+  pe.inst = c.inst;
+  if ((st = launch_segsum<T, C>(c, LoadIn<T, T, vec_of<T, C>()>{U}, ST, "segsum", by.segsum))) return st;
+  if ((st = launch_pupdate<C>(c, ST, pe, c.part_a, c.part_b, "pupdate", by.pupdate))) return st;
   if ((st = launch_scalar_phase(c, PH_INIT_ALPHA, 1))) return st;
   int32_t nact = 0;
   if ((st = read_counter(c, 0, &nact))) return st;
-  EpiExpandLsmr<T> ee{};
+  EpiExpandLsmr<T, vec_of<T, C>()> ee{};
   ee.U = U;
   ee.inst = c.inst;
   const int64_t cap = std::max<int64_t>(rq.maxiter, 1) + 2;
   for (int64_t it = 1; nact > 0 && it <= cap; ++it) {
-    if ((st = launch_expand<T, C>(c, TabOne<T, T>{V}, ee, c.part_e, "expand", by.expand))) return st;
+    if ((st = launch_expand<T, C>(c, TabOne<T, T, vec_of<T, C>()>{V}, ee, c.part_e, "expand", by.expand))) return st;
     if ((st = launch_scalar_phase(c, PH_BETA, 0))) return st;
-    if ((st = launch_reduce<T, C>(c, LoadIn<T, T>{U}, er, c.part_a, c.part_b, "reduce", by.reduce)))
-      return st;
+    if ((st = launch_segsum<T, C>(c, LoadIn<T, T, vec_of<T, C>()>{U}, ST, "segsum", by.segsum))) return st;
+    if ((st = launch_pupdate<C>(c, ST, pe, c.part_a, c.part_b, "pupdate", by.pupdate))) return st;
     if ((st = launch_scalar_phase(c, PH_ALPHA, 0))) return st;
     if (it % pl->opt_check_every == 0 || it == cap) {
       if ((st = read_counter(c, 0, &nact))) return st;
@@ -399,8 +454,8 @@ static int solve_plain_tile(fe_plan* pl, const SolveReq& rq, int64_t col0, int n
   }
   if (rq.residuals) {
     // r = b - A x (src/AbstractFixedEffectSolver.jl:62)
-    if ((st = launch_expand<T, C>(c, TabOne<T, T>{X},
-                                  EpiBminusAx<double, T>{B64, w.R64.as<double>(), nullptr, c.inst, 0, true},
+    if ((st = launch_expand<T, C>(c, TabOne<T, T, vec_of<T, C>()>{X},
+                                  EpiBminusAx<double, T, vec_of<T, C>()>{B64, w.R64.as<double>(), nullptr, c.inst, 0},
                                   nullptr, "expand_final", by.expand)))
       return st;
     if ((st = unload_tile(pl, c, rq, col0, ncols))) return st;
@@ -409,16 +464,7 @@ static int solve_plain_tile(fe_plan* pl, const SolveReq& rq, int64_t col0, int n
   FE_CK(cudaMemcpyAsync(out.data(), c.inst, h.size() * sizeof(Inst), cudaMemcpyDeviceToHost, c.s));
   FE_CK(cudaStreamSynchronize(c.s));
   if (!rq.residuals && rq.coefs) {
-    for (int k = 0; k < pl->K; ++k) {
-      const int64_t n = pl->nlev[k];
-      if (!n) continue;
-      if ((st = w.coef.ensure((size_t)n * 8))) return st;
-      k_coefs<T><<<grid1(n), 256, 0, c.s>>>(X, C, 0, pl->lev_base[k], n, pl->d_scale_d[k].as<double>(),
-                                              w.coef.as<double>());
-      FE_CK(cudaGetLastError());
-      FE_CK(cudaMemcpyAsync(rq.coefs[k], w.coef.p, (size_t)n * 8, cudaMemcpyDeviceToHost, c.s));
-      FE_CK(cudaStreamSynchronize(c.s));
-    }
+    if ((st = download_coefs<T>(pl, c, X, rq))) return st;
   }
   return prof_flush(pl);
 }
@@ -444,50 +490,53 @@ static int solve_mixed_tile(fe_plan* pl, const SolveReq& rq, int64_t col0, int n
   double* X64 = w.X64.as<double>();
   double* B64 = w.B64.as<double>();
   double* R64 = w.R64.as<double>();
+  double* S64 = static_cast<double*>(c.S);
+  float* S32 = static_cast<float*>(c.S);
   if (rq.residuals) {
-    if ((st = launch_reduce<double, C>(c, LoadIn<double, double>{B64}, EpiStoreX<double>{X64, true},
-                                       nullptr, nullptr, "reduce_warm", 0.0)))
+    if ((st = launch_segsum<double, C>(c, LoadIn<double, double, vec_of<double, C>()>{B64}, S64, "segsum_warm", 0.0)))
+      return st;
+    if ((st = launch_pupdate<C>(c, S64, PEpiStoreX<double, vec_of<double, C>()>{X64, true}, nullptr, nullptr,
+                                "pupdate_warm", 0.0)))
       return st;
   }
-  EpiReduceLsmr<float> er{};
-  er.V = V;
-  er.H = w.H.as<float>();
-  er.Hb = w.Hb.as<float>();
-  er.X = X;
-  er.inst = c.inst;
-  EpiExpandLsmr<float> ee{};
+  PEpiLsmr<float, vec_of<float, C>()> pe{};
+  pe.V = V;
+  pe.H = w.H.as<float>();
+  pe.Hb = w.Hb.as<float>();
+  pe.X = X;
+  pe.inst = c.inst;
+  EpiExpandLsmr<float, vec_of<float, C>()> ee{};
   ee.U = U;
   ee.inst = c.inst;
-  EpiGrad64 eg{};
-  eg.V32 = V;
-  eg.X64 = X64;
-  eg.X32 = X;
-  eg.inst = c.inst;
+  PEpiGrad64<vec_of<double, C>()> pg{};
+  pg.V32 = V;
+  pg.X64 = X64;
+  pg.X32 = X;
+  pg.inst = c.inst;
   const int64_t cap = std::max<int64_t>(rq.maxiter, 1) + 2;
   int64_t total_it = 0;
   for (int round = 0; round <= pl->opt_max_rounds + 1; ++round) {
     FE_CK(cudaMemsetAsync(c.counters + 1, 0, sizeof(int32_t), c.s));
     // r = b - A (x64 + dx32) in FP64, with the FP32 copy as the next inner u
-    if ((st = launch_expand<double, C>(c, TabSum64{X64, X},
-                                       EpiBminusAx<double, double>{B64, R64, U, c.inst, 2, true},
+    if ((st = launch_expand<double, C>(c, TabSum64<vec_of<double, C>()>{X64, X},
+                                       EpiBminusAx<double, double, vec_of<double, C>()>{B64, R64, U, c.inst, 2},
                                        c.part_e, "resid64", by.resid64)))
       return st;
     // g = A'r in FP64 (the next inner v), x64 += dx32, ||x64||
-    if ((st = launch_reduce<double, C>(c, LoadIn<double, double>{R64}, eg, c.part_a, c.part_b,
-                                       "grad64", by.grad64)))
+    if ((st = launch_segsum<double, C>(c, LoadIn<double, double, vec_of<double, C>()>{R64}, S64, "segsum64", by.segsum64)))
       return st;
+    if ((st = launch_pupdate<C>(c, S64, pg, c.part_a, c.part_b, "grad64", by.grad64))) return st;
     if ((st = launch_scalar_phase(c, PH_OUTER, 0))) return st;
     int32_t nout = 0;
     if ((st = read_counter(c, 1, &nout))) return st;
     if (nout == 0) break;
     int32_t nact = nout;
     for (int64_t it = 1; nact > 0 && total_it < cap; ++it, ++total_it) {
-      if ((st = launch_expand<float, C>(c, TabOne<float, float>{V}, ee, c.part_e, "expand", by.expand)))
+      if ((st = launch_expand<float, C>(c, TabOne<float, float, vec_of<float, C>()>{V}, ee, c.part_e, "expand", by.expand)))
         return st;
       if ((st = launch_scalar_phase(c, PH_BETA, 0))) return st;
-      if ((st = launch_reduce<float, C>(c, LoadIn<float, float>{U}, er, c.part_a, c.part_b, "reduce",
-                                        by.reduce)))
-        return st;
+      if ((st = launch_segsum<float, C>(c, LoadIn<float, float, vec_of<float, C>()>{U}, S32, "segsum", by.segsum))) return st;
+      if ((st = launch_pupdate<C>(c, S32, pe, c.part_a, c.part_b, "pupdate", by.pupdate))) return st;
       if ((st = launch_scalar_phase(c, PH_ALPHA, 0))) return st;
       if (it % pl->opt_check_every == 0) {
         if ((st = read_counter(c, 0, &nact))) return st;
@@ -501,16 +550,7 @@ static int solve_mixed_tile(fe_plan* pl, const SolveReq& rq, int64_t col0, int n
   FE_CK(cudaMemcpyAsync(out.data(), c.inst, h.size() * sizeof(Inst), cudaMemcpyDeviceToHost, c.s));
   FE_CK(cudaStreamSynchronize(c.s));
   if (!rq.residuals && rq.coefs) {
-    for (int k = 0; k < pl->K; ++k) {
-      const int64_t n = pl->nlev[k];
-      if (!n) continue;
-      if ((st = w.coef.ensure((size_t)n * 8))) return st;
-      k_coefs<double><<<grid1(n), 256, 0, c.s>>>(X64, C, 0, pl->lev_base[k], n,
-                                                   pl->d_scale_d[k].as<double>(), w.coef.as<double>());
-      FE_CK(cudaGetLastError());
-      FE_CK(cudaMemcpyAsync(rq.coefs[k], w.coef.p, (size_t)n * 8, cudaMemcpyDeviceToHost, c.s));
-      FE_CK(cudaStreamSynchronize(c.s));
-    }
+    if ((st = download_coefs<double>(pl, c, X64, rq))) return st;
   }
   return prof_flush(pl);
 }

@@ -168,7 +168,13 @@ def test_batch_problems_vs_oracle(fe, oracle, synth):
         for p, r in zip(probs, outs):
             ro, it_o, cv_o = oracle.solve_residuals(p.Y[:, 0].astype(np.float64), p.refs, p.nlev,
                                                     p.interaction, p.weights, tol=1e-8)
-            assert rel_err(r, ro) < 1e-5  # inputs are Float32 columns
+            # inputs are Float32 columns.  Problems with about one observation
+            # per level are nearly consistent: their residual is tiny and the
+            # reference's test1 (src/utils/lsmr.jl:200-201) fixes it only to
+            # about tol*||y||, so the bar is relative plus an absolute floor.
+            y64 = p.Y[:, 0].astype(np.float64)
+            err = np.linalg.norm(r - ro)
+            assert err <= 1e-5 * np.linalg.norm(ro) + 1e-6 * np.linalg.norm(y64)
 
 
 def test_device_tensor_path(fe, synth, oracle):
