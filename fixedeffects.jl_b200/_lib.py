@@ -29,6 +29,10 @@ FE_OPT_CHECK_EVERY = 2
 FE_OPT_MAX_ROUNDS = 3
 FE_OPT_PROFILE = 4
 FE_OPT_INNER_RHO = 5
+FE_OPT_FUSE = 6
+FE_OPT_EXPAND_VARIANT = 7
+FE_OPT_SEGSUM_VARIANT = 8
+FE_OPT_AUTOTUNE = 9
 
 # every symbol declared in include/fe_b200.h
 EXPORTS = (

@@ -228,6 +228,22 @@ int fe_plan_set_option(fe_plan* plan, int32_t option, double value) {
       }
       plan->opt_inner_rho = value;
       return FE_OK;
+    case FE_OPT_FUSE:
+      plan->opt_fuse = value != 0 ? 1 : 0;
+      return FE_OK;
+    case FE_OPT_AUTOTUNE:
+      plan->opt_autotune = value != 0 ? 1 : 0;
+      return FE_OK;
+    case FE_OPT_EXPAND_VARIANT:
+    case FE_OPT_SEGSUM_VARIANT: {
+      const int v = (int)value;
+      if (v < -1 || v > 3) {
+        set_error("kernel variant must be -1 (default) or 0..3");
+        return FE_ERR_INVALID;
+      }
+      (option == FE_OPT_EXPAND_VARIANT ? plan->opt_ex_variant : plan->opt_seg_variant) = v;
+      return FE_OK;
+    }
     default:
       set_error("unknown option");
       return FE_ERR_INVALID;

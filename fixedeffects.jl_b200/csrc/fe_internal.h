@@ -25,9 +25,14 @@ constexpr int kScalarThreads = 256;
 constexpr int kSentinel = 0x7fffffff;  // "no level" key
 
 // A contiguous range of observations (sorted order) processed by one warp.
+// Items hold whole levels of the primary FE (the FE that orders the
+// observations), so the expand can also reduce that FE; split >= 0 marks one
+// piece of a primary level too long for one warp.
 struct ExpandItem {
   int64_t ib, ie;
   int32_t prob;
+  int32_t split;
+  int32_t piece;
   int32_t pad;
 };
 
@@ -75,6 +80,7 @@ struct FeDev {
   const float* cwp_f[kMaxFE];    // level order: interaction*sqrt(w), or null
   const double* cwp_d[kMaxFE];
   int64_t lev_base[kMaxFE];      // first row of FE k in a [P][C] slab
+  int32_t primary;               // FE whose levels order the observations
 };
 
 // LSMR state of one instance (problem p, column j).  Scalars are FP64 in every

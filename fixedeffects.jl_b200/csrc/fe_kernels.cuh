@@ -164,37 +164,37 @@ struct TabSum64 {
 // s = (A x)[i, cols] and adds the squared new values to nrm.
 // ---------------------------------------------------------------------------
 // LSMR u-update: U <- av * (A v) + au * U   (src/utils/lsmr.jl:104 with the
-// normalisations of u and v folded into av, au).  Columns whose LSMR has
-// stopped keep their U.
+// normalisations of u and v folded into av, au).  A stopped instance has
+// av = 0, au = 1, so its U is left as it is (its norm is not used).
 template <typename T, int VEC>
 struct EpiExpandLsmr {
   using TP = T;
+  using TN = T;  // norm accumulation within an item
   T* __restrict__ U;
   const Inst* __restrict__ inst;
   T av[VEC], au[VEC];
-  bool actv[VEC];
   bool act;
   __device__ __forceinline__ void begin(int prob, int jl, int C) {
     act = false;
 #pragma unroll
     for (int v = 0; v < VEC; ++v) {
       const Inst& s = inst[(int64_t)prob * C + jl * VEC + v];
-      actv[v] = s.active != 0;
       av[v] = (T)s.ex_av;
       au[v] = (T)s.ex_au;
-      act = act || actv[v];
+      act = act || s.active != 0;
     }
   }
   __device__ __forceinline__ VA<T, VEC> pre(int64_t o) const { return vld<T, VEC>(U + o); }
-  __device__ __forceinline__ void apply(int64_t o, const VA<T, VEC>& s, const VA<T, VEC>& old,
-                                        double (&nrm)[VEC]) {
+  __device__ __forceinline__ VA<T, VEC> apply(int64_t o, const VA<T, VEC>& s,
+                                               const VA<T, VEC>& old, TN (&nrm)[VEC]) {
     VA<T, VEC> u;
 #pragma unroll
     for (int v = 0; v < VEC; ++v) {
-      u.v[v] = actv[v] ? av[v] * s.v[v] + au[v] * old.v[v] : old.v[v];
-      if (actv[v]) nrm[v] += (double)u.v[v] * (double)u.v[v];
+      u.v[v] = av[v] * s.v[v] + au[v] * old.v[v];
+      nrm[v] += u.v[v] * u.v[v];
     }
     vst<T, VEC>(U + o, u);
+    return u;
   }
 };
 
@@ -205,6 +205,7 @@ struct EpiExpandLsmr {
 template <typename TOut, typename TA, int VEC>
 struct EpiBminusAx {
   using TP = double;
+  using TN = double;
   const double* __restrict__ B;
   TOut* __restrict__ out;
   float* __restrict__ out32;  // optional FP32 copy (mixed-precision u)
@@ -223,15 +224,17 @@ struct EpiBminusAx {
     }
   }
   __device__ __forceinline__ VA<double, VEC> pre(int64_t o) const { return vldg<double, VEC>(B + o); }
-  __device__ __forceinline__ void apply(int64_t o, const VA<TA, VEC>& s, const VA<double, VEC>& b,
-                                        double (&nrm)[VEC]) {
+  __device__ __forceinline__ VA<TA, VEC> apply(int64_t o, const VA<TA, VEC>& s,
+                                                const VA<double, VEC>& b, TN (&nrm)[VEC]) {
     VA<TOut, VEC> r;
+    VA<TA, VEC> ret;
     VA<float, VEC> r32;
 #pragma unroll
     for (int v = 0; v < VEC; ++v) {
       const double x = b.v[v] - (double)s.v[v];
       r.v[v] = (TOut)x;
       r32.v[v] = (float)x;
+      ret.v[v] = (TA)r.v[v];
       if (actv[v]) nrm[v] += x * x;
     }
     if (all) {
@@ -245,6 +248,130 @@ struct EpiBminusAx {
           if (out32) out32[o + v] = r32.v[v];
         }
     }
+    return ret;
+  }
+};
+
+// ---------------------------------------------------------------------------
+// Segmented run accumulation shared by k_segsum and the fused k_expand.
+// Rows arrive G at a time (one per lane group) in key order; equal keys are
+// contiguous.  An inclusive segmented scan over the groups plus a carry across
+// steps yields each key's sum; the group holding a key's last row stores it.
+// ---------------------------------------------------------------------------
+template <typename TA, int VEC, int CL, int G>
+struct SegRun {
+  int ckey;
+  VA<TA, VEC> carry;  // running sum of key ckey (the same in every group)
+  VA<TA, VEC> acc;    // per-group partial of ckey from fast-path steps
+  bool pend;          // acc holds something (warp-uniform)
+  __device__ __forceinline__ void init() {
+    ckey = -1;
+    pend = false;
+#pragma unroll
+    for (int v = 0; v < VEC; ++v) {
+      carry.v[v] = TA(0);
+      acc.v[v] = TA(0);
+    }
+  }
+  // carry += sum over groups of acc (fixed xor tree)
+  __device__ __forceinline__ void fold() {
+    if (!pend) return;
+#pragma unroll
+    for (int v = 0; v < VEC; ++v) {
+      TA t = acc.v[v];
+#pragma unroll
+      for (int o = CL; o < 32; o <<= 1) t += __shfl_xor_sync(FE_FULL, t, o);
+      carry.v[v] += t;
+      acc.v[v] = TA(0);
+    }
+    pend = false;
+  }
+  // one warp instruction worth of rows: key km and value x of this lane's
+  // group; nvalid groups hold real rows.  Sk points at the lane's column block
+  // of row 0 of the FE's [levels][C] sum slab.
+  __device__ __forceinline__ void push(int km, VA<TA, VEC> x, int nvalid, int g, int jl, int C,
+                                       TA* __restrict__ Sk) {
+    // fast path: every group continues the current run (long levels)
+    if (G > 1 && ckey >= 0 && __all_sync(FE_FULL, km == ckey)) {
+#pragma unroll
+      for (int v = 0; v < VEC; ++v) acc.v[v] += x.v[v];
+      pend = true;
+      return;
+    }
+    fold();
+    const int k0 = __shfl_sync(FE_FULL, km, jl);
+    if (ckey >= 0 && ckey != k0) {
+      if (g == 0) vst<TA, VEC>(Sk + (int64_t)ckey * C, carry);
+      ckey = -1;
+#pragma unroll
+      for (int v = 0; v < VEC; ++v) carry.v[v] = TA(0);
+    }
+#pragma unroll
+    for (int dd = 1; dd < G; dd <<= 1) {
+      const int ko = __shfl_up_sync(FE_FULL, km, dd * CL);
+      const bool take = g >= dd && ko == km;
+#pragma unroll
+      for (int v = 0; v < VEC; ++v) {
+        const TA xo = __shfl_up_sync(FE_FULL, x.v[v], dd * CL);
+        if (take) x.v[v] += xo;
+      }
+    }
+    if (km == ckey) {
+#pragma unroll
+      for (int v = 0; v < VEC; ++v) x.v[v] += carry.v[v];
+    }
+    const int kn = __shfl_down_sync(FE_FULL, km, CL);
+    if (g < nvalid - 1 && kn != km) vst<TA, VEC>(Sk + (int64_t)km * C, x);
+    const int srcl = (nvalid - 1) * CL + jl;
+    ckey = __shfl_sync(FE_FULL, km, srcl);
+#pragma unroll
+    for (int v = 0; v < VEC; ++v) carry.v[v] = __shfl_sync(FE_FULL, x.v[v], srcl);
+  }
+  // end of a work item.  split < 0: the last key is complete.  Otherwise the
+  // item is piece `piece` of split level `sl`: its partial goes to the piece
+  // buffer ([C][n_pieces]) and the last piece to finish (integer counter)
+  // sums all pieces in piece order and stores the level.  smt: 32 doubles of
+  // shared scratch owned by this warp.
+  __device__ __forceinline__ void finish(int split, int piece, const SplitLevel* __restrict__ splits,
+                                         double* __restrict__ piece_part, int64_t n_pieces,
+                                         int32_t* __restrict__ split_cnt, int g, int jl, int C,
+                                         TA* __restrict__ Sk, double* smt) {
+    fold();
+    if (ckey < 0) return;
+    if (split < 0) {
+      if (g == 0) vst<TA, VEC>(Sk + (int64_t)ckey * C, carry);
+      return;
+    }
+    const int lane = threadIdx.x & 31;
+    const SplitLevel sl = splits[split];
+    if (g == 0) {
+#pragma unroll
+      for (int v = 0; v < VEC; ++v)
+        piece_part[(int64_t)(jl * VEC + v) * n_pieces + sl.first_piece + piece] = (double)carry.v[v];
+    }
+    __threadfence();
+    __syncwarp();
+    int last = 0;
+    if (lane == 0) last = (atomicAdd(split_cnt + split, 1) == sl.npieces - 1) ? 1 : 0;
+    last = __shfl_sync(FE_FULL, last, 0);
+    if (!last) return;
+    __threadfence();
+    for (int jj = 0; jj < C; ++jj) {
+      const double* pp = piece_part + (int64_t)jj * n_pieces + sl.first_piece;
+      double acc = 0.0;
+      for (int q = lane; q < sl.npieces; q += 32) acc += __ldcg(pp + q);
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(FE_FULL, acc, o);
+      if (lane == 0) smt[jj] = acc;
+    }
+    __syncwarp();
+    if (g == 0) {
+      VA<TA, VEC> tot;
+#pragma unroll
+      for (int v = 0; v < VEC; ++v) tot.v[v] = (TA)smt[jl * VEC + v];
+      vst<TA, VEC>(Sk + (int64_t)ckey * C, tot);
+    }
+    if (lane == 0) split_cnt[split] = 0;
   }
 };
 
@@ -254,20 +381,35 @@ struct EpiBminusAx {
 // that every index and row load of a step can be issued before the first is
 // consumed).  The next step's refs and weights are prefetched while the
 // current step's rows are in flight.
+//
+// FUSE: the observations are sorted by the primary FE, so the new values are
+// also reduced by that FE here (the reference's gather! for it,
+// src/SolverCPU.jl:21-27): a contiguous segmented sum of cw * new value per
+// primary level, stored to Sf.  The separate segsum then skips the primary.
 // ---------------------------------------------------------------------------
-template <typename TA, int C, int U, int KB, class Tab, class Epi>
+struct FuseArgs {
+  double* sum;  // [P][C] sum slab (TA-typed), null when not fused
+  const SplitLevel* splits;
+  double* piece_part;
+  int64_t n_pieces;
+  int32_t* split_cnt;
+};
+
+template <typename TA, int C, int U, int KB, bool FUSE, bool PF, class Tab, class Epi>
 __global__ void __launch_bounds__(kThreads)
 k_expand(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_items, Tab tab, Epi epi,
-         double* __restrict__ part, int64_t S) {
+         double* __restrict__ part, int64_t S, FuseArgs fz) {
   using Sh = Shape<TA, C>;
   constexpr int VEC = Sh::VEC, CL = Sh::CL, G = Sh::G;
   constexpr int STEP = G * U;                     // observations per step
   constexpr int NI = STEP >= 32 ? STEP / 32 : 1;  // index registers per lane
   using TP = typename Epi::TP;
+  using TN = typename Epi::TN;
   __shared__ double sm[kWarps][32];
   const int lane = threadIdx.x & 31;
+  const int wib = threadIdx.x >> 5;
   const int g = lane / CL, jl = lane - g * CL;
-  const int64_t w = (int64_t)blockIdx.x * kWarps + (threadIdx.x >> 5);
+  const int64_t w = (int64_t)blockIdx.x * kWarps + wib;
   double nrm[VEC];
 #pragma unroll
   for (int v = 0; v < VEC; ++v) nrm[v] = 0.0;
@@ -276,6 +418,13 @@ k_expand(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_items, T
     epi.begin(it.prob, jl, C);
     if (__any_sync(FE_FULL, epi.act)) {
       const int K = d.K;
+      const int kp = d.primary;
+      TN nit[VEC];  // norms of this item (FP32 for the FP32 path), flushed below
+#pragma unroll
+      for (int v = 0; v < VEC; ++v) nit[v] = TN(0);
+      SegRun<TA, VEC, CL, G> run;
+      run.init();
+      TA* Sf = FUSE ? reinterpret_cast<TA*>(fz.sum) + d.lev_base[kp] * C + jl * VEC : nullptr;
       int rl[KB][NI];
       TA cl[KB][NI];
       auto fetch = [&](int64_t base) {
@@ -285,14 +434,15 @@ k_expand(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_items, T
           for (int r = 0; r < NI; ++r) {
             const int64_t p = base + r * 32 + lane;
             const bool ok = k < K && p < it.ie && (r * 32 + lane) < STEP;
-            rl[k][r] = ok ? __ldg(d.refs[k] + p) : 0;
+            rl[k][r] = ok ? __ldg(d.refs[k] + p) : kSentinel;
             const TA* __restrict__ cw = cw_of<TA>(d, k < K ? k : 0);
             cl[k][r] = (ok && cw) ? __ldg(cw + p) : TA(1);
           }
         }
       };
-      fetch(it.ib);
+      if (PF) fetch(it.ib);
       for (int64_t base = it.ib; base < it.ie; base += STEP) {
+        if (!PF) fetch(base);
         int rc[KB][NI];
         TA cc[KB][NI];
 #pragma unroll
@@ -302,14 +452,18 @@ k_expand(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_items, T
             rc[k][r] = rl[k][r];
             cc[k][r] = cl[k][r];
           }
-        if (base + STEP < it.ie) fetch(base + STEP);
+        if (PF && base + STEP < it.ie) fetch(base + STEP);
         VA<TP, VEC> old[U];
         VA<TA, VEC> s[U];
+        int pkey[U];
+        TA pcw[U];
 #pragma unroll
         for (int u = 0; u < U; ++u) {
           const int64_t i = base + u * G + g;
 #pragma unroll
           for (int v = 0; v < VEC; ++v) s[u].v[v] = TA(0);
+          pkey[u] = kSentinel;
+          pcw[u] = TA(0);
           if (i < it.ie && epi.act) old[u] = epi.pre(i * C + jl * VEC);
         }
 #pragma unroll
@@ -322,6 +476,10 @@ k_expand(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_items, T
               const int q = u * G;  // + g: the same index register (G divides 32)
               const int ref = __shfl_sync(FE_FULL, rc[k][q >> 5], (q & 31) + g);
               const TA c = __shfl_sync(FE_FULL, cc[k][q >> 5], (q & 31) + g);
+              if (FUSE && k == kp) {
+                pkey[u] = ref;
+                pcw[u] = c;
+              }
               const int64_t i = base + u * G + g;
               if (i < it.ie && epi.act) {
                 const TA cs = c * __ldg(sc + ref);
@@ -335,11 +493,29 @@ k_expand(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_items, T
 #pragma unroll
         for (int u = 0; u < U; ++u) {
           const int64_t i = base + u * G + g;
-          if (i < it.ie && epi.act) epi.apply(i * C + jl * VEC, s[u], old[u], nrm);
+          VA<TA, VEC> nv;
+#pragma unroll
+          for (int v = 0; v < VEC; ++v) nv.v[v] = TA(0);
+          if (i < it.ie && epi.act) nv = epi.apply(i * C + jl * VEC, s[u], old[u], nit);
+          if (FUSE) {
+            const int64_t b0 = base + (int64_t)u * G;
+            if (b0 < it.ie) {  // warp-uniform
+              const int nvalid = (int)((it.ie - b0) < G ? (it.ie - b0) : G);
+#pragma unroll
+              for (int v = 0; v < VEC; ++v) nv.v[v] *= pcw[u];
+              run.push(i < it.ie ? pkey[u] : kSentinel, nv, nvalid, g, jl, C, Sf);
+            }
+          }
         }
       }
+      if (FUSE)
+        run.finish(it.split, it.piece, fz.splits, fz.piece_part, fz.n_pieces, fz.split_cnt, g, jl, C,
+                   Sf, sm[wib]);
+#pragma unroll
+      for (int v = 0; v < VEC; ++v) nrm[v] += (double)nit[v];
     }
   }
+  __syncthreads();
   cta_norm_to_slot<C, VEC>(nrm, part, S, (int64_t)blockIdx.x, sm);
 }
 
@@ -378,7 +554,7 @@ struct LoadScaleSq {
 // Sout[level] by the group holding the level's last position.  Split pieces
 // hand their partial to the last piece of the level.
 // ---------------------------------------------------------------------------
-template <typename TA, int C, int U, class Load>
+template <typename TA, int C, int U, bool PF, class Load>
 __global__ void __launch_bounds__(kThreads)
 k_segsum(const FeDev d, const ReduceItem* __restrict__ items, int64_t n_items, Load ld,
          TA* __restrict__ Sout, const SplitLevel* __restrict__ splits,
@@ -399,14 +575,13 @@ k_segsum(const FeDev d, const ReduceItem* __restrict__ items, int64_t n_items, L
   const int32_t* __restrict__ key = d.key[k];
   const TA* __restrict__ cwp = cwp_of<TA>(d, k);
   TA* __restrict__ Sk = Sout + d.lev_base[k] * C + jl * VEC;
-  int ckey = -1;
-  VA<TA, VEC> carry;
-#pragma unroll
-  for (int v = 0; v < VEC; ++v) carry.v[v] = TA(0);
-  for (int64_t base = it.pb; base < it.pe; base += STEP) {
-    int kl[NI];
-    int il[NI];
-    TA cl[NI];
+  SegRun<TA, VEC, CL, G> run;
+  run.init();
+  // index data of a step (level keys, sorted positions, weights), fetched one
+  // step ahead so that the row gathers of a step do not wait for its indices
+  int kl[NI], il[NI];
+  TA cl[NI];
+  auto fetch = [&](int64_t base) {
 #pragma unroll
     for (int r = 0; r < NI; ++r) {
       const int64_t p = base + r * 32 + lane;
@@ -418,6 +593,10 @@ k_segsum(const FeDev d, const ReduceItem* __restrict__ items, int64_t n_items, L
       if (Load::kSquareWeight) c = c * c;
       cl[r] = c;
     }
+  };
+  if (PF) fetch(it.pb);
+  for (int64_t base = it.pb; base < it.pe; base += STEP) {
+    if (!PF) fetch(base);
     VA<TA, VEC> val[U];
     int kk[U];
 #pragma unroll
@@ -436,79 +615,17 @@ k_segsum(const FeDev d, const ReduceItem* __restrict__ items, int64_t n_items, L
         for (int v = 0; v < VEC; ++v) val[u].v[v] = TA(0);
       }
     }
+    if (PF && base + STEP < it.pe) fetch(base + STEP);
 #pragma unroll
     for (int u = 0; u < U; ++u) {
       const int64_t b0 = base + (int64_t)u * G;
       if (b0 >= it.pe) break;  // warp-uniform
       const int nvalid = (int)((it.pe - b0) < G ? (it.pe - b0) : G);
-      const int k0 = __shfl_sync(FE_FULL, kk[u], jl);
-      if (ckey >= 0 && ckey != k0) {
-        if (g == 0) vst<TA, VEC>(Sk + (int64_t)ckey * C, carry);
-        ckey = -1;
-#pragma unroll
-        for (int v = 0; v < VEC; ++v) carry.v[v] = TA(0);
-      }
-      VA<TA, VEC> x = val[u];
-      const int km = kk[u];
-#pragma unroll
-      for (int dd = 1; dd < G; dd <<= 1) {
-        const int ko = __shfl_up_sync(FE_FULL, km, dd * CL);
-        const bool take = g >= dd && ko == km;
-#pragma unroll
-        for (int v = 0; v < VEC; ++v) {
-          const TA xo = __shfl_up_sync(FE_FULL, x.v[v], dd * CL);
-          if (take) x.v[v] += xo;
-        }
-      }
-      if (km == ckey) {
-#pragma unroll
-        for (int v = 0; v < VEC; ++v) x.v[v] += carry.v[v];
-      }
-      const int kn = __shfl_down_sync(FE_FULL, km, CL);
-      if (g < nvalid - 1 && kn != km) vst<TA, VEC>(Sk + (int64_t)km * C, x);
-      const int srcl = (nvalid - 1) * CL + jl;
-      ckey = __shfl_sync(FE_FULL, km, srcl);
-#pragma unroll
-      for (int v = 0; v < VEC; ++v) carry.v[v] = __shfl_sync(FE_FULL, x.v[v], srcl);
+      run.push(kk[u], val[u], nvalid, g, jl, C, Sk);
     }
   }
-  if (ckey < 0) return;
-  if (it.split < 0) {
-    if (g == 0) vst<TA, VEC>(Sk + (int64_t)ckey * C, carry);
-    return;
-  }
-  // split level: piece partials are stored column-major [C][n_pieces]
-  const SplitLevel sl = splits[it.split];
-  if (g == 0) {
-#pragma unroll
-    for (int v = 0; v < VEC; ++v)
-      piece_part[(int64_t)(jl * VEC + v) * n_pieces + sl.first_piece + it.pad] = (double)carry.v[v];
-  }
-  __threadfence();
-  __syncwarp();
-  int last = 0;
-  if (lane == 0) last = (atomicAdd(split_cnt + it.split, 1) == sl.npieces - 1) ? 1 : 0;
-  last = __shfl_sync(FE_FULL, last, 0);
-  if (!last) return;
-  __threadfence();
-  // all 32 lanes sum the pieces of each column in a fixed order
-  const int wib = threadIdx.x >> 5;
-  for (int jj = 0; jj < C; ++jj) {
-    const double* pp = piece_part + (int64_t)jj * n_pieces + sl.first_piece;
-    double acc = 0.0;
-    for (int q = lane; q < sl.npieces; q += 32) acc += __ldcg(pp + q);
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(FE_FULL, acc, o);
-    if (lane == 0) smt[wib][jj] = acc;
-  }
-  __syncwarp();
-  if (g == 0) {
-    VA<TA, VEC> tot;
-#pragma unroll
-    for (int v = 0; v < VEC; ++v) tot.v[v] = (TA)smt[wib][jl * VEC + v];
-    vst<TA, VEC>(Sk + (int64_t)ckey * C, tot);
-  }
-  if (lane == 0) split_cnt[it.split] = 0;
+  run.finish(it.split, it.pad, splits, piece_part, n_pieces, split_cnt, g, jl, C, Sk,
+             smt[threadIdx.x >> 5]);
 }
 
 // ---------------------------------------------------------------------------

@@ -292,6 +292,7 @@ int plan_build(fe_plan* pl, int32_t nprob, const int64_t* n_obs, int32_t K,
     d.key[k] = pl->d_key[k].as<int32_t>();
     d.lev_base[k] = pl->lev_base[k];
   }
+  d.primary = pl->primary;
   return plan_update_weights(pl, weights);
 }
 
@@ -368,7 +369,7 @@ int plan_update_weights(fe_plan* pl, const double* weights) {
   FE_CK(cudaMemsetAsync(sums.p, 0, (size_t)std::max<int64_t>(pl->P, 1) * 8, s));
   if (!its->rd.empty()) {
     const unsigned grid = (unsigned)((its->rd.size() + kWarps - 1) / kWarps);
-    k_segsum<double, 1, 8, LoadScaleSq><<<grid, kThreads, 0, s>>>(
+    k_segsum<double, 1, 8, false, LoadScaleSq><<<grid, kThreads, 0, s>>>(
         dd, its->d_rd.as<ReduceItem>(), (int64_t)its->rd.size(), LoadScaleSq{}, sums.as<double>(),
         its->d_splits.as<SplitLevel>(), piece.as<double>(), its->n_pieces,
         its->d_split_cnt.as<int32_t>());
@@ -427,15 +428,58 @@ int plan_items(fe_plan* pl, int C, ItemSet** out) {
   const int K = pl->K;
   its->ex_slot_off.assign((size_t)nprob + 1, 0);
   its->pu_slot_off.assign((size_t)nprob + 1, 0);
+  std::vector<ReduceItem> rd_prim;
+  const int kp = pl->primary;
   for (int p = 0; p < nprob; ++p) {
-    // expand items: chunks of the problem's sorted observation range, padded
-    // so that every CTA belongs to one problem (its norm slot is per problem)
+    // expand items: whole primary levels of the problem's sorted range packed
+    // up to Te observations (a longer level is cut into pieces), padded so
+    // that every CTA belongs to one problem (its norm slot is per problem)
     const int64_t o0 = pl->prob_obs_off[p], o1 = pl->prob_obs_off[p + 1];
     const size_t e0 = its->ex.size();
-    for (int64_t b = o0; b < o1; b += Te) its->ex.push_back({b, std::min(o1, b + Te), p, 0});
-    while ((its->ex.size() - e0) % kWarps) its->ex.push_back({o1, o1, p, 0});
+    const int64_t plb = pl->prob_lev_off[(size_t)p * K + kp];
+    const int64_t ple = pl->prob_lev_off[(size_t)(p + 1) * K + kp];
+    if (ple == plb) {
+      for (int64_t b = o0; b < o1; b += Te) its->ex.push_back({b, std::min(o1, b + Te), p, -1, 0, 0});
+    } else {
+      const std::vector<int64_t>& off = pl->seg_off[kp];
+      const int64_t base = o0 - off[(size_t)plb];  // sorted position of level-order position
+      int64_t cur_b = -1, cur_e = -1;
+      for (int64_t l = plb; l < ple; ++l) {
+        const int64_t b = off[(size_t)l] + base, e = off[(size_t)l + 1] + base, cnt = e - b;
+        if (cnt == 0) continue;
+        if (cnt > Te) {
+          if (cur_b >= 0) {
+            its->ex.push_back({cur_b, cur_e, p, -1, 0, 0});
+            cur_b = -1;
+          }
+          const int64_t npieces = (cnt + Te - 1) / Te;
+          const int64_t psz = (cnt + npieces - 1) / npieces;
+          SplitLevel sl;
+          sl.first_piece = (int32_t)its->ex_n_pieces;
+          sl.npieces = (int32_t)npieces;
+          sl.fe = kp;
+          sl.level = (int32_t)l;
+          const int32_t sid = (int32_t)its->ex_splits.size();
+          its->ex_splits.push_back(sl);
+          for (int64_t q = 0; q < npieces; ++q) {
+            const int64_t pb = b + q * psz, pe = std::min(e, pb + psz);
+            its->ex.push_back({pb, pe, p, sid, (int32_t)q, 0});
+          }
+          its->ex_n_pieces += npieces;
+          continue;
+        }
+        if (cur_b < 0) cur_b = b;
+        cur_e = e;
+        if (cur_e - cur_b >= Te) {
+          its->ex.push_back({cur_b, cur_e, p, -1, 0, 0});
+          cur_b = -1;
+        }
+      }
+      if (cur_b >= 0) its->ex.push_back({cur_b, cur_e, p, -1, 0, 0});
+    }
+    while ((its->ex.size() - e0) % kWarps) its->ex.push_back({o1, o1, p, -1, 0, 0});
     if (its->ex.size() == e0)
-      for (int w = 0; w < kWarps; ++w) its->ex.push_back({o1, o1, p, 0});
+      for (int w = 0; w < kWarps; ++w) its->ex.push_back({o1, o1, p, -1, 0, 0});
     its->ex_slot_off[p + 1] = (int64_t)(its->ex.size() / kWarps);
     // P-side items: chunks of the problem's slab rows, per FE, padded likewise
     const size_t q0 = its->pu.size();
@@ -449,8 +493,10 @@ int plan_items(fe_plan* pl, int C, ItemSet** out) {
       for (int w = 0; w < kWarps; ++w) its->pu.push_back({0, 0, 0, p});
     its->pu_slot_off[p + 1] = (int64_t)(its->pu.size() / kWarps);
     // segmented-sum items: whole levels packed up to Tr positions; a longer
-    // level is cut into pieces
+    // level is cut into pieces.  Items of the primary FE go to a second list
+    // (appended after all others): the fused expand reduces that FE itself.
     for (int k = 0; k < K; ++k) {
+      std::vector<ReduceItem>& dst = (k == kp) ? rd_prim : its->rd;
       const int64_t lb = pl->prob_lev_off[(size_t)p * K + k];
       const int64_t le = pl->prob_lev_off[(size_t)(p + 1) * K + k];
       if (le == lb) continue;
@@ -461,7 +507,7 @@ int plan_items(fe_plan* pl, int C, ItemSet** out) {
         if (cnt == 0) continue;
         if (cnt > Tr) {
           if (cur_b >= 0) {
-            its->rd.push_back({cur_b, cur_e, k, p, -1, 0});
+            dst.push_back({cur_b, cur_e, k, p, -1, 0});
             cur_b = -1;
           }
           const int64_t npieces = (cnt + Tr - 1) / Tr;
@@ -475,25 +521,23 @@ int plan_items(fe_plan* pl, int C, ItemSet** out) {
           its->splits.push_back(sl);
           for (int64_t q = 0; q < npieces; ++q) {
             const int64_t pb = b + q * psz, pe = std::min(e, pb + psz);
-            its->rd.push_back({pb, pe, k, p, sid, (int32_t)q});
+            dst.push_back({pb, pe, k, p, sid, (int32_t)q});
           }
           its->n_pieces += npieces;
           continue;
         }
-        if (cur_b < 0) {
-          cur_b = b;
-          cur_e = e;
-        } else {
-          cur_e = e;
-        }
+        if (cur_b < 0) cur_b = b;
+        cur_e = e;
         if (cur_e - cur_b >= Tr) {
-          its->rd.push_back({cur_b, cur_e, k, p, -1, 0});
+          dst.push_back({cur_b, cur_e, k, p, -1, 0});
           cur_b = -1;
         }
       }
-      if (cur_b >= 0) its->rd.push_back({cur_b, cur_e, k, p, -1, 0});
+      if (cur_b >= 0) dst.push_back({cur_b, cur_e, k, p, -1, 0});
     }
   }
+  its->rd_np = (int64_t)its->rd.size();
+  its->rd.insert(its->rd.end(), rd_prim.begin(), rd_prim.end());
   for (int p = 0; p < nprob; ++p) {
     its->ex_slot_off[p + 1] = std::max(its->ex_slot_off[p + 1], its->ex_slot_off[p]);
     its->pu_slot_off[p + 1] = std::max(its->pu_slot_off[p + 1], its->pu_slot_off[p]);
@@ -508,9 +552,12 @@ int plan_items(fe_plan* pl, int C, ItemSet** out) {
   if (!st) st = upload(its->d_pu, its->pu.data(), its->pu.size(), s);
   if (!st) st = upload(its->d_ex_off, its->ex_slot_off.data(), its->ex_slot_off.size(), s);
   if (!st) st = upload(its->d_pu_off, its->pu_slot_off.data(), its->pu_slot_off.size(), s);
+  if (!st) st = upload(its->d_ex_splits, its->ex_splits.data(), its->ex_splits.size(), s);
   if (!st) st = its->d_split_cnt.ensure(std::max<size_t>(its->splits.size(), 1) * 4);
+  if (!st) st = its->d_ex_split_cnt.ensure(std::max<size_t>(its->ex_splits.size(), 1) * 4);
   if (st) return st;
   FE_CK(cudaMemsetAsync(its->d_split_cnt.p, 0, std::max<size_t>(its->splits.size(), 1) * 4, s));
+  FE_CK(cudaMemsetAsync(its->d_ex_split_cnt.p, 0, std::max<size_t>(its->ex_splits.size(), 1) * 4, s));
   FE_CK(cudaStreamSynchronize(s));
   *out = its.get();
   pl->items[C] = std::move(its);

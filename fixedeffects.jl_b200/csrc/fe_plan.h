@@ -44,19 +44,23 @@ struct ItemSet {
   int C = 0;
   std::vector<ExpandItem> ex;
   std::vector<ReduceItem> rd;
-  std::vector<SplitLevel> splits;
+  std::vector<SplitLevel> splits;      // level pieces of the segsum items
+  std::vector<SplitLevel> ex_splits;   // primary-level pieces of the expand items
+  int64_t rd_np = 0;                   // segsum items of non-primary FEs (first)
+  int64_t ex_n_pieces = 0;
   std::vector<PItem> pu;
   std::vector<int64_t> ex_slot_off;       // per problem, expand norm slots (CTAs)
   std::vector<int64_t> pu_slot_off;       // per problem, P-side norm slots (CTAs)
   int64_t n_pieces = 0;
   int64_t Se = 0, Sp = 0;                 // slot counts
   DevBuf d_ex, d_rd, d_splits, d_pu, d_ex_off, d_pu_off, d_split_cnt;
+  DevBuf d_ex_splits, d_ex_split_cnt;
 };
 
 struct Workspace {
   int C = 0;
   DevBuf B64, R64, U, V, H, Hb, X, X64, S;
-  DevBuf part_e, part_a, part_b, piece_part, inst, counters;
+  DevBuf part_e, part_a, part_b, piece_part, ex_piece_part, inst, counters;
   DevBuf coef;
   DevBuf ystage;  // device copy of host Y for host-buffer solves
 };
@@ -107,8 +111,15 @@ struct fe_plan {
   int32_t opt_check_every = 4; // iterations between host convergence checks
   int32_t opt_max_rounds = 8;  // mixed-precision refinement rounds
   int32_t opt_unroll = 0;      // reserved
-  double opt_inner_rho = 1e-6;
+  double opt_inner_rho = 1e-8;
   double opt_inner_theta = 0.5;
+  int32_t opt_fuse = 0;        // reduce the primary FE inside the expand
+  int32_t opt_ex_variant = -1; // expand kernel variant (-1: tuned default)
+  int32_t opt_seg_variant = -1; // segsum kernel variant (-1: tuned default)
+  int32_t opt_autotune = 1;     // time the variants on first use of a tile shape
+  // tuned variants per (tile width C, element size): {expand, segsum}
+  std::map<std::pair<int, int>, std::pair<int, int>> tuned;
+  std::string tune_signature;   // plan shape, key of the persisted tuning cache
 
   std::map<int, std::unique_ptr<fe::ItemSet>> items;  // by C
   fe::Workspace ws;

@@ -13,6 +13,16 @@
 
 namespace fe {
 
+// Kernel coefficients of a stopped instance: the expand keeps U
+// (U <- 0*(A v) + 1*U) and the P-side update is skipped (upd_mode 0, no v).
+__device__ static void deactivate(Inst& s) {
+  s.active = 0;
+  s.ex_av = 0.0;
+  s.ex_au = 1.0;
+  s.upd_mode = 0;
+  s.do_v = 0;
+}
+
 __device__ static void lsmr_test(Inst& s) {
   // src/utils/lsmr.jl:188-215
   const double test1 = s.normr / s.normb;
@@ -123,6 +133,7 @@ __device__ static void lsmr_init(Inst& s, int init_mode) {
   s.active = (s.normAr != 0.0 && s.maxiter > 0 && !s.skip_lsmr) ? 1 : 0;
   s.ex_av = s.s_v;
   s.ex_au = -s.alpha * s.u_scale;
+  if (!s.active) deactivate(s);
 }
 
 __global__ void __launch_bounds__(kScalarThreads) k_scalar(ScalarArgs a) {
@@ -206,7 +217,7 @@ __global__ void __launch_bounds__(kScalarThreads) k_scalar(ScalarArgs a) {
         lsmr_test(s);
         s.pending = 0;
         if (s.istop) {
-          s.active = 0;
+          deactivate(s);
           break;
         }
       }
@@ -251,13 +262,13 @@ __global__ void __launch_bounds__(kScalarThreads) k_scalar(ScalarArgs a) {
       if (conv) {
         s.converged = 1;
         s.outer_active = 0;
-        s.active = 0;
+        deactivate(s);
         break;
       }
       if (s.iter_total >= s.maxiter_total || s.outer_rounds >= s.max_rounds) {
         s.converged = 0;
         s.outer_active = 0;
-        s.active = 0;
+        deactivate(s);
         break;
       }
       s.outer_rounds += 1;

@@ -1,0 +1,785 @@
+// fe_solve_impl.cuh -- solve drivers of the fixed-effects LSMR hot path.
+// Included by one translation unit per column-tile width (fe_tile_c*.cu),
+// which instantiates solve_tile_C<C>; fe_solve.cu dispatches on C.
+//
+// Replaces, for one plan, the bodies of
+//   solve_residuals!(r, feM)     src/AbstractFixedEffectSolver.jl:49-68
+//   solve_residuals!(xs, feM)    src/AbstractFixedEffectSolver.jl:74-97
+//   solve_coefficients!(r, feM)  src/AbstractFixedEffectSolver.jl:147-160
+// with all columns of a tile (and all problems of a batch plan) advanced as
+// one batched LSMR; every instance has its own FP64 scalars and stops on its
+// own test.
+//
+// Precision modes:
+//   FP64  : bulk FP64, the plain form of the reference's Float64 solver.
+//   FP32  : bulk FP32 (FP64 scalars), no refinement.
+//   MIXED : FP32 inner LSMR solves on correction problems; the residual
+//           r = b - A x and g = A'r are recomputed in FP64 between them and
+//           tested with the reference's tests (FP64 iterative refinement).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#pragma once
+#include "fe_kernels.cuh"
+#include "fe_plan.h"
+#include "fe_solve.h"
+
+namespace fe {
+
+// ---------------------------------------------------------------------------
+// load / unload / coefficient kernels
+// ---------------------------------------------------------------------------
+// B[q][j] = y[i][col0 + j] * sqrt(w_i) with q the sorted position of i
+// (src/AbstractFixedEffectSolver.jl:50-55).  A CTA stages kLoadRows
+// observations x C columns in shared memory: the reads are coalesced along
+// observations (column-major input), the writes are whole contiguous rows.
+constexpr int kLoadRows = 64;
+template <typename TY>
+__global__ void __launch_bounds__(256) k_load(const TY* __restrict__ Y, int64_t ld, int64_t col0,
+                                              int ncols, int C, const int32_t* __restrict__ dst,
+                                              const double* __restrict__ sw,
+                                              double* __restrict__ B, int64_t N) {
+  __shared__ double tile[kLoadRows][33];
+  __shared__ int64_t rows[kLoadRows];
+  const int64_t i0 = (int64_t)blockIdx.x * kLoadRows;
+  for (int e = threadIdx.x; e < kLoadRows * C; e += blockDim.x) {
+    const int j = e / kLoadRows, r = e - j * kLoadRows;
+    const int64_t i = i0 + r;
+    double v = 0.0;
+    if (i < N && j < ncols) v = (double)Y[i + (col0 + j) * ld] * (sw ? sw[i] : 1.0);
+    tile[r][j] = v;
+  }
+  for (int r = threadIdx.x; r < kLoadRows; r += blockDim.x)
+    rows[r] = (i0 + r < N) ? (int64_t)dst[i0 + r] : -1;
+  __syncthreads();
+  for (int e = threadIdx.x; e < kLoadRows * C; e += blockDim.x) {
+    const int r = e / C, j = e - r * C;
+    const int64_t q = rows[r];
+    if (q >= 0) B[q * C + j] = tile[r][j];
+  }
+}
+
+// y[i][col0 + j] = R[q][j] / sqrt(w_i)  (src/AbstractFixedEffectSolver.jl:62-66):
+// whole rows in, coalesced columns out.
+template <typename TY>
+__global__ void __launch_bounds__(256) k_unload(const double* __restrict__ R, int64_t ld,
+                                                int64_t col0, int ncols, int C,
+                                                const int32_t* __restrict__ dst,
+                                                const double* __restrict__ sw,
+                                                TY* __restrict__ Y, int64_t N) {
+  __shared__ double tile[kLoadRows][33];
+  __shared__ int64_t rows[kLoadRows];
+  const int64_t i0 = (int64_t)blockIdx.x * kLoadRows;
+  for (int r = threadIdx.x; r < kLoadRows; r += blockDim.x)
+    rows[r] = (i0 + r < N) ? (int64_t)dst[i0 + r] : -1;
+  __syncthreads();
+  for (int e = threadIdx.x; e < kLoadRows * C; e += blockDim.x) {
+    const int r = e / C, j = e - r * C;
+    const int64_t q = rows[r];
+    tile[r][j] = q >= 0 ? R[q * C + j] : 0.0;
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < kLoadRows * ncols; e += blockDim.x) {
+    const int j = e / kLoadRows, r = e - j * kLoadRows;
+    const int64_t i = i0 + r;
+    if (i < N) Y[i + (col0 + j) * ld] = (TY)(tile[r][j] / (sw ? sw[i] : 1.0));
+  }
+}
+
+// coefficients in original units: x_k .* scale_k  (src/AbstractFixedEffectSolver.jl:155-157)
+template <typename TX>
+__global__ void k_coefs(const TX* __restrict__ X, int C, int j, int64_t base, int64_t n,
+                        const double* __restrict__ scale, double* __restrict__ out) {
+  const int64_t l = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (l < n) out[l] = (double)X[(base + l) * C + j] * scale[l];
+}
+
+static inline unsigned grid1(int64_t n, int b = 256) { return (unsigned)((n + b - 1) / b); }
+
+// ---------------------------------------------------------------------------
+// profiling: CUDA events around launches on the plan's stream
+// ---------------------------------------------------------------------------
+struct ProfScope {
+  fe_plan* pl;
+  const char* name;
+  double bytes;
+  cudaEvent_t a = nullptr, b = nullptr;
+  ProfScope(fe_plan* p, const char* n, double by) : pl(p), name(n), bytes(by) {
+    if (!pl->prof.on) return;
+    a = take();
+    b = take();
+    cudaEventRecord(a, pl->stream);
+  }
+  cudaEvent_t take() {
+    if (!pl->prof.pool.empty()) {
+      cudaEvent_t e = pl->prof.pool.back();
+      pl->prof.pool.pop_back();
+      return e;
+    }
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    return e;
+  }
+  ~ProfScope() {
+    if (!pl->prof.on) return;
+    cudaEventRecord(b, pl->stream);
+    pl->prof.pending.push_back({name, {a, b}});
+    pl->prof.bytes_per_launch[name] = bytes;
+  }
+};
+
+
+// ---------------------------------------------------------------------------
+// solve context for one tile
+// ---------------------------------------------------------------------------
+struct Ctx {
+  fe_plan* pl;
+  ItemSet* its;
+  FeDev d;
+  int C;
+  cudaStream_t s;
+  Inst* inst;
+  int32_t* counters;
+  int32_t* h_counters;
+  int n_inst;
+  double* part_e;
+  double* part_a;
+  double* part_b;
+  double* piece;
+  double* ex_piece;
+  void* S;
+};
+
+// Kernel variants (unroll depth = row slots per lane group per step, and
+// whether the next step's indices are prefetched).  Variant 0 is the default;
+// fe_plan_set_option(FE_OPT_EXPAND_VARIANT / FE_OPT_SEGSUM_VARIANT) selects
+// another, which is how the tuner compares them.
+//   expand: 0 U=2 PF, 1 U=4 PF, 2 U=2 no-PF, 3 U=4 no-PF
+//   segsum: 0 U=8 no-PF, 1 U=4 PF, 2 U=8 PF, 3 U=4 no-PF
+constexpr int kVariants = 4;
+template <int C> struct Tune {
+  static constexpr int kPU = 4;
+};
+// tuning state of the tile being solved
+struct TuneSel {
+  int ex = -1, seg = -1;
+};
+inline TuneSel& cur_tune() {
+  static thread_local TuneSel t;
+  return t;
+}
+inline int pick_ex(const fe_plan* pl) {
+  return pl->opt_ex_variant >= 0 ? pl->opt_ex_variant : (cur_tune().ex >= 0 ? cur_tune().ex : 0);
+}
+inline int pick_seg(const fe_plan* pl) {
+  return pl->opt_seg_variant >= 0 ? pl->opt_seg_variant : (cur_tune().seg >= 0 ? cur_tune().seg : 0);
+}
+template <typename T, int C> constexpr int vec_of() { return Shape<T, C>::VEC; }
+
+template <int KB, int U, bool PF, typename TA, int C, class Tab, class Epi>
+static void expand_kbu(Ctx& c, Tab tab, Epi epi, double* part, void* fuse_sum) {
+  const unsigned grid = (unsigned)(c.its->ex.size() / kWarps);
+  const ExpandItem* items = c.its->d_ex.as<ExpandItem>();
+  const int64_t n = (int64_t)c.its->ex.size();
+  FuseArgs fz{static_cast<double*>(fuse_sum), c.its->d_ex_splits.as<SplitLevel>(), c.ex_piece,
+              c.its->ex_n_pieces, c.its->d_ex_split_cnt.as<int32_t>()};
+  if (fuse_sum)
+    k_expand<TA, C, U, KB, true, PF, Tab, Epi><<<grid, kThreads, 0, c.s>>>(c.d, items, n, tab, epi,
+                                                                          part, c.its->Se, fz);
+  else
+    k_expand<TA, C, U, KB, false, PF, Tab, Epi><<<grid, kThreads, 0, c.s>>>(c.d, items, n, tab, epi,
+                                                                           part, c.its->Se, fz);
+}
+
+template <int KB, typename TA, int C, class Tab, class Epi>
+static void expand_kb(Ctx& c, Tab tab, Epi epi, double* part, void* fuse_sum) {
+  const int var = pick_ex(c.pl);
+  switch (var) {
+    case 1: expand_kbu<KB, 4, true, TA, C>(c, tab, epi, part, fuse_sum); break;
+    case 2: expand_kbu<KB, 2, false, TA, C>(c, tab, epi, part, fuse_sum); break;
+    case 3: expand_kbu<KB, 4, false, TA, C>(c, tab, epi, part, fuse_sum); break;
+    default: expand_kbu<KB, 2, true, TA, C>(c, tab, epi, part, fuse_sum); break;
+  }
+}
+
+// fuse_sum: when non-null, the expand also reduces the primary FE into this
+// [P][C] sum slab (TA-typed), and the following segsum skips that FE.
+template <typename TA, int C, class Tab, class Epi>
+static int launch_expand(Ctx& c, Tab tab, Epi epi, double* part, const char* name, double bytes,
+                         void* fuse_sum = nullptr) {
+  ProfScope ps(c.pl, name, bytes);
+  if (c.d.K <= 2)
+    expand_kb<2, TA, C>(c, tab, epi, part, fuse_sum);
+  else if (c.d.K <= 4)
+    expand_kb<4, TA, C>(c, tab, epi, part, fuse_sum);
+  else
+    expand_kb<kMaxFE, TA, C>(c, tab, epi, part, fuse_sum);
+  FE_CK(cudaGetLastError());
+  return 0;
+}
+
+// all_fes: reduce every FE; otherwise skip the primary (reduced by a fused
+// expand).
+template <typename TA, int C, class Load>
+static int launch_segsum(Ctx& c, Load ld, TA* out, const char* name, double bytes,
+                         bool all_fes = true) {
+  const int64_t n = all_fes ? (int64_t)c.its->rd.size() : c.its->rd_np;
+  if (n == 0) return 0;
+  ProfScope ps(c.pl, name, bytes);
+  const unsigned grid = (unsigned)((n + kWarps - 1) / kWarps);
+  const ReduceItem* items = c.its->d_rd.as<ReduceItem>();
+  const SplitLevel* sp = c.its->d_splits.as<SplitLevel>();
+  int32_t* cnt = c.its->d_split_cnt.as<int32_t>();
+  const int var = pick_seg(c.pl);
+  switch (var) {
+    case 1:
+      k_segsum<TA, C, 4, true, Load><<<grid, kThreads, 0, c.s>>>(c.d, items, n, ld, out, sp, c.piece,
+                                                                 c.its->n_pieces, cnt);
+      break;
+    case 2:
+      k_segsum<TA, C, 8, true, Load><<<grid, kThreads, 0, c.s>>>(c.d, items, n, ld, out, sp, c.piece,
+                                                                 c.its->n_pieces, cnt);
+      break;
+    case 3:
+      k_segsum<TA, C, 4, false, Load><<<grid, kThreads, 0, c.s>>>(c.d, items, n, ld, out, sp, c.piece,
+                                                                  c.its->n_pieces, cnt);
+      break;
+    default:
+      k_segsum<TA, C, 8, false, Load><<<grid, kThreads, 0, c.s>>>(c.d, items, n, ld, out, sp, c.piece,
+                                                                  c.its->n_pieces, cnt);
+      break;
+  }
+  FE_CK(cudaGetLastError());
+  return 0;
+}
+
+template <int C, class Epi>
+static int launch_pupdate(Ctx& c, const typename Epi::TS* S, Epi epi, double* pa, double* pb,
+                          const char* name, double bytes) {
+  ProfScope ps(c.pl, name, bytes);
+  const unsigned grid = (unsigned)(c.its->pu.size() / kWarps);
+  k_pupdate<C, Tune<C>::kPU, Epi><<<grid, kThreads, 0, c.s>>>(
+      c.d, c.its->d_pu.as<PItem>(), (int64_t)c.its->pu.size(), S, epi, pa, pb, c.its->Sp);
+  FE_CK(cudaGetLastError());
+  return 0;
+}
+
+static int launch_scalar_phase(Ctx& c, int phase, int init_mode) {
+  ProfScope ps(c.pl, "scalar", 0.0);
+  ScalarArgs a;
+  memset(&a, 0, sizeof(a));
+  a.inst = c.inst;
+  a.C = c.C;
+  a.phase = phase;
+  a.init_mode = init_mode;
+  a.counters = c.counters;
+  a.off0 = c.its->d_ex_off.as<int64_t>();
+  a.S0 = c.its->Se;
+  a.off1 = c.its->d_pu_off.as<int64_t>();
+  a.S1 = c.its->Sp;
+  switch (phase) {
+    case PH_INIT_BETA:
+    case PH_BETA:
+      a.part0 = c.part_e;
+      break;
+    case PH_INIT_ALPHA:
+    case PH_ALPHA:
+      a.part1 = c.part_a;
+      a.part2 = c.part_b;
+      break;
+    case PH_OUTER:
+      a.part0 = c.part_e;
+      a.part1 = c.part_a;
+      a.part2 = c.part_b;
+      break;
+    default:
+      break;
+  }
+  launch_scalar(a, c.n_inst, c.s);
+  FE_CK(cudaGetLastError());
+  return 0;
+}
+
+static int read_counter(Ctx& c, int idx, int32_t* out) {
+  FE_CK(cudaMemcpyAsync(c.h_counters + idx, c.counters + idx, sizeof(int32_t),
+                        cudaMemcpyDeviceToHost, c.s));
+  FE_CK(cudaStreamSynchronize(c.s));
+  *out = c.h_counters[idx];
+  return 0;
+}
+
+// The primary FE is reduced inside the expand for tiles of 4+ columns; for
+// narrower tiles the extra scan costs more than the pass it saves.
+static bool use_fuse(const fe_plan* pl, int C) { return pl->opt_fuse != 0 && C >= 4; }
+
+// algorithmic bytes per launch (the roofline numerators): every index vector
+// and observation row once, every coefficient-table row once
+struct Bytes {
+  double expand, segsum, pupdate, resid64, segsum64, grad64;
+};
+static Bytes alg_bytes(const fe_plan* pl, int C, int sT) {
+  Bytes b{};
+  const bool fuse = use_fuse(pl, C);
+  const double N = (double)pl->N;
+  double P = 0, Pprim = 0, pos = 0, posmeta = 0, cw = 0, cw64 = 0, cwp = 0, cwp64 = 0;
+  for (int k = 0; k < pl->K; ++k) {
+    P += (double)pl->nlev[k];
+    const bool has_cw = pl->weighted || pl->interacted[k];
+    if (has_cw) {
+      cw += N * sT;
+      cw64 += N * 8.0;
+    }
+    if (fuse && k == pl->primary) {
+      Pprim = (double)pl->nlev[k];
+      continue;  // reduced inside the expand
+    }
+    pos += (double)pl->seg_len[k];
+    posmeta += (double)pl->seg_len[k] * (4.0 + (pl->perm_identity[k] ? 0.0 : 4.0));
+    if (has_cw) {
+      cwp += (double)pl->seg_len[k] * sT;
+      cwp64 += (double)pl->seg_len[k] * 8.0;
+    }
+  }
+  const double refs = N * 4.0 * pl->K;
+  b.expand = refs + cw + 2.0 * N * C * sT + P * C * sT + Pprim * C * sT;
+  b.segsum = posmeta + cwp + pos * C * sT + (P - Pprim) * C * sT;
+  b.pupdate = 9.0 * P * C * sT;
+  b.resid64 = refs + cw64 + N * C * (8.0 + 8.0 + 4.0) + P * C * 12.0 + Pprim * C * 8.0;
+  b.segsum64 = posmeta + cwp64 + pos * C * 8.0 + (P - Pprim) * C * 8.0;
+  b.grad64 = P * C * (8.0 + 4.0 + 8.0 + 4.0 + 8.0);
+  return b;
+}
+
+static int prepare(fe_plan* pl, int C, int sT, bool mixed, Ctx& c) {
+  ItemSet* its = nullptr;
+  int st = plan_items(pl, C, &its);
+  if (st) return st;
+  Workspace& w = pl->ws;
+  const size_t N = (size_t)std::max<int64_t>(pl->N, 1), P = (size_t)pl->P;
+  const size_t nC = (size_t)C;
+  if ((st = w.B64.ensure(N * nC * 8))) return st;
+  if ((st = w.R64.ensure(N * nC * 8))) return st;
+  if ((st = w.U.ensure(N * nC * (size_t)sT))) return st;
+  if ((st = w.V.ensure(P * nC * (size_t)sT))) return st;
+  if ((st = w.H.ensure(P * nC * (size_t)sT))) return st;
+  if ((st = w.Hb.ensure(P * nC * (size_t)sT))) return st;
+  if ((st = w.X.ensure(P * nC * (size_t)sT))) return st;
+  if (mixed && (st = w.X64.ensure(P * nC * 8))) return st;
+  if ((st = w.part_e.ensure((size_t)std::max<int64_t>(its->Se, 1) * nC * 8))) return st;
+  if ((st = w.part_a.ensure((size_t)std::max<int64_t>(its->Sp, 1) * nC * 8))) return st;
+  if ((st = w.part_b.ensure((size_t)std::max<int64_t>(its->Sp, 1) * nC * 8))) return st;
+  if ((st = w.S.ensure(P * nC * 8))) return st;
+  if ((st = w.piece_part.ensure((size_t)std::max<int64_t>(its->n_pieces, 1) * nC * 8))) return st;
+  if ((st = w.ex_piece_part.ensure((size_t)std::max<int64_t>(its->ex_n_pieces, 1) * nC * 8))) return st;
+  if ((st = w.inst.ensure((size_t)pl->nprob * nC * sizeof(Inst)))) return st;
+  if ((st = w.counters.ensure(64))) return st;
+  if (!pl->host_pinned) FE_CK(cudaMallocHost(&pl->host_pinned, 64));
+  c.pl = pl;
+  c.its = its;
+  c.d = pl->dev;
+  c.d.C = C;
+  c.C = C;
+  c.s = pl->stream;
+  c.inst = w.inst.as<Inst>();
+  c.counters = w.counters.as<int32_t>();
+  c.h_counters = static_cast<int32_t*>(pl->host_pinned);
+  c.n_inst = pl->nprob * C;
+  c.part_e = w.part_e.as<double>();
+  c.part_a = w.part_a.as<double>();
+  c.part_b = w.part_b.as<double>();
+  c.piece = w.piece_part.as<double>();
+  c.ex_piece = w.ex_piece_part.as<double>();
+  c.S = w.S.p;
+  // coefficient-side slabs start at zero (levels without observations and
+  // the null levels are never written afterwards)
+  FE_CK(cudaMemsetAsync(w.V.p, 0, P * nC * (size_t)sT, c.s));
+  FE_CK(cudaMemsetAsync(w.H.p, 0, P * nC * (size_t)sT, c.s));
+  FE_CK(cudaMemsetAsync(w.Hb.p, 0, P * nC * (size_t)sT, c.s));
+  FE_CK(cudaMemsetAsync(w.X.p, 0, P * nC * (size_t)sT, c.s));
+  if (mixed) FE_CK(cudaMemsetAsync(w.X64.p, 0, P * nC * 8, c.s));
+  FE_CK(cudaMemsetAsync(w.S.p, 0, P * nC * 8, c.s));
+  FE_CK(cudaMemsetAsync(c.counters, 0, 64, c.s));
+  return 0;
+}
+
+static int load_tile(fe_plan* pl, Ctx& c, const SolveReq& rq, int64_t col0, int ncols) {
+  const int64_t N = pl->N;
+  if (N == 0) return 0;
+  const double* sw = pl->weighted ? pl->d_sw_orig.as<double>() : nullptr;
+  ProfScope ps(pl, "load", (double)N * ncols * (rq.dtype == 0 ? 8 : 4) + (double)N * c.C * 8);
+  if (rq.dtype == 0)
+    k_load<double><<<grid1(N, kLoadRows), 256, 0, c.s>>>((const double*)rq.Y, rq.ld, col0, ncols, c.C,
+                                                pl->d_obs_dst.as<int32_t>(), sw,
+                                                pl->ws.B64.as<double>(), N);
+  else
+    k_load<float><<<grid1(N, kLoadRows), 256, 0, c.s>>>((const float*)rq.Y, rq.ld, col0, ncols, c.C,
+                                               pl->d_obs_dst.as<int32_t>(), sw,
+                                               pl->ws.B64.as<double>(), N);
+  FE_CK(cudaGetLastError());
+  return 0;
+}
+
+static int unload_tile(fe_plan* pl, Ctx& c, const SolveReq& rq, int64_t col0, int ncols) {
+  const int64_t N = pl->N;
+  if (N == 0) return 0;
+  const double* sw = pl->weighted ? pl->d_sw_orig.as<double>() : nullptr;
+  ProfScope ps(pl, "unload", (double)N * ncols * (rq.dtype == 0 ? 8 : 4) + (double)N * c.C * 8);
+  if (rq.dtype == 0)
+    k_unload<double><<<grid1(N, kLoadRows), 256, 0, c.s>>>(pl->ws.R64.as<double>(), rq.ld, col0, ncols, c.C,
+                                                  pl->d_obs_dst.as<int32_t>(), sw, (double*)rq.Y, N);
+  else
+    k_unload<float><<<grid1(N, kLoadRows), 256, 0, c.s>>>(pl->ws.R64.as<double>(), rq.ld, col0, ncols, c.C,
+                                                 pl->d_obs_dst.as<int32_t>(), sw, (float*)rq.Y, N);
+  FE_CK(cudaGetLastError());
+  return 0;
+}
+
+static void init_insts(fe_plan* pl, const SolveReq& rq, int C, int ncols, std::vector<Inst>& h) {
+  h.assign((size_t)pl->nprob * C, Inst{});
+  const bool mixed = rq.precision == 1;
+  const int64_t mi = rq.residuals ? rq.maxiter - 1 : rq.maxiter;
+  for (int p = 0; p < pl->nprob; ++p)
+    for (int j = 0; j < C; ++j) {
+      Inst& s = h[(size_t)p * C + j];
+      memset(&s, 0, sizeof(s));
+      s.ctol = 1e-8;  // 1/conlim, conlim = 1e8 (src/utils/lsmr.jl:47)
+      s.skip_lsmr = (rq.residuals && pl->prob_nfe[p] <= 1) ? 1 : 0;
+      if (mixed) {
+        s.atol = 0.0;
+        s.btol = 0.0;
+        s.tol_a = rq.tol;
+        s.tol_b = rq.tol;
+        s.maxiter_total = mi;
+        s.maxiter = mi;
+        s.inner_theta_tol = pl->opt_inner_theta * rq.tol;
+        s.inner_rho = pl->opt_inner_rho;
+        s.outer_active = j < ncols ? 1 : 0;
+        s.converged = j < ncols ? 0 : 1;
+        s.max_rounds = pl->opt_max_rounds;
+      } else {
+        s.atol = rq.tol;
+        s.btol = rq.tol;
+        s.maxiter = mi;
+      }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// autotuner: the expand and segsum variants of the LSMR loop timed on this
+// plan's own index data (values are irrelevant to the timing: U and V are
+// zeroed scratch), best of two launches each; the winner is kept per (C, T)
+// and persisted through tune_cache_{load,store} (fe_solve.cu).
+// ---------------------------------------------------------------------------
+bool tune_cache_load(fe_plan* pl, int C, int sT, int* ex, int* seg);
+void tune_cache_store(fe_plan* pl, int C, int sT, int ex, int seg);
+
+template <typename T, int C>
+static int autotune(fe_plan* pl, Ctx& c) {
+  const std::pair<int, int> key(C, (int)sizeof(T));
+  auto f = pl->tuned.find(key);
+  if (f != pl->tuned.end()) {
+    cur_tune().ex = f->second.first;
+    cur_tune().seg = f->second.second;
+    return 0;
+  }
+  int ex = 0, seg = 0;
+  if (tune_cache_load(pl, C, (int)sizeof(T), &ex, &seg)) {
+    pl->tuned[key] = {ex, seg};
+    cur_tune().ex = ex;
+    cur_tune().seg = seg;
+    return 0;
+  }
+  if (!pl->opt_autotune) {
+    cur_tune().ex = 0;
+    cur_tune().seg = 0;
+    return 0;
+  }
+  Workspace& w = pl->ws;
+  const size_t N = (size_t)pl->N, P = (size_t)pl->P;
+  FE_CK(cudaMemsetAsync(w.U.p, 0, N * C * sizeof(T), c.s));
+  std::vector<Inst> h((size_t)pl->nprob * C);
+  for (Inst& s : h) {
+    memset(&s, 0, sizeof(s));
+    s.active = 1;
+    s.ex_av = 1.0;
+    s.ex_au = 0.5;
+  }
+  FE_CK(cudaMemcpyAsync(c.inst, h.data(), h.size() * sizeof(Inst), cudaMemcpyHostToDevice, c.s));
+  (void)P;
+  cudaEvent_t e0, e1;
+  FE_CK(cudaEventCreate(&e0));
+  FE_CK(cudaEventCreate(&e1));
+  const bool prof = pl->prof.on;
+  pl->prof.on = false;
+  const int save_ex = pl->opt_ex_variant, save_seg = pl->opt_seg_variant;
+  EpiExpandLsmr<T, vec_of<T, C>()> ee{};
+  ee.U = w.U.as<T>();
+  ee.inst = c.inst;
+  float best_e = 1e30f, best_s = 1e30f;
+  int st = 0;
+  for (int v = 0; v < kVariants && !st; ++v) {
+    pl->opt_ex_variant = v;
+    float ms = 1e30f;
+    for (int rep = 0; rep < 3 && !st; ++rep) {
+      cudaEventRecord(e0, c.s);
+      st = launch_expand<T, C>(c, TabOne<T, T, vec_of<T, C>()>{w.V.as<T>()}, ee, c.part_e, "tune", 0.0);
+      cudaEventRecord(e1, c.s);
+      cudaEventSynchronize(e1);
+      float t = 0.f;
+      cudaEventElapsedTime(&t, e0, e1);
+      if (rep > 0) ms = std::min(ms, t);
+    }
+    if (ms < best_e) {
+      best_e = ms;
+      ex = v;
+    }
+  }
+  for (int v = 0; v < kVariants && !st; ++v) {
+    pl->opt_seg_variant = v;
+    float ms = 1e30f;
+    for (int rep = 0; rep < 3 && !st; ++rep) {
+      cudaEventRecord(e0, c.s);
+      st = launch_segsum<T, C>(c, LoadIn<T, T, vec_of<T, C>()>{w.U.as<T>()}, static_cast<T*>(c.S), "tune",
+                               0.0, !use_fuse(pl, C));
+      cudaEventRecord(e1, c.s);
+      cudaEventSynchronize(e1);
+      float t = 0.f;
+      cudaEventElapsedTime(&t, e0, e1);
+      if (rep > 0) ms = std::min(ms, t);
+    }
+    if (ms < best_s) {
+      best_s = ms;
+      seg = v;
+    }
+  }
+  pl->opt_ex_variant = save_ex;
+  pl->opt_seg_variant = save_seg;
+  pl->prof.on = prof;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (st) return st;
+  // the tuning launches wrote scratch values into S and the item counters are
+  // back at zero (every split level completed); clear S for the solve
+  FE_CK(cudaMemsetAsync(c.S, 0, P * C * 8, c.s));
+  pl->tuned[key] = {ex, seg};
+  tune_cache_store(pl, C, (int)sizeof(T), ex, seg);
+  cur_tune().ex = ex;
+  cur_tune().seg = seg;
+  return 0;
+}
+
+// ---------------------------------------------------------------------------
+// coefficient download (solve_coefficients!)
+// ---------------------------------------------------------------------------
+template <typename TX>
+static int download_coefs(fe_plan* pl, Ctx& c, const TX* X, const SolveReq& rq) {
+  Workspace& w = pl->ws;
+  for (int k = 0; k < pl->K; ++k) {
+    const int64_t n = pl->nlev[k];
+    if (!n) continue;
+    int st = w.coef.ensure((size_t)n * 8);
+    if (st) return st;
+    k_coefs<TX><<<grid1(n), 256, 0, c.s>>>(X, c.C, 0, pl->lev_base[k], n,
+                                             pl->d_scale_d[k].as<double>(), w.coef.as<double>());
+    FE_CK(cudaGetLastError());
+    FE_CK(cudaMemcpyAsync(rq.coefs[k], w.coef.p, (size_t)n * 8, cudaMemcpyDeviceToHost, c.s));
+    FE_CK(cudaStreamSynchronize(c.s));
+  }
+  return 0;
+}
+
+// ---------------------------------------------------------------------------
+// plain LSMR (bulk type T) on one tile
+// ---------------------------------------------------------------------------
+template <typename T, int C>
+static int solve_plain_tile(fe_plan* pl, const SolveReq& rq, int64_t col0, int ncols,
+                            std::vector<Inst>& out) {
+  Ctx c;
+  int st = prepare(pl, C, (int)sizeof(T), false, c);
+  if (st) return st;
+  if ((st = autotune<T, C>(pl, c))) return st;
+  Workspace& w = pl->ws;
+  const Bytes by = alg_bytes(pl, C, (int)sizeof(T));
+  std::vector<Inst> h;
+  init_insts(pl, rq, C, ncols, h);
+  FE_CK(cudaMemcpyAsync(c.inst, h.data(), h.size() * sizeof(Inst), cudaMemcpyHostToDevice, c.s));
+  if ((st = load_tile(pl, c, rq, col0, ncols))) return st;
+  T* U = w.U.as<T>();
+  T* V = w.V.as<T>();
+  T* X = w.X.as<T>();
+  double* B64 = w.B64.as<double>();
+  double* S64 = static_cast<double*>(c.S);
+  T* ST = static_cast<T*>(c.S);
+  // warm start x = A'b (src/AbstractFixedEffectSolver.jl:56); solve_coefficients! starts at 0
+  if (rq.residuals) {
+    if ((st = launch_segsum<double, C>(c, LoadIn<double, double, vec_of<double, C>()>{B64}, S64, "segsum_warm", 0.0)))
+      return st;
+    if ((st = launch_pupdate<C>(c, S64, PEpiStoreX<T, vec_of<double, C>()>{X, true}, nullptr, nullptr, "pupdate_warm", 0.0)))
+      return st;
+  }
+  // u = b - A x, beta (lsmr.jl:63-64)
+  const bool fuse = use_fuse(pl, C);
+  void* fs = fuse ? c.S : nullptr;
+  if ((st = launch_expand<T, C>(c, TabOne<T, T, vec_of<T, C>()>{X},
+                                EpiBminusAx<T, T, vec_of<T, C>()>{B64, U, nullptr, c.inst, 0}, c.part_e,
+                                "expand_init", by.expand, fs)))
+    return st;
+  if ((st = launch_scalar_phase(c, PH_INIT_BETA, 0))) return st;
+  PEpiLsmr<T, vec_of<T, C>()> pe{};
+  pe.V = V;
+  pe.H = w.H.as<T>();
+  pe.Hb = w.Hb.as<T>();
+  pe.X = X;
+  pe.inst = c.inst;
+  if ((st = launch_segsum<T, C>(c, LoadIn<T, T, vec_of<T, C>()>{U}, ST, "segsum", by.segsum, !fuse)))
+    return st;
+  if ((st = launch_pupdate<C>(c, ST, pe, c.part_a, c.part_b, "pupdate", by.pupdate))) return st;
+  if ((st = launch_scalar_phase(c, PH_INIT_ALPHA, 1))) return st;
+  int32_t nact = 0;
+  if ((st = read_counter(c, 0, &nact))) return st;
+  EpiExpandLsmr<T, vec_of<T, C>()> ee{};
+  ee.U = U;
+  ee.inst = c.inst;
+  const int64_t cap = std::max<int64_t>(rq.maxiter, 1) + 2;
+  for (int64_t it = 1; nact > 0 && it <= cap; ++it) {
+    if ((st = launch_expand<T, C>(c, TabOne<T, T, vec_of<T, C>()>{V}, ee, c.part_e, "expand", by.expand,
+                                  fs)))
+      return st;
+    if ((st = launch_scalar_phase(c, PH_BETA, 0))) return st;
+    if ((st = launch_segsum<T, C>(c, LoadIn<T, T, vec_of<T, C>()>{U}, ST, "segsum", by.segsum, !fuse)))
+      return st;
+    if ((st = launch_pupdate<C>(c, ST, pe, c.part_a, c.part_b, "pupdate", by.pupdate))) return st;
+    if ((st = launch_scalar_phase(c, PH_ALPHA, 0))) return st;
+    if (it % pl->opt_check_every == 0 || it == cap) {
+      if ((st = read_counter(c, 0, &nact))) return st;
+    }
+  }
+  if (rq.residuals) {
+    // r = b - A x (src/AbstractFixedEffectSolver.jl:62)
+    if ((st = launch_expand<T, C>(c, TabOne<T, T, vec_of<T, C>()>{X},
+                                  EpiBminusAx<double, T, vec_of<T, C>()>{B64, w.R64.as<double>(), nullptr, c.inst, 0},
+                                  nullptr, "expand_final", by.expand)))
+      return st;
+    if ((st = unload_tile(pl, c, rq, col0, ncols))) return st;
+  }
+  out.resize(h.size());
+  FE_CK(cudaMemcpyAsync(out.data(), c.inst, h.size() * sizeof(Inst), cudaMemcpyDeviceToHost, c.s));
+  FE_CK(cudaStreamSynchronize(c.s));
+  if (!rq.residuals && rq.coefs) {
+    if ((st = download_coefs<T>(pl, c, X, rq))) return st;
+  }
+  return prof_flush(pl);
+}
+
+// ---------------------------------------------------------------------------
+// mixed precision: FP32 inner LSMR + FP64 iterative refinement, one tile
+// ---------------------------------------------------------------------------
+template <int C>
+static int solve_mixed_tile(fe_plan* pl, const SolveReq& rq, int64_t col0, int ncols,
+                            std::vector<Inst>& out) {
+  Ctx c;
+  int st = prepare(pl, C, 4, true, c);
+  if (st) return st;
+  if ((st = autotune<float, C>(pl, c))) return st;
+  Workspace& w = pl->ws;
+  const Bytes by = alg_bytes(pl, C, 4);
+  std::vector<Inst> h;
+  init_insts(pl, rq, C, ncols, h);
+  FE_CK(cudaMemcpyAsync(c.inst, h.data(), h.size() * sizeof(Inst), cudaMemcpyHostToDevice, c.s));
+  if ((st = load_tile(pl, c, rq, col0, ncols))) return st;
+  float* U = w.U.as<float>();
+  float* V = w.V.as<float>();
+  float* X = w.X.as<float>();
+  double* X64 = w.X64.as<double>();
+  double* B64 = w.B64.as<double>();
+  double* R64 = w.R64.as<double>();
+  double* S64 = static_cast<double*>(c.S);
+  float* S32 = static_cast<float*>(c.S);
+  if (rq.residuals) {
+    if ((st = launch_segsum<double, C>(c, LoadIn<double, double, vec_of<double, C>()>{B64}, S64, "segsum_warm", 0.0)))
+      return st;
+    if ((st = launch_pupdate<C>(c, S64, PEpiStoreX<double, vec_of<double, C>()>{X64, true}, nullptr, nullptr,
+                                "pupdate_warm", 0.0)))
+      return st;
+  }
+  PEpiLsmr<float, vec_of<float, C>()> pe{};
+  pe.V = V;
+  pe.H = w.H.as<float>();
+  pe.Hb = w.Hb.as<float>();
+  pe.X = X;
+  pe.inst = c.inst;
+  EpiExpandLsmr<float, vec_of<float, C>()> ee{};
+  ee.U = U;
+  ee.inst = c.inst;
+  PEpiGrad64<vec_of<double, C>()> pg{};
+  pg.V32 = V;
+  pg.X64 = X64;
+  pg.X32 = X;
+  pg.inst = c.inst;
+  const int64_t cap = std::max<int64_t>(rq.maxiter, 1) + 2;
+  int64_t total_it = 0;
+  const bool fuse = use_fuse(pl, C);
+  void* fs = fuse ? c.S : nullptr;
+  for (int round = 0; round <= pl->opt_max_rounds + 1; ++round) {
+    FE_CK(cudaMemsetAsync(c.counters + 1, 0, sizeof(int32_t), c.s));
+    // r = b - A (x64 + dx32) in FP64, with the FP32 copy as the next inner u
+    if ((st = launch_expand<double, C>(c, TabSum64<vec_of<double, C>()>{X64, X},
+                                       EpiBminusAx<double, double, vec_of<double, C>()>{B64, R64, U, c.inst, 2},
+                                       c.part_e, "resid64", by.resid64, fs)))
+      return st;
+    // g = A'r in FP64 (the next inner v), x64 += dx32, ||x64||
+    if ((st = launch_segsum<double, C>(c, LoadIn<double, double, vec_of<double, C>()>{R64}, S64, "segsum64",
+                                       by.segsum64, !fuse)))
+      return st;
+    if ((st = launch_pupdate<C>(c, S64, pg, c.part_a, c.part_b, "grad64", by.grad64))) return st;
+    if ((st = launch_scalar_phase(c, PH_OUTER, 0))) return st;
+    int32_t nout = 0;
+    if ((st = read_counter(c, 1, &nout))) return st;
+    if (nout == 0) break;
+    int32_t nact = nout;
+    for (int64_t it = 1; nact > 0 && total_it < cap; ++it, ++total_it) {
+      if ((st = launch_expand<float, C>(c, TabOne<float, float, vec_of<float, C>()>{V}, ee, c.part_e,
+                                        "expand", by.expand, fs)))
+        return st;
+      if ((st = launch_scalar_phase(c, PH_BETA, 0))) return st;
+      if ((st = launch_segsum<float, C>(c, LoadIn<float, float, vec_of<float, C>()>{U}, S32, "segsum",
+                                        by.segsum, !fuse)))
+        return st;
+      if ((st = launch_pupdate<C>(c, S32, pe, c.part_a, c.part_b, "pupdate", by.pupdate))) return st;
+      if ((st = launch_scalar_phase(c, PH_ALPHA, 0))) return st;
+      if (it % pl->opt_check_every == 0) {
+        if ((st = read_counter(c, 0, &nact))) return st;
+      }
+    }
+  }
+  if (rq.residuals) {
+    if ((st = unload_tile(pl, c, rq, col0, ncols))) return st;
+  }
+  out.resize(h.size());
+  FE_CK(cudaMemcpyAsync(out.data(), c.inst, h.size() * sizeof(Inst), cudaMemcpyDeviceToHost, c.s));
+  FE_CK(cudaStreamSynchronize(c.s));
+  if (!rq.residuals && rq.coefs) {
+    if ((st = download_coefs<double>(pl, c, X64, rq))) return st;
+  }
+  return prof_flush(pl);
+}
+
+template <int C>
+int solve_tile_C(fe_plan* pl, const SolveReq& rq, int64_t col0, int ncols,
+                        std::vector<Inst>& out) {
+  switch (rq.precision) {
+    case 0:
+      return solve_plain_tile<double, C>(pl, rq, col0, ncols, out);
+    case 2:
+      return solve_plain_tile<float, C>(pl, rq, col0, ncols, out);
+    default:
+      return solve_mixed_tile<C>(pl, rq, col0, ncols, out);
+  }
+}
+
+}  // namespace fe

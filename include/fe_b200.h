@@ -57,6 +57,13 @@ extern "C" {
 #define FE_OPT_MAX_ROUNDS 3  /* FP64 refinement rounds (FE_PREC_MIXED) */
 #define FE_OPT_PROFILE 4     /* 1: time every launch with CUDA events */
 #define FE_OPT_INNER_RHO 5   /* FP32 inner-solve floor (relative ||A'r|| drop) */
+#define FE_OPT_FUSE 6        /* 1: reduce the primary FE inside the expand (default 0) */
+#define FE_OPT_EXPAND_VARIANT 7 /* expand kernel variant 0..3, -1 = default */
+#define FE_OPT_SEGSUM_VARIANT 8 /* segsum kernel variant 0..3, -1 = default */
+#define FE_OPT_AUTOTUNE 9    /* 1 (default): time the kernel variants on the first
+                                solve of a tile shape; the choice is kept in the
+                                plan and in the tuning cache file
+                                ($FE_B200_TUNE_CACHE, "off" disables) */
 
 typedef struct fe_plan fe_plan;
 

@@ -1,5 +1,7 @@
 import json
+import os
 import sys
+import tempfile
 from pathlib import Path
 
 import pytest
@@ -12,6 +14,9 @@ import __graft_entry__ as graft  # noqa: E402
 
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA (B200) device")
+    # keep the kernel-variant tuning cache of the tests out of the user's home
+    os.environ.setdefault("FE_B200_TUNE_CACHE",
+                          os.path.join(tempfile.mkdtemp(prefix="fe_b200_tune_"), "tune.txt"))
 
 
 def cuda_available() -> bool:

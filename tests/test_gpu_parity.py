@@ -274,3 +274,43 @@ def test_zipf_split_levels(fe, oracle):
         feM.close()
         assert cvs.all()
         assert max(rel_err(R[:, j], R_o[:, j]) for j in range(2)) < REL
+
+
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_fused_primary_reduce_matches_unfused(fe, synth, oracle, prec):
+    # the primary FE reduced inside the expand (default) vs by the segsum
+    pb = synth.make(4, scale=0.0003, ncols=6)
+    fes = [fe.FixedEffect.from_refs(r, n, a) for r, n, a in zip(pb.refs, pb.nlev, pb.interaction)]
+    Y = np.asfortranarray(pb.Y.astype(np.float64))
+    R_o, _, _ = oracle.solve_residuals_cols(Y, pb.refs, pb.nlev, pb.interaction, pb.weights, tol=1e-8)
+    out = []
+    for fuse in (1, 0):
+        feM = fe.AbstractFixedEffectSolver(fes, pb.weights, "CUDA", np.float64, precision=prec)
+        feM.set_option(fe._lib.FE_OPT_FUSE, fuse)
+        R, its, cvs = feM.solve_residuals(Y.copy(), tol=1e-8)
+        feM.close()
+        assert cvs.all()
+        out.append(R)
+    for R in out:
+        assert max(rel_err(R[:, j], R_o[:, j]) for j in range(Y.shape[1])) < REL
+
+
+def test_autotuner_persists_choice(fe, synth, tmp_path, monkeypatch):
+    cache = tmp_path / "tune.txt"
+    monkeypatch.setenv("FE_B200_TUNE_CACHE", str(cache))
+    pb = synth.make(2, scale=0.002, ncols=8)
+    fes = [fe.FixedEffect.from_refs(r, n) for r, n in zip(pb.refs, pb.nlev)]
+    Y = np.asfortranarray(pb.Y.astype(np.float64))
+    feM = fe.AbstractFixedEffectSolver(fes, None, "CUDA", np.float32)
+    R1, _, _ = feM.solve_residuals(Y.copy(), tol=1e-8)
+    feM.close()
+    lines = cache.read_text().strip().splitlines()
+    assert len(lines) == 1
+    sig, C, sT, ex, seg = lines[0].split()
+    assert (int(C), int(sT)) == (8, 4) and 0 <= int(ex) < 4 and 0 <= int(seg) < 4
+    # a second plan of the same shape reuses the cached choice (no new line)
+    feM = fe.AbstractFixedEffectSolver(fes, None, "CUDA", np.float32)
+    R2, _, _ = feM.solve_residuals(Y.copy(), tol=1e-8)
+    feM.close()
+    assert len(cache.read_text().strip().splitlines()) == 1
+    assert np.array_equal(R1, R2)
