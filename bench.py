@@ -377,6 +377,41 @@ def run_ours(args):
     return 0
 
 
+def run_sweep(args):
+    """Times every expand x segsum kernel variant on the workload (mixed
+    precision, 32-column tile) and for the per-column FP64 form; prints a
+    markdown table.  The autotuner makes the same choice at run time."""
+    import torch
+    torch.cuda.set_device(0)
+    import __graft_entry__ as g
+    fe = g.load_package()
+    pb = make_workload(args.scale, 0, args.ncols)
+    fes = [fe.FixedEffect.from_refs(r, n, a) for r, n, a in zip(pb.refs, pb.nlev, pb.interaction)]
+    Y0 = torch.from_numpy(np.ascontiguousarray(pb.Y.T)).cuda().t()
+    print("| mode | expand | segsum | ms per solve | solves/s |\n|---|---:|---:|---:|---:|")
+    for prec, tile, ncols in (("mixed", 0, pb.Y.shape[1]), ("fp64", 1, min(4, pb.Y.shape[1]))):
+        feM = fe.AbstractFixedEffectSolver(fes, pb.weights, "CUDA", np.float64, precision=prec)
+        feM.set_option(fe._lib.FE_OPT_TILE, tile)
+        for e in range(4):
+            for sv in range(4):
+                feM.set_option(fe._lib.FE_OPT_EXPAND_VARIANT, e)
+                feM.set_option(fe._lib.FE_OPT_SEGSUM_VARIANT, sv)
+                best = 1e30
+                for _ in range(3):
+                    Y = Y0[:, :ncols].clone().t().contiguous().t()
+                    if prec == "fp64":
+                        Y = Y.double().t().contiguous().t()
+                    torch.cuda.synchronize()
+                    t = time.perf_counter()
+                    feM.solve_residuals(Y, tol=1e-8, maxiter=10000)
+                    torch.cuda.synchronize()
+                    best = min(best, time.perf_counter() - t)
+                mode = f"{prec} C={'32' if tile == 0 else '1'}"
+                print(f"| {mode} | {e} | {sv} | {best * 1e3:.1f} | {ncols / best:.1f} |", flush=True)
+        feM.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -388,7 +423,11 @@ def main():
     ap.add_argument("--plain-cols", type=int, default=4)
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--sweep-variants", action="store_true",
+                    help="time every expand/segsum kernel variant and print a table")
     args = ap.parse_args()
+    if args.sweep_variants:
+        return run_sweep(args)
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)
