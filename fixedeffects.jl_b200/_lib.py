@@ -41,7 +41,7 @@ EXPORTS = (
     "fe_plan_destroy", "fe_solve_residuals", "fe_solve_residuals_device",
     "fe_solve_coefficients", "fe_plan_problem_results", "fe_plan_last_solve_info",
     "fe_plan_get_integer_plan", "fe_plan_get_scales", "fe_plan_primary",
-    "fe_plan_kernel_stat", "fe_plan_reset_stats",
+    "fe_plan_kernel_stat", "fe_plan_reset_stats", "fe_plan_scales_noalloc",
 )
 
 _i64p = ctypes.POINTER(ctypes.c_int64)
@@ -104,6 +104,7 @@ def load(path: Path | str | None = None):
         "fe_plan_kernel_stat": (ctypes.c_int, [_vp, ctypes.c_int32, ctypes.c_char_p,
                                                ctypes.c_int64, _i64p, _f64p, _f64p]),
         "fe_plan_reset_stats": (ctypes.c_int, [_vp]),
+        "fe_plan_scales_noalloc": (ctypes.c_int, [_vp, ctypes.c_int32, _vp, _vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

@@ -19,10 +19,16 @@
 namespace fe {
 
 namespace {
-thread_local std::string g_err;
+// fixed-size per-thread message buffer: reporting an error allocates nothing
+thread_local char g_err[1024];
 }
-void set_error(const std::string& msg) { g_err = msg; }
-const char* last_error() { return g_err.c_str(); }
+void set_error(const std::string& msg) { set_error_cstr(msg.c_str()); }
+void set_error_cstr(const char* msg) {
+  size_t n = 0;
+  for (; msg[n] && n + 1 < sizeof(g_err); ++n) g_err[n] = msg[n];
+  g_err[n] = '\0';
+}
+const char* last_error() { return g_err; }
 
 DevBuf::~DevBuf() {
   if (p) cudaFree(p);

@@ -17,6 +17,7 @@ namespace fe {
 
 // thread-local last error (fe_last_error)
 void set_error(const std::string& msg);
+void set_error_cstr(const char* msg);
 const char* last_error();
 
 #define FE_CK(call)                                                                     \

@@ -177,6 +177,29 @@ int fe_plan_kernel_stat(fe_plan* plan, int32_t index, char* name, int64_t name_l
                         int64_t* launches, double* total_ms, double* alg_bytes);
 int fe_plan_reset_stats(fe_plan* plan);
 
+/*
+ * fe_plan_scales_noalloc -- no counterpart in the reference.
+ *
+ * Recomputes the Jacobi scales of fixed effect `fe_index` of an existing plan
+ * (the values fe_plan_get_scales returns, src/SolverCPU.jl:78-89) into
+ * `scale_out_dev`, n_levels[fe_index] doubles of DEVICE memory, enqueued on
+ * `stream` (NULL: the plan's stream), without allocating any memory.  It is
+ * for callers that cannot call cudaMalloc at that point: a stream being
+ * captured into a CUDA graph, a caller whose device memory belongs to its own
+ * pool or runtime (e.g. Julia's CUDA.jl), a host callback.
+ *
+ * Its scratch is one file-scope device array of FE_NOALLOC_SCRATCH_BYTES
+ * (8 MiB) that every GPU which loads the library holds until the process
+ * exits; fixed effects whose level sums do not fit (about 1e6 levels) are
+ * rejected with FE_ERR_INVALID and a message.  The first call on a device
+ * looks up the array's device address (cudaGetSymbolAddress); make that first
+ * call before any stream capture.  All calls share the array and it keeps
+ * the last call's contents (each call clears what must start at zero): calls
+ * that overlap on the GPU race and must be serialized by the caller.
+ */
+#define FE_NOALLOC_SCRATCH_BYTES (8u << 20)
+int fe_plan_scales_noalloc(fe_plan* plan, int32_t fe_index, double* scale_out_dev, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
