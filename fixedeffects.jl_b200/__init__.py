@@ -260,9 +260,11 @@ class FixedEffectSolverB200:
                 raise ValueError("device y must be contiguous")
             ld = self.N
         else:
-            if y.stride(0) != 1:
+            if y.stride(0) != 1 and ncols > 1:
                 raise ValueError("device Y must be column-major (y.t() contiguous)")
-            ld = y.stride(1)
+            # a single column is contiguous whatever stride torch reports for
+            # its size-1 dimension
+            ld = y.stride(1) if ncols > 1 else self.N
         its = np.zeros(ncols, dtype=np.int64)
         cvs = np.zeros(ncols, dtype=np.uint8)
         dt = FE_DTYPE_F64 if y.dtype == torch.float64 else FE_DTYPE_F32

@@ -33,6 +33,8 @@ FE_OPT_FUSE = 6
 FE_OPT_EXPAND_VARIANT = 7
 FE_OPT_SEGSUM_VARIANT = 8
 FE_OPT_AUTOTUNE = 9
+FE_OPT_MIXED_WARM_START = 10
+FE_OPT_GRAPH = 11
 
 # every symbol declared in include/fe_b200.h
 EXPORTS = (

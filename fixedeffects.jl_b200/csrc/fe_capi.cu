@@ -234,11 +234,18 @@ int fe_plan_set_option(fe_plan* plan, int32_t option, double value) {
     case FE_OPT_AUTOTUNE:
       plan->opt_autotune = value != 0 ? 1 : 0;
       return FE_OK;
+    case FE_OPT_MIXED_WARM_START:
+      plan->opt_mixed_warm = value != 0 ? 1 : 0;
+      return FE_OK;
+    case FE_OPT_GRAPH:
+      plan->opt_graph = value != 0 ? 1 : 0;
+      return FE_OK;
     case FE_OPT_EXPAND_VARIANT:
     case FE_OPT_SEGSUM_VARIANT: {
       const int v = (int)value;
-      if (v < -1 || v > 3) {
-        set_error("kernel variant must be -1 (default) or 0..3");
+      const int vmax = option == FE_OPT_EXPAND_VARIANT ? 3 : 5;
+      if (v < -1 || v > vmax) {
+        set_error("kernel variant must be -1 (default) or 0..3 (expand), 0..5 (segsum)");
         return FE_ERR_INVALID;
       }
       (option == FE_OPT_EXPAND_VARIANT ? plan->opt_ex_variant : plan->opt_seg_variant) = v;

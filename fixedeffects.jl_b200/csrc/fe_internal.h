@@ -55,13 +55,30 @@ struct PItem {
   int32_t prob;
 };
 
-// A level cut into pieces.  The last piece to finish sums all piece partials
-// in piece order (deterministic) and finalizes the level.
+// A level cut into pieces, combined in two deterministic stages: the pieces
+// form blocks of kSplitBlock; the last piece of a block to finish sums the
+// block's pieces in piece order, and the last block to finish sums the block
+// partials in block order and stores the level.  (Integer counters decide who
+// is last; the summation order does not depend on it.)
+constexpr int kSplitBlock = 32;
 struct SplitLevel {
   int32_t first_piece;
   int32_t npieces;
   int32_t fe;
-  int32_t level;     // FE-local level id
+  int32_t level;        // FE-local level id
+  int32_t first_block;  // index of its first block in the block arrays
+  int32_t nblocks;
+};
+
+// Scratch of the split-level combine (per launch list).
+struct SplitArgs {
+  const SplitLevel* splits;
+  double* piece_part;   // [C][n_pieces]
+  int64_t n_pieces;
+  double* block_part;   // [C][n_blocks]
+  int64_t n_blocks;
+  int32_t* level_cnt;   // per split level
+  int32_t* block_cnt;   // per block
 };
 
 // Device-side view of a plan (passed by value to kernels).

@@ -29,6 +29,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <type_traits>
+
 #include "fe_internal.h"
 
 namespace fe {
@@ -328,14 +330,11 @@ struct SegRun {
     for (int v = 0; v < VEC; ++v) carry.v[v] = __shfl_sync(FE_FULL, x.v[v], srcl);
   }
   // end of a work item.  split < 0: the last key is complete.  Otherwise the
-  // item is piece `piece` of split level `sl`: its partial goes to the piece
-  // buffer ([C][n_pieces]) and the last piece to finish (integer counter)
-  // sums all pieces in piece order and stores the level.  smt: 32 doubles of
-  // shared scratch owned by this warp.
-  __device__ __forceinline__ void finish(int split, int piece, const SplitLevel* __restrict__ splits,
-                                         double* __restrict__ piece_part, int64_t n_pieces,
-                                         int32_t* __restrict__ split_cnt, int g, int jl, int C,
-                                         TA* __restrict__ Sk, double* smt) {
+  // item is piece `piece` of split level sa.splits[split], combined in two
+  // deterministic stages (see SplitLevel).  smt: 32 doubles of shared scratch
+  // owned by this warp.
+  __device__ __forceinline__ void finish(int split, int piece, const SplitArgs& sa, int g, int jl,
+                                         int C, TA* __restrict__ Sk, double* smt) {
     fold();
     if (ckey < 0) return;
     if (split < 0) {
@@ -343,23 +342,43 @@ struct SegRun {
       return;
     }
     const int lane = threadIdx.x & 31;
-    const SplitLevel sl = splits[split];
+    const SplitLevel sl = sa.splits[split];
     if (g == 0) {
 #pragma unroll
       for (int v = 0; v < VEC; ++v)
-        piece_part[(int64_t)(jl * VEC + v) * n_pieces + sl.first_piece + piece] = (double)carry.v[v];
+        sa.piece_part[(int64_t)(jl * VEC + v) * sa.n_pieces + sl.first_piece + piece] =
+            (double)carry.v[v];
     }
+    // stage 1: the last piece of the block sums the block
+    const int blk = piece / kSplitBlock;
+    const int p0 = blk * kSplitBlock;
+    const int np = min(kSplitBlock, sl.npieces - p0);
     __threadfence();
     __syncwarp();
     int last = 0;
-    if (lane == 0) last = (atomicAdd(split_cnt + split, 1) == sl.npieces - 1) ? 1 : 0;
+    if (lane == 0) last = (atomicAdd(sa.block_cnt + sl.first_block + blk, 1) == np - 1) ? 1 : 0;
     last = __shfl_sync(FE_FULL, last, 0);
     if (!last) return;
     __threadfence();
     for (int jj = 0; jj < C; ++jj) {
-      const double* pp = piece_part + (int64_t)jj * n_pieces + sl.first_piece;
+      double acc = lane < np ? __ldcg(sa.piece_part + (int64_t)jj * sa.n_pieces + sl.first_piece + p0 + lane) : 0.0;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(FE_FULL, acc, o);
+      if (lane == 0) sa.block_part[(int64_t)jj * sa.n_blocks + sl.first_block + blk] = acc;
+    }
+    if (lane == 0) sa.block_cnt[sl.first_block + blk] = 0;
+    // stage 2: the last block sums the level
+    __threadfence();
+    __syncwarp();
+    last = 0;
+    if (lane == 0) last = (atomicAdd(sa.level_cnt + split, 1) == sl.nblocks - 1) ? 1 : 0;
+    last = __shfl_sync(FE_FULL, last, 0);
+    if (!last) return;
+    __threadfence();
+    for (int jj = 0; jj < C; ++jj) {
+      const double* bp = sa.block_part + (int64_t)jj * sa.n_blocks + sl.first_block;
       double acc = 0.0;
-      for (int q = lane; q < sl.npieces; q += 32) acc += __ldcg(pp + q);
+      for (int q = lane; q < sl.nblocks; q += 32) acc += __ldcg(bp + q);
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(FE_FULL, acc, o);
       if (lane == 0) smt[jj] = acc;
@@ -371,7 +390,7 @@ struct SegRun {
       for (int v = 0; v < VEC; ++v) tot.v[v] = (TA)smt[jl * VEC + v];
       vst<TA, VEC>(Sk + (int64_t)ckey * C, tot);
     }
-    if (lane == 0) split_cnt[split] = 0;
+    if (lane == 0) sa.level_cnt[split] = 0;
   }
 };
 
@@ -389,10 +408,7 @@ struct SegRun {
 // ---------------------------------------------------------------------------
 struct FuseArgs {
   double* sum;  // [P][C] sum slab (TA-typed), null when not fused
-  const SplitLevel* splits;
-  double* piece_part;
-  int64_t n_pieces;
-  int32_t* split_cnt;
+  SplitArgs sa;
 };
 
 template <typename TA, int C, int U, int KB, bool FUSE, bool PF, class Tab, class Epi>
@@ -508,9 +524,7 @@ k_expand(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_items, T
           }
         }
       }
-      if (FUSE)
-        run.finish(it.split, it.piece, fz.splits, fz.piece_part, fz.n_pieces, fz.split_cnt, g, jl, C,
-                   Sf, sm[wib]);
+      if (FUSE) run.finish(it.split, it.piece, fz.sa, g, jl, C, Sf, sm[wib]);
 #pragma unroll
       for (int v = 0; v < VEC; ++v) nrm[v] += (double)nit[v];
     }
@@ -526,6 +540,7 @@ template <typename TIn, typename TA, int VEC>
 struct LoadIn {
   const TIn* __restrict__ in;
   static constexpr bool kSquareWeight = false;
+  static constexpr bool kAsyncable = std::is_same<TIn, TA>::value;  // raw rows can be copied
   __device__ __forceinline__ VA<TA, VEC> load(int64_t off) const {
     const VA<TIn, VEC> a = vld<TIn, VEC>(in + off);
     VA<TA, VEC> r;
@@ -539,6 +554,7 @@ struct LoadIn {
 // is 1.  C = 1.
 struct LoadScaleSq {
   static constexpr bool kSquareWeight = true;
+  static constexpr bool kAsyncable = false;
   __device__ __forceinline__ VA<double, 1> load(int64_t) const {
     VA<double, 1> r;
     r.v[0] = 1.0;
@@ -557,8 +573,7 @@ struct LoadScaleSq {
 template <typename TA, int C, int U, bool PF, class Load>
 __global__ void __launch_bounds__(kThreads)
 k_segsum(const FeDev d, const ReduceItem* __restrict__ items, int64_t n_items, Load ld,
-         TA* __restrict__ Sout, const SplitLevel* __restrict__ splits,
-         double* __restrict__ piece_part, int64_t n_pieces, int32_t* __restrict__ split_cnt) {
+         TA* __restrict__ Sout, SplitArgs sa) {
   using Sh = Shape<TA, C>;
   constexpr int VEC = Sh::VEC, CL = Sh::CL, G = Sh::G;
   constexpr int STEP = G * U;
@@ -624,8 +639,152 @@ k_segsum(const FeDev d, const ReduceItem* __restrict__ items, int64_t n_items, L
       run.push(kk[u], val[u], nvalid, g, jl, C, Sk);
     }
   }
-  run.finish(it.split, it.pad, splits, piece_part, n_pieces, split_cnt, g, jl, C, Sk,
-             smt[threadIdx.x >> 5]);
+  run.finish(it.split, it.pad, sa, g, jl, C, Sk, smt[threadIdx.x >> 5]);
+}
+
+// ---------------------------------------------------------------------------
+// k_segsum_async: the same segmented sum with the level-order row gathers
+// moved off the registers.  Each warp keeps an S-stage ring in shared memory;
+// step t+S-1 is issued with cp.async (hand-written PTX) while step t is
+// consumed, so S-1 steps of row gathers are in flight per warp whatever the
+// register count.  Each lane copies exactly the row chunks it later reads
+// (group g, column block jl), so a lane's own cp.async.wait_group makes its
+// data visible; keys and weights are copied by lane jl = 0 of each group and
+// shared through a __syncwarp.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void cp_async_bytes16(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem));
+}
+__device__ __forceinline__ void cp_async_bytes8(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem));
+}
+__device__ __forceinline__ void cp_async_bytes4(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem));
+}
+template <int B>
+__device__ __forceinline__ void cp_async(void* smem, const void* gmem) {
+  if (B == 16) cp_async_bytes16(smem, gmem);
+  else if (B == 8) cp_async_bytes8(smem, gmem);
+  else cp_async_bytes4(smem, gmem);
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+
+// shared memory per warp of k_segsum_async
+template <typename TA, int C, int U, int S>
+struct AsyncSegLayout {
+  using Sh = Shape<TA, C>;
+  static constexpr int STEP = Sh::G * U;
+  static constexpr int kRowBytes = C * (int)sizeof(TA);
+  static constexpr int kStageRows = STEP * kRowBytes;
+  static constexpr int kStage = kStageRows + STEP * (4 + (int)sizeof(TA));
+  static constexpr int kWarpBytes = S * kStage;
+};
+
+template <typename TA, int C, int U, int S, class Load>
+__global__ void __launch_bounds__(kThreads)
+k_segsum_async(const FeDev d, const ReduceItem* __restrict__ items, int64_t n_items, Load ld,
+               TA* __restrict__ Sout, SplitArgs sa) {
+  using Sh = Shape<TA, C>;
+  constexpr int VEC = Sh::VEC, CL = Sh::CL, G = Sh::G;
+  using L = AsyncSegLayout<TA, C, U, S>;
+  constexpr int STEP = L::STEP;
+  constexpr int NI = STEP >= 32 ? STEP / 32 : 1;
+  constexpr int CHUNK = VEC * (int)sizeof(TA);  // bytes a lane copies per row
+  extern __shared__ __align__(16) unsigned char dyn_smem[];
+  __shared__ double smt[kWarps][32];
+  const int lane = threadIdx.x & 31;
+  const int wib = threadIdx.x >> 5;
+  const int g = lane / CL, jl = lane - g * CL;
+  const int64_t w = (int64_t)blockIdx.x * kWarps + wib;
+  if (w >= n_items) return;
+  const ReduceItem it = items[w];
+  if (it.pe <= it.pb) return;
+  unsigned char* ring = dyn_smem + (size_t)wib * L::kWarpBytes;
+  const int k = it.fe;
+  const int32_t* __restrict__ perm = d.perm[k];
+  const int32_t* __restrict__ key = d.key[k];
+  const TA* __restrict__ cwp = cwp_of<TA>(d, k);
+  const TA* __restrict__ in = ld.in;
+  TA* __restrict__ Sk = Sout + d.lev_base[k] * C + jl * VEC;
+  const int64_t nsteps = (it.pe - it.pb + STEP - 1) / STEP;
+  // sorted positions of the step to issue next (loaded one step early)
+  int il[NI];
+  auto load_idx = [&](int64_t step) {
+#pragma unroll
+    for (int r = 0; r < NI; ++r) {
+      const int64_t p = it.pb + step * STEP + r * 32 + lane;
+      const bool ok = step < nsteps && p < it.pe && (r * 32 + lane) < STEP;
+      il[r] = ok ? (perm ? __ldg(perm + p) : (int)p) : -1;
+    }
+  };
+  auto issue = [&](int64_t step) {
+    if (step < nsteps) {
+      unsigned char* st = ring + (int)(step % S) * L::kStage;
+      int32_t* skey = reinterpret_cast<int32_t*>(st + L::kStageRows);
+      TA* scw = reinterpret_cast<TA*>(st + L::kStageRows + STEP * 4);
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int q = u * G;
+        const int i = __shfl_sync(FE_FULL, il[q >> 5], (q & 31) + g);
+        const int row = u * G + g;
+        const int64_t p = it.pb + step * STEP + row;
+        if (i >= 0) {
+          cp_async<CHUNK>(st + row * L::kRowBytes + jl * CHUNK, in + (int64_t)i * C + jl * VEC);
+          if (jl == 0) {
+            cp_async_bytes4(skey + row, key + p);
+            if (cwp) cp_async<(int)sizeof(TA)>(scw + row, cwp + p);
+          }
+        }
+      }
+    }
+    cp_async_commit();  // one group per step, empty past the end
+  };
+  load_idx(0);
+#pragma unroll
+  for (int t = 0; t < S - 1; ++t) {
+    issue(t);
+    load_idx(t + 1);
+  }
+  SegRun<TA, VEC, CL, G> run;
+  run.init();
+  for (int64_t t = 0; t < nsteps; ++t) {
+    issue(t + S - 1);
+    load_idx(t + S);
+    cp_async_wait<S - 1>();
+    __syncwarp();
+    const unsigned char* st = ring + (int)(t % S) * L::kStage;
+    const int32_t* skey = reinterpret_cast<const int32_t*>(st + L::kStageRows);
+    const TA* scw = reinterpret_cast<const TA*>(st + L::kStageRows + STEP * 4);
+    const int64_t base = it.pb + t * STEP;
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int64_t b0 = base + (int64_t)u * G;
+      if (b0 >= it.pe) break;  // warp-uniform
+      const int row = u * G + g;
+      const bool ok = b0 + g < it.pe;
+      const int km = ok ? skey[row] : kSentinel;
+      VA<TA, VEC> x;
+      if (ok) {
+        x = vld<TA, VEC>(reinterpret_cast<const TA*>(st + row * L::kRowBytes + jl * CHUNK));
+        const TA c = cwp ? scw[row] : TA(1);
+#pragma unroll
+        for (int v = 0; v < VEC; ++v) x.v[v] *= c;
+      } else {
+#pragma unroll
+        for (int v = 0; v < VEC; ++v) x.v[v] = TA(0);
+      }
+      const int nvalid = (int)((it.pe - b0) < G ? (it.pe - b0) : G);
+      run.push(km, x, nvalid, g, jl, C, Sk);
+    }
+    __syncwarp();  // the stage is refilled by the next issue
+  }
+  cp_async_wait<0>();
+  run.finish(it.split, it.pad, sa, g, jl, C, Sk, smt[wib]);
 }
 
 // ---------------------------------------------------------------------------

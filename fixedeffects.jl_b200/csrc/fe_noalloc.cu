@@ -63,9 +63,7 @@ int scratch_address(int device, void** out) {
 template <int U>
 __global__ void __launch_bounds__(kThreads)
 k_segsum_scale_one_fe(const FeDev d, const ReduceItem* __restrict__ items, int64_t n_items,
-                      int fe, double* __restrict__ sums, const SplitLevel* __restrict__ splits,
-                      double* __restrict__ piece_part, int64_t n_pieces,
-                      int32_t* __restrict__ split_cnt) {
+                      int fe, double* __restrict__ sums, SplitArgs sa) {
   using Sh = Shape<double, 1>;
   constexpr int VEC = Sh::VEC, CL = Sh::CL, G = Sh::G;
   constexpr int STEP = G * U;
@@ -109,8 +107,7 @@ k_segsum_scale_one_fe(const FeDev d, const ReduceItem* __restrict__ items, int64
       run.push(km, x, nvalid, g, jl, 1, sums);
     }
   }
-  run.finish(it.split, it.pad, splits, piece_part, n_pieces, split_cnt, g, jl, 1, sums,
-             smt[threadIdx.x >> 5]);
+  run.finish(it.split, it.pad, sa, g, jl, 1, sums, smt[threadIdx.x >> 5]);
 }
 
 // scale = 1/sqrt(sum), or 0 for an empty sum (src/SolverCPU.jl:84-88)
@@ -149,11 +146,14 @@ extern "C" int fe_plan_scales_noalloc(fe_plan* plan, int32_t fe_index, double* s
     return FE_ERR_INVALID;
   }
   const ItemSet* its = f->second.get();
-  // scratch layout: [level sums | piece partials | split counters]
+  // scratch layout: [level sums | piece partials | block partials |
+  //                  level counters | block counters]
   const size_t sums_bytes = ((size_t)nlev * sizeof(double) + 255) & ~(size_t)255;
   const size_t piece_bytes = (((size_t)its->n_pieces) * sizeof(double) + 255) & ~(size_t)255;
+  const size_t block_bytes = (((size_t)its->n_blocks) * sizeof(double) + 255) & ~(size_t)255;
   const size_t cnt_bytes = (its->splits.size() * sizeof(int32_t) + 255) & ~(size_t)255;
-  if (sums_bytes + piece_bytes + cnt_bytes > kNoAllocScratchBytes) {
+  const size_t bcnt_bytes = (((size_t)its->n_blocks) * sizeof(int32_t) + 255) & ~(size_t)255;
+  if (sums_bytes + piece_bytes + block_bytes + cnt_bytes + bcnt_bytes > kNoAllocScratchBytes) {
     set_error_cstr(
         "fe_plan_scales_noalloc: the fixed effect needs more scratch than FE_NOALLOC_SCRATCH_BYTES "
         "(8 MiB: about 1e6 levels); use fe_plan_update_weights/fe_plan_get_scales");
@@ -170,7 +170,9 @@ extern "C" int fe_plan_scales_noalloc(fe_plan* plan, int32_t fe_index, double* s
   unsigned char* b = static_cast<unsigned char*>(base);
   double* sums = reinterpret_cast<double*>(b);
   double* pieces = reinterpret_cast<double*>(b + sums_bytes);
-  int32_t* cnt = reinterpret_cast<int32_t*>(b + sums_bytes + piece_bytes);
+  double* blocks = reinterpret_cast<double*>(b + sums_bytes + piece_bytes);
+  int32_t* cnt = reinterpret_cast<int32_t*>(b + sums_bytes + piece_bytes + block_bytes);
+  int32_t* bcnt = reinterpret_cast<int32_t*>(b + sums_bytes + piece_bytes + block_bytes + cnt_bytes);
   cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : plan->stream;
   // levels without positions are never written by the sum kernel and the
   // split counters must start at zero: clear both (the array keeps the
@@ -178,6 +180,8 @@ extern "C" int fe_plan_scales_noalloc(fe_plan* plan, int32_t fe_index, double* s
   cudaError_t e = cudaMemsetAsync(sums, 0, (size_t)nlev * sizeof(double), s);
   if (e == cudaSuccess && !its->splits.empty())
     e = cudaMemsetAsync(cnt, 0, its->splits.size() * sizeof(int32_t), s);
+  if (e == cudaSuccess && its->n_blocks > 0)
+    e = cudaMemsetAsync(bcnt, 0, (size_t)its->n_blocks * sizeof(int32_t), s);
   if (e != cudaSuccess) {
     (void)cudaGetLastError();
     set_error_cstr("fe_plan_scales_noalloc: cudaMemsetAsync failed");
@@ -188,9 +192,10 @@ extern "C" int fe_plan_scales_noalloc(fe_plan* plan, int32_t fe_index, double* s
   const int64_t n_items = (int64_t)its->rd.size();
   if (n_items > 0) {
     const unsigned grid = (unsigned)((n_items + kWarps - 1) / kWarps);
-    k_segsum_scale_one_fe<8><<<grid, kThreads, 0, s>>>(
-        d, its->d_rd.as<ReduceItem>(), n_items, fe_index, sums, its->d_splits.as<SplitLevel>(),
-        pieces, its->n_pieces, cnt);
+    SplitArgs sa{its->d_splits.as<SplitLevel>(), pieces, its->n_pieces, blocks, its->n_blocks, cnt,
+                 bcnt};
+    k_segsum_scale_one_fe<8><<<grid, kThreads, 0, s>>>(d, its->d_rd.as<ReduceItem>(), n_items,
+                                                        fe_index, sums, sa);
   }
   k_scale_from_sums<<<(unsigned)((nlev + 255) / 256), 256, 0, s>>>(sums, nlev, scale_out_dev);
   e = cudaGetLastError();

@@ -368,17 +368,19 @@ int plan_update_weights(fe_plan* pl, const double* weights) {
   if (st) return st;
   FeDev dd = d;
   dd.C = 1;
-  DevBuf sums, piece;
+  DevBuf sums, piece, block;
   st = sums.ensure((size_t)std::max<int64_t>(pl->P, 1) * 8);
   if (!st) st = piece.ensure((size_t)std::max<int64_t>(its->n_pieces, 1) * 8);
+  if (!st) st = block.ensure((size_t)std::max<int64_t>(its->n_blocks, 1) * 8);
   if (st) return st;
   FE_CK(cudaMemsetAsync(sums.p, 0, (size_t)std::max<int64_t>(pl->P, 1) * 8, s));
   if (!its->rd.empty()) {
     const unsigned grid = (unsigned)((its->rd.size() + kWarps - 1) / kWarps);
+    SplitArgs sa{its->d_splits.as<SplitLevel>(), piece.as<double>(), its->n_pieces,
+                 block.as<double>(), its->n_blocks, its->d_split_cnt.as<int32_t>(),
+                 its->d_block_cnt.as<int32_t>()};
     k_segsum<double, 1, 8, false, LoadScaleSq><<<grid, kThreads, 0, s>>>(
-        dd, its->d_rd.as<ReduceItem>(), (int64_t)its->rd.size(), LoadScaleSq{}, sums.as<double>(),
-        its->d_splits.as<SplitLevel>(), piece.as<double>(), its->n_pieces,
-        its->d_split_cnt.as<int32_t>());
+        dd, its->d_rd.as<ReduceItem>(), (int64_t)its->rd.size(), LoadScaleSq{}, sums.as<double>(), sa);
     FE_CK(cudaGetLastError());
   }
   if (!its->pu.empty()) {
@@ -465,6 +467,9 @@ int plan_items(fe_plan* pl, int C, ItemSet** out) {
           sl.npieces = (int32_t)npieces;
           sl.fe = kp;
           sl.level = (int32_t)l;
+          sl.nblocks = (int32_t)((npieces + kSplitBlock - 1) / kSplitBlock);
+          sl.first_block = (int32_t)its->ex_n_blocks;
+          its->ex_n_blocks += sl.nblocks;
           const int32_t sid = (int32_t)its->ex_splits.size();
           its->ex_splits.push_back(sl);
           for (int64_t q = 0; q < npieces; ++q) {
@@ -523,6 +528,9 @@ int plan_items(fe_plan* pl, int C, ItemSet** out) {
           sl.npieces = (int32_t)npieces;
           sl.fe = k;
           sl.level = (int32_t)l;
+          sl.nblocks = (int32_t)((npieces + kSplitBlock - 1) / kSplitBlock);
+          sl.first_block = (int32_t)its->n_blocks;
+          its->n_blocks += sl.nblocks;
           const int32_t sid = (int32_t)its->splits.size();
           its->splits.push_back(sl);
           for (int64_t q = 0; q < npieces; ++q) {
@@ -559,11 +567,19 @@ int plan_items(fe_plan* pl, int C, ItemSet** out) {
   if (!st) st = upload(its->d_ex_off, its->ex_slot_off.data(), its->ex_slot_off.size(), s);
   if (!st) st = upload(its->d_pu_off, its->pu_slot_off.data(), its->pu_slot_off.size(), s);
   if (!st) st = upload(its->d_ex_splits, its->ex_splits.data(), its->ex_splits.size(), s);
-  if (!st) st = its->d_split_cnt.ensure(std::max<size_t>(its->splits.size(), 1) * 4);
-  if (!st) st = its->d_ex_split_cnt.ensure(std::max<size_t>(its->ex_splits.size(), 1) * 4);
+  const size_t nsc = std::max<size_t>(its->splits.size(), 1) * 4;
+  const size_t nesc = std::max<size_t>(its->ex_splits.size(), 1) * 4;
+  const size_t nbc = (size_t)std::max<int64_t>(its->n_blocks, 1) * 4;
+  const size_t nebc = (size_t)std::max<int64_t>(its->ex_n_blocks, 1) * 4;
+  if (!st) st = its->d_split_cnt.ensure(nsc);
+  if (!st) st = its->d_ex_split_cnt.ensure(nesc);
+  if (!st) st = its->d_block_cnt.ensure(nbc);
+  if (!st) st = its->d_ex_block_cnt.ensure(nebc);
   if (st) return st;
-  FE_CK(cudaMemsetAsync(its->d_split_cnt.p, 0, std::max<size_t>(its->splits.size(), 1) * 4, s));
-  FE_CK(cudaMemsetAsync(its->d_ex_split_cnt.p, 0, std::max<size_t>(its->ex_splits.size(), 1) * 4, s));
+  FE_CK(cudaMemsetAsync(its->d_split_cnt.p, 0, nsc, s));
+  FE_CK(cudaMemsetAsync(its->d_ex_split_cnt.p, 0, nesc, s));
+  FE_CK(cudaMemsetAsync(its->d_block_cnt.p, 0, nbc, s));
+  FE_CK(cudaMemsetAsync(its->d_ex_block_cnt.p, 0, nebc, s));
   FE_CK(cudaStreamSynchronize(s));
   *out = its.get();
   pl->items[C] = std::move(its);
@@ -580,6 +596,8 @@ int plan_destroy(fe_plan* pl) {
     cudaEventDestroy(pr.second.second);
   }
   if (pl->host_pinned) cudaFreeHost(pl->host_pinned);
+  for (auto& g : pl->graphs)
+    if (g.second.exec) cudaGraphExecDestroy(g.second.exec);
   cudaStream_t s = pl->stream;
   bool own = pl->own_stream;
   delete pl;

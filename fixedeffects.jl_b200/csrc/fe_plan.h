@@ -52,18 +52,26 @@ struct ItemSet {
   std::vector<PItem> pu;
   std::vector<int64_t> ex_slot_off;       // per problem, expand norm slots (CTAs)
   std::vector<int64_t> pu_slot_off;       // per problem, P-side norm slots (CTAs)
-  int64_t n_pieces = 0;
+  int64_t n_pieces = 0, n_blocks = 0;
+  int64_t ex_n_blocks = 0;
   int64_t Se = 0, Sp = 0;                 // slot counts
-  DevBuf d_ex, d_rd, d_splits, d_pu, d_ex_off, d_pu_off, d_split_cnt;
-  DevBuf d_ex_splits, d_ex_split_cnt;
+  DevBuf d_ex, d_rd, d_splits, d_pu, d_ex_off, d_pu_off, d_split_cnt, d_block_cnt;
+  DevBuf d_ex_splits, d_ex_split_cnt, d_ex_block_cnt;
 };
 
 struct Workspace {
   int C = 0;
   DevBuf B64, R64, U, V, H, Hb, X, X64, S;
-  DevBuf part_e, part_a, part_b, piece_part, ex_piece_part, inst, counters;
+  DevBuf part_e, part_a, part_b, piece_part, ex_piece_part, block_part, ex_block_part, inst,
+      counters;
   DevBuf coef;
   DevBuf ystage;  // device copy of host Y for host-buffer solves
+};
+
+// A captured run of LSMR iterations (the inner loop of one tile shape).
+struct LoopGraph {
+  cudaGraphExec_t exec = nullptr;
+  size_t key = 0;  // fingerprint of everything the captured launches use
 };
 
 struct Profile {
@@ -118,6 +126,9 @@ struct fe_plan {
   int32_t opt_ex_variant = -1; // expand kernel variant (-1: tuned default)
   int32_t opt_seg_variant = -1; // segsum kernel variant (-1: tuned default)
   int32_t opt_autotune = 1;     // time the variants on first use of a tile shape
+  int32_t opt_mixed_warm = 1;   // mixed precision starts from x0 = A'b (else x0 = 0)
+  int32_t opt_graph = 1;        // replay the LSMR iterations from a CUDA graph
+  std::map<std::pair<int, int>, fe::LoopGraph> graphs;  // by (C, precision)
   // tuned variants per (tile width C, element size): {expand, segsum}
   std::map<std::pair<int, int>, std::pair<int, int>> tuned;
   std::string tune_signature;   // plan shape, key of the persisted tuning cache

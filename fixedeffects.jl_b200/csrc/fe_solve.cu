@@ -76,7 +76,7 @@ static const std::string& tune_signature(fe_plan* pl) {
       (void)cudaGetLastError();
       os << "unknown";
     }
-    os << "/kv1/N" << pl->N << "/P" << pl->nprob << "/K" << pl->K << "/w" << (pl->weighted ? 1 : 0);
+    os << "/kv2/N" << pl->N << "/P" << pl->nprob << "/K" << pl->K << "/w" << (pl->weighted ? 1 : 0);
     for (int k = 0; k < pl->K; ++k) os << "/" << pl->nlev[k] << (pl->interacted[k] ? "i" : "");
     pl->tune_signature = os.str();
   }
@@ -96,7 +96,7 @@ bool tune_cache_load(fe_plan* pl, int C, int sT, int* ex, int* seg) {
     std::string s;
     int c = 0, t = 0, e = 0, g = 0;
     if (!(is >> s >> c >> t >> e >> g)) continue;
-    if (s == sig && c == C && t == sT && e >= 0 && e < 4 && g >= 0 && g < 4) {
+    if (s == sig && c == C && t == sT && e >= 0 && e < 4 && g >= 0 && g < 6) {
       *ex = e;
       *seg = g;
       found = true;  // the last matching line wins

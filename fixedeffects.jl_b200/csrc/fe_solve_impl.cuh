@@ -153,6 +153,17 @@ struct Ctx {
   double* piece;
   double* ex_piece;
   void* S;
+  SplitArgs seg_split() const {
+    return SplitArgs{its->d_splits.as<SplitLevel>(), piece, its->n_pieces, block, its->n_blocks,
+                     its->d_split_cnt.as<int32_t>(), its->d_block_cnt.as<int32_t>()};
+  }
+  SplitArgs ex_split() const {
+    return SplitArgs{its->d_ex_splits.as<SplitLevel>(), ex_piece, its->ex_n_pieces, ex_block,
+                     its->ex_n_blocks, its->d_ex_split_cnt.as<int32_t>(),
+                     its->d_ex_block_cnt.as<int32_t>()};
+  }
+  double* block;
+  double* ex_block;
 };
 
 // Kernel variants (unroll depth = row slots per lane group per step, and
@@ -160,8 +171,10 @@ struct Ctx {
 // fe_plan_set_option(FE_OPT_EXPAND_VARIANT / FE_OPT_SEGSUM_VARIANT) selects
 // another, which is how the tuner compares them.
 //   expand: 0 U=2 PF, 1 U=4 PF, 2 U=2 no-PF, 3 U=4 no-PF
-//   segsum: 0 U=8 no-PF, 1 U=4 PF, 2 U=8 PF, 3 U=4 no-PF
+//   segsum: 0 U=8 no-PF, 1 U=4 PF, 2 U=8 PF, 3 U=4 no-PF,
+//           4 cp.async ring U=4 x 4 stages, 5 cp.async ring U=2 x 6 stages
 constexpr int kVariants = 4;
+constexpr int kSegVariants = 6;
 template <int C> struct Tune {
   static constexpr int kPU = 4;
 };
@@ -186,8 +199,7 @@ static void expand_kbu(Ctx& c, Tab tab, Epi epi, double* part, void* fuse_sum) {
   const unsigned grid = (unsigned)(c.its->ex.size() / kWarps);
   const ExpandItem* items = c.its->d_ex.as<ExpandItem>();
   const int64_t n = (int64_t)c.its->ex.size();
-  FuseArgs fz{static_cast<double*>(fuse_sum), c.its->d_ex_splits.as<SplitLevel>(), c.ex_piece,
-              c.its->ex_n_pieces, c.its->d_ex_split_cnt.as<int32_t>()};
+  FuseArgs fz{static_cast<double*>(fuse_sum), c.ex_split()};
   if (fuse_sum)
     k_expand<TA, C, U, KB, true, PF, Tab, Epi><<<grid, kThreads, 0, c.s>>>(c.d, items, n, tab, epi,
                                                                           part, c.its->Se, fz);
@@ -223,6 +235,22 @@ static int launch_expand(Ctx& c, Tab tab, Epi epi, double* part, const char* nam
   return 0;
 }
 
+template <typename TA, int C, int U, int S, class Load>
+static int launch_segsum_async(Ctx& c, Load ld, TA* out, const ReduceItem* items, int64_t n,
+                               unsigned grid) {
+  using L = AsyncSegLayout<TA, C, U, S>;
+  const int smem = kWarps * L::kWarpBytes;
+  static bool attr_set = false;  // per instantiation (set once per process)
+  if (!attr_set) {
+    FE_CK(cudaFuncSetAttribute(k_segsum_async<TA, C, U, S, Load>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    attr_set = true;
+  }
+  k_segsum_async<TA, C, U, S, Load><<<grid, kThreads, smem, c.s>>>(c.d, items, n, ld, out,
+                                                                    c.seg_split());
+  return 0;
+}
+
 // all_fes: reduce every FE; otherwise skip the primary (reduced by a fused
 // expand).
 template <typename TA, int C, class Load>
@@ -233,25 +261,29 @@ static int launch_segsum(Ctx& c, Load ld, TA* out, const char* name, double byte
   ProfScope ps(c.pl, name, bytes);
   const unsigned grid = (unsigned)((n + kWarps - 1) / kWarps);
   const ReduceItem* items = c.its->d_rd.as<ReduceItem>();
-  const SplitLevel* sp = c.its->d_splits.as<SplitLevel>();
-  int32_t* cnt = c.its->d_split_cnt.as<int32_t>();
+  const SplitArgs sa = c.seg_split();
   const int var = pick_seg(c.pl);
+  if constexpr (Load::kAsyncable) {
+    if (var == 4 || var == 5) {
+      const int st = var == 4 ? launch_segsum_async<TA, C, 4, 4>(c, ld, out, items, n, grid)
+                              : launch_segsum_async<TA, C, 2, 6>(c, ld, out, items, n, grid);
+      if (st) return st;
+      FE_CK(cudaGetLastError());
+      return 0;
+    }
+  }
   switch (var) {
     case 1:
-      k_segsum<TA, C, 4, true, Load><<<grid, kThreads, 0, c.s>>>(c.d, items, n, ld, out, sp, c.piece,
-                                                                 c.its->n_pieces, cnt);
+      k_segsum<TA, C, 4, true, Load><<<grid, kThreads, 0, c.s>>>(c.d, items, n, ld, out, sa);
       break;
     case 2:
-      k_segsum<TA, C, 8, true, Load><<<grid, kThreads, 0, c.s>>>(c.d, items, n, ld, out, sp, c.piece,
-                                                                 c.its->n_pieces, cnt);
+      k_segsum<TA, C, 8, true, Load><<<grid, kThreads, 0, c.s>>>(c.d, items, n, ld, out, sa);
       break;
     case 3:
-      k_segsum<TA, C, 4, false, Load><<<grid, kThreads, 0, c.s>>>(c.d, items, n, ld, out, sp, c.piece,
-                                                                  c.its->n_pieces, cnt);
+      k_segsum<TA, C, 4, false, Load><<<grid, kThreads, 0, c.s>>>(c.d, items, n, ld, out, sa);
       break;
     default:
-      k_segsum<TA, C, 8, false, Load><<<grid, kThreads, 0, c.s>>>(c.d, items, n, ld, out, sp, c.piece,
-                                                                  c.its->n_pieces, cnt);
+      k_segsum<TA, C, 8, false, Load><<<grid, kThreads, 0, c.s>>>(c.d, items, n, ld, out, sa);
       break;
   }
   FE_CK(cudaGetLastError());
@@ -376,6 +408,8 @@ static int prepare(fe_plan* pl, int C, int sT, bool mixed, Ctx& c) {
   if ((st = w.S.ensure(P * nC * 8))) return st;
   if ((st = w.piece_part.ensure((size_t)std::max<int64_t>(its->n_pieces, 1) * nC * 8))) return st;
   if ((st = w.ex_piece_part.ensure((size_t)std::max<int64_t>(its->ex_n_pieces, 1) * nC * 8))) return st;
+  if ((st = w.block_part.ensure((size_t)std::max<int64_t>(its->n_blocks, 1) * nC * 8))) return st;
+  if ((st = w.ex_block_part.ensure((size_t)std::max<int64_t>(its->ex_n_blocks, 1) * nC * 8))) return st;
   if ((st = w.inst.ensure((size_t)pl->nprob * nC * sizeof(Inst)))) return st;
   if ((st = w.counters.ensure(64))) return st;
   if (!pl->host_pinned) FE_CK(cudaMallocHost(&pl->host_pinned, 64));
@@ -394,6 +428,8 @@ static int prepare(fe_plan* pl, int C, int sT, bool mixed, Ctx& c) {
   c.part_b = w.part_b.as<double>();
   c.piece = w.piece_part.as<double>();
   c.ex_piece = w.ex_piece_part.as<double>();
+  c.block = w.block_part.as<double>();
+  c.ex_block = w.ex_block_part.as<double>();
   c.S = w.S.p;
   // coefficient-side slabs start at zero (levels without observations and
   // the null levels are never written afterwards)
@@ -470,6 +506,69 @@ static void init_insts(fe_plan* pl, const SolveReq& rq, int C, int ncols, std::v
 }
 
 // ---------------------------------------------------------------------------
+// CUDA-graph replay of the LSMR loop: `body` enqueues one iteration; m of them
+// are captured once per (tile width, precision) and workspace layout, then
+// replayed between host convergence checks.  Every per-iteration quantity
+// lives in device memory (the Inst array), so the launches are identical from
+// one iteration to the next.  Profiling mode launches directly instead (its
+// per-launch CUDA events cannot be read back from inside a graph).
+// ---------------------------------------------------------------------------
+template <class Body>
+static int run_loop(fe_plan* pl, Ctx& c, int prec, int64_t cap, int32_t nact0, Body body,
+                    int64_t* done_iters) {
+  int32_t nact = nact0;
+  const int m = std::max(1, pl->opt_check_every);
+  int64_t it = 0;
+  const bool graph = pl->opt_graph != 0 && !pl->prof.on;
+  LoopGraph* lg = nullptr;
+  if (graph) {
+    size_t key = (size_t)c.C * 1000003u ^ (size_t)m;
+    const void* ptrs[] = {c.inst, c.part_e, c.part_a, c.part_b, c.piece, c.ex_piece, c.S,
+                          c.block, c.ex_block, pl->ws.U.p, pl->ws.V.p, pl->ws.H.p, pl->ws.Hb.p,
+                          pl->ws.X.p, c.its, c.counters, c.s};
+    for (const void* p : ptrs) key = key * 1315423911u + (size_t)p;
+    key = key * 31 + (size_t)cur_tune().ex * 7 + (size_t)cur_tune().seg;
+    lg = &pl->graphs[{c.C, prec}];
+    if (!lg->exec || lg->key != key) {
+      if (lg->exec) {
+        cudaGraphExecDestroy(lg->exec);
+        lg->exec = nullptr;
+      }
+      cudaGraph_t g = nullptr;
+      FE_CK(cudaStreamBeginCapture(c.s, cudaStreamCaptureModeThreadLocal));
+      int st = 0;
+      for (int r = 0; r < m && !st; ++r) st = body();
+      const cudaError_t e = cudaStreamEndCapture(c.s, &g);
+      if (st) {
+        if (g) cudaGraphDestroy(g);
+        return st;
+      }
+      FE_CK(e);
+      const cudaError_t ei = cudaGraphInstantiate(&lg->exec, g, 0);
+      cudaGraphDestroy(g);
+      FE_CK(ei);
+      lg->key = key;
+    }
+  }
+  while (nact > 0 && it < cap) {
+    if (graph) {
+      FE_CK(cudaGraphLaunch(lg->exec, c.s));
+      it += m;
+    } else {
+      for (int r = 0; r < m; ++r) {
+        int st = body();
+        if (st) return st;
+      }
+      it += m;
+    }
+    int st = read_counter(c, 0, &nact);
+    if (st) return st;
+  }
+  if (done_iters) *done_iters = it;
+  return 0;
+}
+
+// ---------------------------------------------------------------------------
 // autotuner: the expand and segsum variants of the LSMR loop timed on this
 // plan's own index data (values are irrelevant to the timing: U and V are
 // zeroed scratch), best of two launches each; the winner is kept per (C, T)
@@ -539,7 +638,7 @@ static int autotune(fe_plan* pl, Ctx& c) {
       ex = v;
     }
   }
-  for (int v = 0; v < kVariants && !st; ++v) {
+  for (int v = 0; v < kSegVariants && !st; ++v) {
     pl->opt_seg_variant = v;
     float ms = 1e30f;
     for (int rep = 0; rep < 3 && !st; ++rep) {
@@ -646,19 +745,18 @@ static int solve_plain_tile(fe_plan* pl, const SolveReq& rq, int64_t col0, int n
   ee.U = U;
   ee.inst = c.inst;
   const int64_t cap = std::max<int64_t>(rq.maxiter, 1) + 2;
-  for (int64_t it = 1; nact > 0 && it <= cap; ++it) {
-    if ((st = launch_expand<T, C>(c, TabOne<T, T, vec_of<T, C>()>{V}, ee, c.part_e, "expand", by.expand,
-                                  fs)))
-      return st;
-    if ((st = launch_scalar_phase(c, PH_BETA, 0))) return st;
-    if ((st = launch_segsum<T, C>(c, LoadIn<T, T, vec_of<T, C>()>{U}, ST, "segsum", by.segsum, !fuse)))
-      return st;
-    if ((st = launch_pupdate<C>(c, ST, pe, c.part_a, c.part_b, "pupdate", by.pupdate))) return st;
-    if ((st = launch_scalar_phase(c, PH_ALPHA, 0))) return st;
-    if (it % pl->opt_check_every == 0 || it == cap) {
-      if ((st = read_counter(c, 0, &nact))) return st;
-    }
-  }
+  auto body = [&]() -> int {
+    int e;
+    if ((e = launch_expand<T, C>(c, TabOne<T, T, vec_of<T, C>()>{V}, ee, c.part_e, "expand", by.expand,
+                                 fs)))
+      return e;
+    if ((e = launch_scalar_phase(c, PH_BETA, 0))) return e;
+    if ((e = launch_segsum<T, C>(c, LoadIn<T, T, vec_of<T, C>()>{U}, ST, "segsum", by.segsum, !fuse)))
+      return e;
+    if ((e = launch_pupdate<C>(c, ST, pe, c.part_a, c.part_b, "pupdate", by.pupdate))) return e;
+    return launch_scalar_phase(c, PH_ALPHA, 0);
+  };
+  if ((st = run_loop(pl, c, (int)sizeof(T), cap, nact, body, nullptr))) return st;
   if (rq.residuals) {
     // r = b - A x (src/AbstractFixedEffectSolver.jl:62)
     if ((st = launch_expand<T, C>(c, TabOne<T, T, vec_of<T, C>()>{X},
@@ -700,7 +798,7 @@ static int solve_mixed_tile(fe_plan* pl, const SolveReq& rq, int64_t col0, int n
   double* R64 = w.R64.as<double>();
   double* S64 = static_cast<double*>(c.S);
   float* S32 = static_cast<float*>(c.S);
-  if (rq.residuals) {
+  if (rq.residuals && pl->opt_mixed_warm) {
     if ((st = launch_segsum<double, C>(c, LoadIn<double, double, vec_of<double, C>()>{B64}, S64, "segsum_warm", 0.0)))
       return st;
     if ((st = launch_pupdate<C>(c, S64, PEpiStoreX<double, vec_of<double, C>()>{X64, true}, nullptr, nullptr,
@@ -741,21 +839,21 @@ static int solve_mixed_tile(fe_plan* pl, const SolveReq& rq, int64_t col0, int n
     int32_t nout = 0;
     if ((st = read_counter(c, 1, &nout))) return st;
     if (nout == 0) break;
-    int32_t nact = nout;
-    for (int64_t it = 1; nact > 0 && total_it < cap; ++it, ++total_it) {
-      if ((st = launch_expand<float, C>(c, TabOne<float, float, vec_of<float, C>()>{V}, ee, c.part_e,
-                                        "expand", by.expand, fs)))
-        return st;
-      if ((st = launch_scalar_phase(c, PH_BETA, 0))) return st;
-      if ((st = launch_segsum<float, C>(c, LoadIn<float, float, vec_of<float, C>()>{U}, S32, "segsum",
-                                        by.segsum, !fuse)))
-        return st;
-      if ((st = launch_pupdate<C>(c, S32, pe, c.part_a, c.part_b, "pupdate", by.pupdate))) return st;
-      if ((st = launch_scalar_phase(c, PH_ALPHA, 0))) return st;
-      if (it % pl->opt_check_every == 0) {
-        if ((st = read_counter(c, 0, &nact))) return st;
-      }
-    }
+    auto body = [&]() -> int {
+      int e;
+      if ((e = launch_expand<float, C>(c, TabOne<float, float, vec_of<float, C>()>{V}, ee, c.part_e,
+                                       "expand", by.expand, fs)))
+        return e;
+      if ((e = launch_scalar_phase(c, PH_BETA, 0))) return e;
+      if ((e = launch_segsum<float, C>(c, LoadIn<float, float, vec_of<float, C>()>{U}, S32, "segsum",
+                                       by.segsum, !fuse)))
+        return e;
+      if ((e = launch_pupdate<C>(c, S32, pe, c.part_a, c.part_b, "pupdate", by.pupdate))) return e;
+      return launch_scalar_phase(c, PH_ALPHA, 0);
+    };
+    int64_t done = 0;
+    if ((st = run_loop(pl, c, 1, cap - total_it, nout, body, &done))) return st;
+    total_it += done;
   }
   if (rq.residuals) {
     if ((st = unload_tile(pl, c, rq, col0, ncols))) return st;

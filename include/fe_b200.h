@@ -59,11 +59,16 @@ extern "C" {
 #define FE_OPT_INNER_RHO 5   /* FP32 inner-solve floor (relative ||A'r|| drop) */
 #define FE_OPT_FUSE 6        /* 1: reduce the primary FE inside the expand (default 0) */
 #define FE_OPT_EXPAND_VARIANT 7 /* expand kernel variant 0..3, -1 = default */
-#define FE_OPT_SEGSUM_VARIANT 8 /* segsum kernel variant 0..3, -1 = default */
+#define FE_OPT_SEGSUM_VARIANT 8 /* segsum kernel variant 0..5, -1 = default */
 #define FE_OPT_AUTOTUNE 9    /* 1 (default): time the kernel variants on the first
                                 solve of a tile shape; the choice is kept in the
                                 plan and in the tuning cache file
                                 ($FE_B200_TUNE_CACHE, "off" disables) */
+#define FE_OPT_MIXED_WARM_START 10 /* FE_PREC_MIXED residual solves start from
+                                      x0 = A'b like the reference (1, default)
+                                      or from x0 = 0 (0) */
+#define FE_OPT_GRAPH 11      /* 1 (default): replay the LSMR iterations between host
+                                convergence checks from a captured CUDA graph */
 
 typedef struct fe_plan fe_plan;
 

@@ -314,3 +314,45 @@ def test_autotuner_persists_choice(fe, synth, tmp_path, monkeypatch):
     feM.close()
     assert len(cache.read_text().strip().splitlines()) == 1
     assert np.array_equal(R1, R2)
+
+
+@pytest.mark.parametrize("tile", [32, 8, 1])
+def test_every_kernel_variant_matches_oracle(fe, synth, oracle, tile):
+    # Zipf firms (split levels), a 20-level FE, weights: every code path of the
+    # expand and segsum variants the autotuner can pick
+    pb = synth.make(4, scale=0.0003, ncols=3)
+    rng = np.random.default_rng(5)
+    yr = rng.integers(1, 21, pb.N)
+    refs = pb.refs + [yr]
+    nlev = pb.nlev + [20]
+    fes = [fe.FixedEffect.from_refs(r, n) for r, n in zip(refs, nlev)]
+    Y = np.asfortranarray(pb.Y.astype(np.float64))
+    R_o, _, _ = oracle.solve_residuals_cols(Y, refs, nlev, None, pb.weights, tol=1e-8)
+    for prec in ("fp64", "mixed"):
+        feM = fe.AbstractFixedEffectSolver(fes, pb.weights, "CUDA", np.float64, precision=prec)
+        feM.set_option(fe._lib.FE_OPT_TILE, tile)
+        for ev, sv in [(0, 0), (1, 1), (2, 2), (3, 3), (0, 4), (3, 5)]:
+            feM.set_option(fe._lib.FE_OPT_EXPAND_VARIANT, ev)
+            feM.set_option(fe._lib.FE_OPT_SEGSUM_VARIANT, sv)
+            R, its, cvs = feM.solve_residuals(Y.copy(), tol=1e-8)
+            assert cvs.all(), (prec, ev, sv)
+            err = max(rel_err(R[:, j], R_o[:, j]) for j in range(Y.shape[1]))
+            assert err < REL, (prec, ev, sv, err)
+        feM.close()
+
+
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_graph_replay_matches_direct_launches(fe, synth, prec):
+    pb = synth.make(0, scale=0.05)
+    fes = [fe.FixedEffect.from_refs(r, n) for r, n in zip(pb.refs, pb.nlev)]
+    Y = np.asfortranarray(np.repeat(pb.Y.astype(np.float64), 3, axis=1))
+    out = []
+    for graph in (1, 0):
+        feM = fe.AbstractFixedEffectSolver(fes, None, "CUDA", np.float64, precision=prec)
+        feM.set_option(fe._lib.FE_OPT_GRAPH, graph)
+        R, its, cvs = feM.solve_residuals(Y.copy(), tol=1e-8)
+        R2, its2, _ = feM.solve_residuals(Y.copy(), tol=1e-8)  # a replay of the cached graph
+        feM.close()
+        assert cvs.all() and np.array_equal(R, R2) and np.array_equal(its, its2)
+        out.append((R, its))
+    assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
