@@ -23,6 +23,8 @@ constexpr int kWarps = 8;          // warps per CTA in the expand/reduce kernels
 constexpr int kThreads = kWarps * 32;
 constexpr int kScalarThreads = 256;
 constexpr int kSentinel = 0x7fffffff;  // "no level" key
+constexpr int kSmallRows = 32;         // rows of the row-sum pass's small-FE tables
+constexpr int kRowSumSmallFE = 2;      // small FEs the row-sum pass reduces
 
 // A contiguous range of observations (sorted order) processed by one warp.
 // Items hold whole levels of the primary FE (the FE that orders the

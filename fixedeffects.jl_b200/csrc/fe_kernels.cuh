@@ -90,6 +90,29 @@ __device__ __forceinline__ void vst(T* p, const VA<T, V>& a) {
   for (int q = 0; q < IO::kN; ++q) reinterpret_cast<typename IO::Cr*>(p)[q] = c[q];
 }
 
+// Asynchronous global -> shared copies (cp.async, hand-written PTX).
+__device__ __forceinline__ void cp_async_bytes16(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem));
+}
+__device__ __forceinline__ void cp_async_bytes8(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem));
+}
+__device__ __forceinline__ void cp_async_bytes4(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem));
+}
+template <int B>
+__device__ __forceinline__ void cp_async(void* smem, const void* gmem) {
+  if (B == 16) cp_async_bytes16(smem, gmem);
+  else if (B == 8) cp_async_bytes8(smem, gmem);
+  else cp_async_bytes4(smem, gmem);
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+
 // lane shape for accumulation type TA and tile width C
 template <typename TA, int C>
 struct Shape {
@@ -400,21 +423,11 @@ struct SegRun {
 // that every index and row load of a step can be issued before the first is
 // consumed).  The next step's refs and weights are prefetched while the
 // current step's rows are in flight.
-//
-// FUSE: the observations are sorted by the primary FE, so the new values are
-// also reduced by that FE here (the reference's gather! for it,
-// src/SolverCPU.jl:21-27): a contiguous segmented sum of cw * new value per
-// primary level, stored to Sf.  The separate segsum then skips the primary.
 // ---------------------------------------------------------------------------
-struct FuseArgs {
-  double* sum;  // [P][C] sum slab (TA-typed), null when not fused
-  SplitArgs sa;
-};
-
-template <typename TA, int C, int U, int KB, bool FUSE, bool PF, class Tab, class Epi>
+template <typename TA, int C, int U, int KB, bool PF, class Tab, class Epi>
 __global__ void __launch_bounds__(kThreads)
 k_expand(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_items, Tab tab, Epi epi,
-         double* __restrict__ part, int64_t S, FuseArgs fz) {
+         double* __restrict__ part, int64_t S) {
   using Sh = Shape<TA, C>;
   constexpr int VEC = Sh::VEC, CL = Sh::CL, G = Sh::G;
   constexpr int STEP = G * U;                     // observations per step
@@ -434,13 +447,9 @@ k_expand(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_items, T
     epi.begin(it.prob, jl, C);
     if (__any_sync(FE_FULL, epi.act)) {
       const int K = d.K;
-      const int kp = d.primary;
       TN nit[VEC];  // norms of this item (FP32 for the FP32 path), flushed below
 #pragma unroll
       for (int v = 0; v < VEC; ++v) nit[v] = TN(0);
-      SegRun<TA, VEC, CL, G> run;
-      run.init();
-      TA* Sf = FUSE ? reinterpret_cast<TA*>(fz.sum) + d.lev_base[kp] * C + jl * VEC : nullptr;
       int rl[KB][NI];
       TA cl[KB][NI];
       auto fetch = [&](int64_t base) {
@@ -471,15 +480,11 @@ k_expand(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_items, T
         if (PF && base + STEP < it.ie) fetch(base + STEP);
         VA<TP, VEC> old[U];
         VA<TA, VEC> s[U];
-        int pkey[U];
-        TA pcw[U];
 #pragma unroll
         for (int u = 0; u < U; ++u) {
           const int64_t i = base + u * G + g;
 #pragma unroll
           for (int v = 0; v < VEC; ++v) s[u].v[v] = TA(0);
-          pkey[u] = kSentinel;
-          pcw[u] = TA(0);
           if (i < it.ie && epi.act) old[u] = epi.pre(i * C + jl * VEC);
         }
 #pragma unroll
@@ -492,10 +497,6 @@ k_expand(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_items, T
               const int q = u * G;  // + g: the same index register (G divides 32)
               const int ref = __shfl_sync(FE_FULL, rc[k][q >> 5], (q & 31) + g);
               const TA c = __shfl_sync(FE_FULL, cc[k][q >> 5], (q & 31) + g);
-              if (FUSE && k == kp) {
-                pkey[u] = ref;
-                pcw[u] = c;
-              }
               const int64_t i = base + u * G + g;
               if (i < it.ie && epi.act) {
                 const TA cs = c * __ldg(sc + ref);
@@ -509,22 +510,9 @@ k_expand(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_items, T
 #pragma unroll
         for (int u = 0; u < U; ++u) {
           const int64_t i = base + u * G + g;
-          VA<TA, VEC> nv;
-#pragma unroll
-          for (int v = 0; v < VEC; ++v) nv.v[v] = TA(0);
-          if (i < it.ie && epi.act) nv = epi.apply(i * C + jl * VEC, s[u], old[u], nit);
-          if (FUSE) {
-            const int64_t b0 = base + (int64_t)u * G;
-            if (b0 < it.ie) {  // warp-uniform
-              const int nvalid = (int)((it.ie - b0) < G ? (it.ie - b0) : G);
-#pragma unroll
-              for (int v = 0; v < VEC; ++v) nv.v[v] *= pcw[u];
-              run.push(i < it.ie ? pkey[u] : kSentinel, nv, nvalid, g, jl, C, Sf);
-            }
-          }
+          if (i < it.ie && epi.act) (void)epi.apply(i * C + jl * VEC, s[u], old[u], nit);
         }
       }
-      if (FUSE) run.finish(it.split, it.piece, fz.sa, g, jl, C, Sf, sm[wib]);
 #pragma unroll
       for (int v = 0; v < VEC; ++v) nrm[v] += (double)nit[v];
     }
@@ -534,10 +522,221 @@ k_expand(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_items, T
 }
 
 // ---------------------------------------------------------------------------
+// k_rowsum: the reductions that need no gather (the reference's gather!,
+// src/SolverCPU.jl:21-27, for those FEs) in one contiguous pass over the
+// sorted observation rows of a 32-column tile:
+//   - the primary FE: observations are sorted by it, so each of its levels is
+//     a contiguous run of rows;
+//   - small FEs (at most kSmallRows table rows in total, e.g. a year FE):
+//     summed into a per-warp table in shared memory.
+// One column per lane.  A step loads the keys (and weights) of STEP rows with
+// one coalesced load per FE and the STEP rows themselves (STEP independent
+// loads per lane, 4 KB per warp in flight), then walks them in order: a
+// primary level is stored at each key change, and every row is added into the
+// small-FE tables.  The segsum then gathers only the remaining (large) FEs.
+//
+// Work split: CTA b takes the contiguous item range
+// [b n / grid, (b+1) n / grid) of the expand items (whole primary levels, or
+// pieces of long ones) and its warps take every 8th item of it, so the
+// tables' summation order depends only on the grid size.  At the end the 8
+// warp tables are summed (warp order, FP64) into the CTA's partial slot;
+// k_small_combine sums the slots in CTA order into the [P][C] slab.
+// ---------------------------------------------------------------------------
+struct RowSumArgs {
+  void* sum;                  // [P][C] TA slab: primary level sums
+  SplitArgs sa;               // pieces of long primary levels
+  double* small_part;         // [grid][small_rows][C] CTA partials of the small FEs
+  int32_t n_small;            // small FEs (<= kRowSumSmallFE)
+  int32_t small_fe[kRowSumSmallFE];
+  int32_t small_off[kRowSumSmallFE];  // first table row of each
+  int32_t small_rows;         // table rows in use
+};
+
+// rows per step: 4 KB of rows per warp (one buffer of the double buffer)
+template <typename TA> struct RowSumStep {
+  static constexpr int value = sizeof(TA) == 4 ? 32 : 16;
+};
+
+// One row of the walk: r is the row within the step (a compile-time constant
+// in the unrolled full-step walk).
+template <typename TA, int C, bool W, int NS>
+__device__ __forceinline__ void rowsum_row(int r, const TA* __restrict__ rows, TA& acc,
+                                           uint32_t bmask, int kpr, TA cpv, int k0, TA c0, int k1,
+                                           TA c1, TA* __restrict__ Sf, TA* __restrict__ tbl,
+                                           int lane) {
+  const TA x = rows[r * C];
+  acc += W ? x * __shfl_sync(FE_FULL, cpv, r) : x;
+  if ((bmask >> r) & 1u) {
+    const int kr = __shfl_sync(FE_FULL, kpr, r);
+    Sf[(int64_t)kr * C] = acc;
+    acc = TA(0);
+  }
+  if (NS > 0) {
+    const int t0 = __shfl_sync(FE_FULL, k0, r);
+    tbl[t0 * C + lane] += W ? x * __shfl_sync(FE_FULL, c0, r) : x;
+  }
+  if (NS > 1) {
+    const int t1 = __shfl_sync(FE_FULL, k1, r);
+    tbl[t1 * C + lane] += W ? x * __shfl_sync(FE_FULL, c1, r) : x;
+  }
+}
+
+// W: some reduced FE has weights (cw); NS: small FEs reduced in the tables.
+template <typename TA, int C, bool W, int NS>
+__global__ void __launch_bounds__(kThreads, 4)
+k_rowsum(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_items,
+         const TA* __restrict__ src, RowSumArgs rs) {
+  static_assert(C == 32, "the walk puts one column on each lane");
+  constexpr int STEP = RowSumStep<TA>::value;
+  constexpr int BUF = STEP * C;                               // elements per buffer
+  constexpr int CHUNKS = BUF * (int)sizeof(TA) / 16 / 32;     // 16-byte copies per lane
+  constexpr int ROWCH = C * (int)sizeof(TA) / 16;             // 16-byte chunks per row
+  __shared__ double smt[kWarps][32];
+  extern __shared__ __align__(16) unsigned char rowsum_smem[];
+  const int lane = threadIdx.x & 31;
+  const int wib = threadIdx.x >> 5;
+  TA* wbuf = reinterpret_cast<TA*>(rowsum_smem) + (size_t)wib * 2 * BUF;     // 2 row buffers
+  TA* tbl = reinterpret_cast<TA*>(rowsum_smem) + (size_t)kWarps * 2 * BUF +  // small-FE table
+            (size_t)wib * rs.small_rows * C;
+  for (int e = lane; e < rs.small_rows * C; e += 32) tbl[e] = TA(0);
+  __syncwarp();
+  const int kp = d.primary;
+  TA* __restrict__ Sf = reinterpret_cast<TA*>(rs.sum) + d.lev_base[kp] * C + lane;
+  const int32_t* __restrict__ refp = d.refs[kp];
+  const TA* __restrict__ cwp = cw_of<TA>(d, kp);
+  const int32_t* __restrict__ ref0 = NS > 0 ? d.refs[rs.small_fe[0]] : nullptr;
+  const int32_t* __restrict__ ref1 = NS > 1 ? d.refs[rs.small_fe[1]] : nullptr;
+  const TA* __restrict__ cw0 = NS > 0 ? cw_of<TA>(d, rs.small_fe[0]) : nullptr;
+  const TA* __restrict__ cw1 = NS > 1 ? cw_of<TA>(d, rs.small_fe[1]) : nullptr;
+  const int off0 = rs.small_off[0], off1 = rs.small_off[1];
+  const int64_t w0 = (int64_t)blockIdx.x * n_items / gridDim.x;
+  const int64_t w1 = (int64_t)(blockIdx.x + 1) * n_items / gridDim.x;
+  for (int64_t wi = w0 + wib; wi < w1; wi += kWarps) {
+    const ExpandItem it = items[wi];
+    const int64_t ie = it.ie;
+    if (ie <= it.ib) continue;
+    // copy the rows of the step at `base` into buffer b (one commit group)
+    auto issue = [=](int64_t base, int b) {
+      const int nv = (int)((ie - base) < STEP ? (ie - base) : STEP);
+      const unsigned char* g = reinterpret_cast<const unsigned char*>(src + base * C);
+      unsigned char* sp = reinterpret_cast<unsigned char*>(wbuf + b * BUF);
+#pragma unroll
+      for (int q = 0; q < CHUNKS; ++q) {
+        const int ch = q * 32 + lane;
+        if (ch < nv * ROWCH) cp_async_bytes16(sp + ch * 16, g + ch * 16);
+      }
+      cp_async_commit();
+    };
+    // keys and weights of the step at `base` (row base + lane); a missing
+    // weight vector reads as 1
+    int kpr_n = kSentinel, k0_n = 0, k1_n = 0;
+    TA cp_n = TA(1), c0_n = TA(1), c1_n = TA(1);
+    auto keys = [&kpr_n, &k0_n, &k1_n, &cp_n, &c0_n, &c1_n, ie, lane, refp, cwp, ref0, ref1, cw0,
+                 cw1, off0, off1](int64_t base) {
+      const int64_t p = base + lane;
+      const bool ok = lane < STEP && p < ie;
+      kpr_n = ok ? __ldg(refp + p) : kSentinel;
+      if (W) cp_n = (ok && cwp) ? __ldg(cwp + p) : TA(1);
+      if (NS > 0) {
+        k0_n = ok ? off0 + __ldg(ref0 + p) : 0;
+        if (W) c0_n = (ok && cw0) ? __ldg(cw0 + p) : TA(1);
+      }
+      if (NS > 1) {
+        k1_n = ok ? off1 + __ldg(ref1 + p) : 0;
+        if (W) c1_n = (ok && cw1) ? __ldg(cw1 + p) : TA(1);
+      }
+    };
+    issue(it.ib, 0);
+    keys(it.ib);
+    int ckey = -1;  // primary level of the open run (warp-uniform)
+    TA acc = TA(0);
+    int b = 0;
+    for (int64_t base = it.ib; base < ie; base += STEP, b ^= 1) {
+      const int kpr = kpr_n, k0 = k0_n, k1 = k1_n;
+      const TA cpv = cp_n, c0 = c0_n, c1 = c1_n;
+      const int nvalid = (int)((ie - base) < STEP ? (ie - base) : STEP);
+      if (base + STEP < ie) {
+        issue(base + STEP, b ^ 1);
+        keys(base + STEP);
+        cp_async_wait<1>();
+      } else {
+        cp_async_wait<0>();
+      }
+      __syncwarp();  // every lane's copies of this step are visible
+      const int kn = __shfl_down_sync(FE_FULL, kpr, 1);
+      const uint32_t bmask = __ballot_sync(FE_FULL, lane + 1 < nvalid && kn != kpr);
+      const int kfirst = __shfl_sync(FE_FULL, kpr, 0);
+      if (ckey >= 0 && ckey != kfirst) {
+        Sf[(int64_t)ckey * C] = acc;
+        acc = TA(0);
+      }
+      const TA* __restrict__ rows = wbuf + b * BUF + lane;
+      if (nvalid == STEP) {
+#pragma unroll
+        for (int r = 0; r < STEP; ++r)
+          rowsum_row<TA, C, W, NS>(r, rows, acc, bmask, kpr, cpv, k0, c0, k1, c1, Sf, tbl, lane);
+      } else {
+#pragma unroll 1
+        for (int r = 0; r < nvalid; ++r)
+          rowsum_row<TA, C, W, NS>(r, rows, acc, bmask, kpr, cpv, k0, c0, k1, c1, Sf, tbl, lane);
+      }
+      ckey = __shfl_sync(FE_FULL, kpr, nvalid - 1);
+      __syncwarp();  // buffer b is free for the copies of step + 2
+    }
+    // the open run: a whole level, or one piece of a long one
+    SegRun<TA, 1, 32, 1> run;
+    run.ckey = ckey;
+    run.carry.v[0] = acc;
+    run.acc.v[0] = TA(0);
+    run.pend = false;
+    run.finish(it.split, it.piece, rs.sa, 0, lane, C, Sf, smt[wib]);
+  }
+  if (NS > 0) {
+    __syncthreads();
+    const int n = rs.small_rows * C;
+    double* __restrict__ out = rs.small_part + (int64_t)blockIdx.x * n;
+    const TA* t0 = reinterpret_cast<const TA*>(rowsum_smem) + (size_t)kWarps * 2 * BUF;
+    for (int e = threadIdx.x; e < n; e += kThreads) {
+      double t = 0.0;
+#pragma unroll
+      for (int w = 0; w < kWarps; ++w) t += (double)t0[(size_t)w * n + e];
+      out[e] = t;
+    }
+  }
+}
+
+// Small-FE level sums = the row-sum CTA partials summed in CTA order.  One
+// CTA per table row; thread t sums the slots q, q + Q, ... of column t % C
+// (Q = kThreads / C groups), and the groups are added in group order.
+struct SmallRows {
+  int64_t slab_row[kSmallRows];  // [P][C] slab row of each table row
+};
+template <typename TA, int C>
+__global__ void __launch_bounds__(kThreads)
+k_small_combine(const double* __restrict__ part, int nparts, int small_rows, SmallRows m,
+                TA* __restrict__ out) {
+  constexpr int Q = kThreads / C;
+  __shared__ double sm[Q][C];
+  const int row = blockIdx.x;
+  const int c = threadIdx.x % C, q = threadIdx.x / C;
+  double a = 0.0;
+  for (int b = q; b < nparts; b += Q) a += __ldcg(part + ((int64_t)b * small_rows + row) * C + c);
+  sm[q][c] = a;
+  __syncthreads();
+  if (threadIdx.x < C) {
+    double t = 0.0;
+#pragma unroll
+    for (int j = 0; j < Q; ++j) t += sm[j][threadIdx.x];
+    out[m.slab_row[row] * C + threadIdx.x] = (TA)t;
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Segmented-sum value loaders: the per-position vector summed into a level.
 // ---------------------------------------------------------------------------
 template <typename TIn, typename TA, int VEC>
 struct LoadIn {
+  using InType = TIn;
   const TIn* __restrict__ in;
   static constexpr bool kSquareWeight = false;
   static constexpr bool kAsyncable = std::is_same<TIn, TA>::value;  // raw rows can be copied
@@ -652,28 +851,6 @@ k_segsum(const FeDev d, const ReduceItem* __restrict__ items, int64_t n_items, L
 // data visible; keys and weights are copied by lane jl = 0 of each group and
 // shared through a __syncwarp.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ void cp_async_bytes16(void* smem, const void* gmem) {
-  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem));
-}
-__device__ __forceinline__ void cp_async_bytes8(void* smem, const void* gmem) {
-  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem));
-}
-__device__ __forceinline__ void cp_async_bytes4(void* smem, const void* gmem) {
-  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem));
-}
-template <int B>
-__device__ __forceinline__ void cp_async(void* smem, const void* gmem) {
-  if (B == 16) cp_async_bytes16(smem, gmem);
-  else if (B == 8) cp_async_bytes8(smem, gmem);
-  else cp_async_bytes4(smem, gmem);
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
-
 // shared memory per warp of k_segsum_async
 template <typename TA, int C, int U, int S>
 struct AsyncSegLayout {

@@ -436,8 +436,28 @@ int plan_items(fe_plan* pl, int C, ItemSet** out) {
   const int K = pl->K;
   its->ex_slot_off.assign((size_t)nprob + 1, 0);
   its->pu_slot_off.assign((size_t)nprob + 1, 0);
-  std::vector<ReduceItem> rd_prim;
+  std::vector<ReduceItem> rd_prim, rd_small;
   const int kp = pl->primary;
+  its->sms = sms;
+  // small FEs (32-column tiles of single-problem plans): the non-primary FEs
+  // with the fewest levels whose tables (levels + null level) fit kSmallRows
+  if (C == 32 && pl->nprob == 1) {
+    std::vector<int> order;
+    for (int k = 0; k < pl->K; ++k)
+      if (k != pl->primary) order.push_back(k);
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int a, int b) { return pl->nlev[a] < pl->nlev[b]; });
+    int nsmall = 0;
+    for (int k : order) {
+      const int64_t rows = pl->nlev[k] + 1;
+      if (its->small_rows + rows > kSmallRows || nsmall == kRowSumSmallFE) break;
+      ++nsmall;
+      its->small_mask |= 1u << k;
+      its->small_off[k] = its->small_rows;
+      for (int64_t l = 0; l < rows; ++l) its->small_slab_row.push_back(pl->lev_base[k] + l);
+      its->small_rows += (int32_t)rows;
+    }
+  }
   for (int p = 0; p < nprob; ++p) {
     // expand items: whole primary levels of the problem's sorted range packed
     // up to Te observations (a longer level is cut into pieces), padded so
@@ -507,7 +527,8 @@ int plan_items(fe_plan* pl, int C, ItemSet** out) {
     // level is cut into pieces.  Items of the primary FE go to a second list
     // (appended after all others): the fused expand reduces that FE itself.
     for (int k = 0; k < K; ++k) {
-      std::vector<ReduceItem>& dst = (k == kp) ? rd_prim : its->rd;
+      std::vector<ReduceItem>& dst =
+          (k == kp) ? rd_prim : (((its->small_mask >> k) & 1u) ? rd_small : its->rd);
       const int64_t lb = pl->prob_lev_off[(size_t)p * K + k];
       const int64_t le = pl->prob_lev_off[(size_t)(p + 1) * K + k];
       if (le == lb) continue;
@@ -550,6 +571,8 @@ int plan_items(fe_plan* pl, int C, ItemSet** out) {
       if (cur_b >= 0) dst.push_back({cur_b, cur_e, k, p, -1, 0});
     }
   }
+  its->rd_large = (int64_t)its->rd.size();
+  its->rd.insert(its->rd.end(), rd_small.begin(), rd_small.end());
   its->rd_np = (int64_t)its->rd.size();
   its->rd.insert(its->rd.end(), rd_prim.begin(), rd_prim.end());
   for (int p = 0; p < nprob; ++p) {

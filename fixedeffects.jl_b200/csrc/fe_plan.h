@@ -47,7 +47,16 @@ struct ItemSet {
   std::vector<ReduceItem> rd;
   std::vector<SplitLevel> splits;      // level pieces of the segsum items
   std::vector<SplitLevel> ex_splits;   // primary-level pieces of the expand items
-  int64_t rd_np = 0;                   // segsum items of non-primary FEs (first)
+  // segsum items are ordered [large non-primary FEs | small FEs | primary FE];
+  // the row-sum pass (32-column tiles of single-problem plans) reduces the last two
+  // groups itself, so the segsum then runs only the first rd_large items
+  int64_t rd_large = 0;
+  int64_t rd_np = 0;                   // items of non-primary FEs (first)
+  uint32_t small_mask = 0;             // FEs reduced in the row-sum tables
+  int32_t small_rows = 0;              // table rows (levels + null level)
+  int32_t small_off[kMaxFE] = {};      // first table row of each small FE
+  std::vector<int64_t> small_slab_row; // [P][C] slab row of each table row
+  int sms = 148;                       // multiprocessors of the plan's device
   int64_t ex_n_pieces = 0;
   std::vector<PItem> pu;
   std::vector<int64_t> ex_slot_off;       // per problem, expand norm slots (CTAs)
@@ -64,6 +73,7 @@ struct Workspace {
   DevBuf B64, R64, U, V, H, Hb, X, X64, S;
   DevBuf part_e, part_a, part_b, piece_part, ex_piece_part, block_part, ex_block_part, inst,
       counters;
+  DevBuf small_part;  // the row-sum CTA partials of the small FEs
   DevBuf coef;
   DevBuf ystage;  // device copy of host Y for host-buffer solves
 };
@@ -122,7 +132,7 @@ struct fe_plan {
   int32_t opt_unroll = 0;      // reserved
   double opt_inner_rho = 1e-8;
   double opt_inner_theta = 0.5;
-  int32_t opt_fuse = 0;        // reduce the primary FE inside the expand
+  int32_t opt_fuse = 1;        // row-sum pass: primary and small FEs reduced contiguously
   int32_t opt_ex_variant = -1; // expand kernel variant (-1: tuned default)
   int32_t opt_seg_variant = -1; // segsum kernel variant (-1: tuned default)
   int32_t opt_autotune = 1;     // time the variants on first use of a tile shape

@@ -164,6 +164,8 @@ struct Ctx {
   }
   double* block;
   double* ex_block;
+  double* small_part;  // the row-sum pass's CTA partials of the small FEs
+  bool rowsum;         // primary and small FEs reduced by the row-sum pass
 };
 
 // Kernel variants (unroll depth = row slots per lane group per step, and
@@ -195,44 +197,111 @@ inline int pick_seg(const fe_plan* pl) {
 template <typename T, int C> constexpr int vec_of() { return Shape<T, C>::VEC; }
 
 template <int KB, int U, bool PF, typename TA, int C, class Tab, class Epi>
-static void expand_kbu(Ctx& c, Tab tab, Epi epi, double* part, void* fuse_sum) {
+static int expand_kbu(Ctx& c, Tab tab, Epi epi, double* part) {
   const unsigned grid = (unsigned)(c.its->ex.size() / kWarps);
   const ExpandItem* items = c.its->d_ex.as<ExpandItem>();
   const int64_t n = (int64_t)c.its->ex.size();
-  FuseArgs fz{static_cast<double*>(fuse_sum), c.ex_split()};
-  if (fuse_sum)
-    k_expand<TA, C, U, KB, true, PF, Tab, Epi><<<grid, kThreads, 0, c.s>>>(c.d, items, n, tab, epi,
-                                                                          part, c.its->Se, fz);
-  else
-    k_expand<TA, C, U, KB, false, PF, Tab, Epi><<<grid, kThreads, 0, c.s>>>(c.d, items, n, tab, epi,
-                                                                           part, c.its->Se, fz);
+  k_expand<TA, C, U, KB, PF, Tab, Epi><<<grid, kThreads, 0, c.s>>>(c.d, items, n, tab, epi, part,
+                                                                   c.its->Se);
+  FE_CK(cudaGetLastError());
+  return 0;
 }
 
 template <int KB, typename TA, int C, class Tab, class Epi>
-static void expand_kb(Ctx& c, Tab tab, Epi epi, double* part, void* fuse_sum) {
+static int expand_kb(Ctx& c, Tab tab, Epi epi, double* part) {
   const int var = pick_ex(c.pl);
   switch (var) {
-    case 1: expand_kbu<KB, 4, true, TA, C>(c, tab, epi, part, fuse_sum); break;
-    case 2: expand_kbu<KB, 2, false, TA, C>(c, tab, epi, part, fuse_sum); break;
-    case 3: expand_kbu<KB, 4, false, TA, C>(c, tab, epi, part, fuse_sum); break;
-    default: expand_kbu<KB, 2, true, TA, C>(c, tab, epi, part, fuse_sum); break;
+    case 1: return expand_kbu<KB, 4, true, TA, C>(c, tab, epi, part);
+    case 2: return expand_kbu<KB, 2, false, TA, C>(c, tab, epi, part);
+    case 3: return expand_kbu<KB, 4, false, TA, C>(c, tab, epi, part);
+    default: return expand_kbu<KB, 2, true, TA, C>(c, tab, epi, part);
   }
 }
 
-// fuse_sum: when non-null, the expand also reduces the primary FE into this
-// [P][C] sum slab (TA-typed), and the following segsum skips that FE.
 template <typename TA, int C, class Tab, class Epi>
-static int launch_expand(Ctx& c, Tab tab, Epi epi, double* part, const char* name, double bytes,
-                         void* fuse_sum = nullptr) {
+static int launch_expand(Ctx& c, Tab tab, Epi epi, double* part, const char* name, double bytes) {
   ProfScope ps(c.pl, name, bytes);
-  if (c.d.K <= 2)
-    expand_kb<2, TA, C>(c, tab, epi, part, fuse_sum);
-  else if (c.d.K <= 4)
-    expand_kb<4, TA, C>(c, tab, epi, part, fuse_sum);
-  else
-    expand_kb<kMaxFE, TA, C>(c, tab, epi, part, fuse_sum);
-  FE_CK(cudaGetLastError());
-  return 0;
+  if (c.d.K <= 2) return expand_kb<2, TA, C>(c, tab, epi, part);
+  if (c.d.K <= 4) return expand_kb<4, TA, C>(c, tab, epi, part);
+  return expand_kb<kMaxFE, TA, C>(c, tab, epi, part);
+}
+
+// The contiguous row-sum pass (k_rowsum: primary and small FEs) and the
+// combine of its small-FE partials.  32-column tiles only.
+template <typename TA, int C, bool W, int NS>
+static int rowsum_launch(Ctx& c, const TA* src, TA* out) {
+  if constexpr (C == 32) {
+    auto kern = k_rowsum<TA, C, W, NS>;
+    constexpr int STEP = RowSumStep<TA>::value;
+    const size_t smem =
+        (size_t)kWarps * (2 * STEP + c.its->small_rows) * C * sizeof(TA);
+    // per instantiation: the opt-in shared-memory limit (set once) and the
+    // resident CTAs per SM for the last shared-memory size seen
+    static bool attr_set = false;
+    static size_t occ_smem = (size_t)-1;
+    static int occ = 1;
+    if (!attr_set) {
+      FE_CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)(kWarps * (2 * STEP + kSmallRows) * C * sizeof(TA))));
+      attr_set = true;
+    }
+    if (occ_smem != smem) {
+      int o = 0;
+      FE_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, kern, kThreads, smem));
+      occ = std::max(o, 1);
+      occ_smem = smem;
+    }
+    const int64_t n = (int64_t)c.its->ex.size();
+    const int64_t grid =
+        std::max<int64_t>(1, std::min<int64_t>(c.its->Se, (int64_t)occ * c.its->sms));
+    RowSumArgs rs{};
+    rs.sum = out;
+    rs.sa = c.ex_split();
+    rs.small_part = c.small_part;
+    rs.small_rows = c.its->small_rows;
+    for (int k = 0; k < c.d.K; ++k)
+      if ((c.its->small_mask >> k) & 1u) {
+        rs.small_fe[rs.n_small] = k;
+        rs.small_off[rs.n_small] = c.its->small_off[k];
+        ++rs.n_small;
+      }
+    kern<<<(unsigned)grid, kThreads, smem, c.s>>>(c.d, c.its->d_ex.as<ExpandItem>(), n, src, rs);
+    FE_CK(cudaGetLastError());
+    if (c.its->small_rows > 0) {
+      SmallRows m{};
+      for (int r = 0; r < c.its->small_rows; ++r) m.slab_row[r] = c.its->small_slab_row[(size_t)r];
+      k_small_combine<TA, C><<<(unsigned)c.its->small_rows, kThreads, 0, c.s>>>(
+          c.small_part, (int)grid, c.its->small_rows, m, out);
+      FE_CK(cudaGetLastError());
+    }
+    return 0;
+  } else {
+    (void)c;
+    (void)src;
+    (void)out;
+    set_error_cstr("row-sum pass requested for a tile narrower than 32 columns");
+    return 1;
+  }
+}
+
+template <typename TA, int C>
+static int launch_rowsum(Ctx& c, const TA* src, TA* out) {
+  const fe_plan* pl = c.pl;
+  bool w = false;
+  int ns = 0;
+  for (int k = 0; k < pl->K; ++k) {
+    const bool small = ((c.its->small_mask >> k) & 1u) != 0;
+    if (small) ++ns;
+    if ((small || k == pl->primary) && (pl->weighted || pl->interacted[k])) w = true;
+  }
+  switch (ns * 2 + (w ? 1 : 0)) {
+    case 0: return rowsum_launch<TA, C, false, 0>(c, src, out);
+    case 1: return rowsum_launch<TA, C, true, 0>(c, src, out);
+    case 2: return rowsum_launch<TA, C, false, 1>(c, src, out);
+    case 3: return rowsum_launch<TA, C, true, 1>(c, src, out);
+    case 4: return rowsum_launch<TA, C, false, 2>(c, src, out);
+    default: return rowsum_launch<TA, C, true, 2>(c, src, out);
+  }
 }
 
 template <typename TA, int C, int U, int S, class Load>
@@ -251,12 +320,21 @@ static int launch_segsum_async(Ctx& c, Load ld, TA* out, const ReduceItem* items
   return 0;
 }
 
-// all_fes: reduce every FE; otherwise skip the primary (reduced by a fused
-// expand).
+// rowsum: the primary and small FEs go through the contiguous row-sum pass
+// (32-column tiles of single-problem plans), the segsum gathers only the
+// large non-primary FEs; otherwise the segsum reduces every FE.
 template <typename TA, int C, class Load>
 static int launch_segsum(Ctx& c, Load ld, TA* out, const char* name, double bytes,
-                         bool all_fes = true) {
-  const int64_t n = all_fes ? (int64_t)c.its->rd.size() : c.its->rd_np;
+                         bool rowsum = false, const char* rs_name = "rowsum", double rs_bytes = 0.0) {
+  if constexpr (!Load::kSquareWeight) {
+    if (rowsum) {
+      ProfScope ps(c.pl, rs_name, rs_bytes);
+      static_assert(std::is_same<typename Load::InType, TA>::value, "rows are summed in their type");
+      const int st = launch_rowsum<TA, C>(c, ld.in, out);
+      if (st) return st;
+    }
+  }
+  const int64_t n = rowsum ? c.its->rd_large : (int64_t)c.its->rd.size();
   if (n == 0) return 0;
   ProfScope ps(c.pl, name, bytes);
   const unsigned grid = (unsigned)((n + kWarps - 1) / kWarps);
@@ -345,20 +423,23 @@ static int read_counter(Ctx& c, int idx, int32_t* out) {
   return 0;
 }
 
-// The primary FE is reduced inside the expand for tiles of 4+ columns; for
-// narrower tiles the extra scan costs more than the pass it saves.
-static bool use_fuse(const fe_plan* pl, int C) { return pl->opt_fuse != 0 && C >= 4; }
+// The row-sum pass serves 32-column tiles (its walk puts one column on each
+// lane) of single-problem plans (its small-FE tables hold one problem).
+static bool use_rowsum(const fe_plan* pl, int C) {
+  return pl->opt_fuse != 0 && C == 32 && pl->nprob == 1;
+}
 
 // algorithmic bytes per launch (the roofline numerators): every index vector
 // and observation row once, every coefficient-table row once
 struct Bytes {
-  double expand, segsum, pupdate, resid64, segsum64, grad64;
+  double expand, segsum, pupdate, resid64, segsum64, grad64, rowsum, rowsum64;
 };
-static Bytes alg_bytes(const fe_plan* pl, int C, int sT) {
+static Bytes alg_bytes(const fe_plan* pl, const ItemSet* its, int C, int sT) {
   Bytes b{};
-  const bool fuse = use_fuse(pl, C);
+  const bool fuse = use_rowsum(pl, C);
   const double N = (double)pl->N;
-  double P = 0, Pprim = 0, pos = 0, posmeta = 0, cw = 0, cw64 = 0, cwp = 0, cwp64 = 0;
+  // Pf: levels whose sums the row-sum pass writes (primary and small FEs)
+  double P = 0, Pf = 0, pos = 0, posmeta = 0, cw = 0, cw64 = 0, cwp = 0, cwp64 = 0;
   for (int k = 0; k < pl->K; ++k) {
     P += (double)pl->nlev[k];
     const bool has_cw = pl->weighted || pl->interacted[k];
@@ -366,9 +447,9 @@ static Bytes alg_bytes(const fe_plan* pl, int C, int sT) {
       cw += N * sT;
       cw64 += N * 8.0;
     }
-    if (fuse && k == pl->primary) {
-      Pprim = (double)pl->nlev[k];
-      continue;  // reduced inside the expand
+    if (fuse && (k == pl->primary || ((its->small_mask >> k) & 1u))) {
+      Pf += (double)pl->nlev[k];
+      continue;  // reduced by the row-sum pass
     }
     pos += (double)pl->seg_len[k];
     posmeta += (double)pl->seg_len[k] * (4.0 + (pl->perm_identity[k] ? 0.0 : 4.0));
@@ -378,11 +459,27 @@ static Bytes alg_bytes(const fe_plan* pl, int C, int sT) {
     }
   }
   const double refs = N * 4.0 * pl->K;
-  b.expand = refs + cw + 2.0 * N * C * sT + P * C * sT + Pprim * C * sT;
-  b.segsum = posmeta + cwp + pos * C * sT + (P - Pprim) * C * sT;
+  // the row-sum pass: one contiguous read of the rows and of the fused FEs'
+  // refs (and weights), the fused levels' sums written
+  double rowsum = 0.0, rowsum64 = 0.0;
+  if (fuse) {
+    double meta = 0.0, meta64 = 0.0;
+    for (int k = 0; k < pl->K; ++k)
+      if (k == pl->primary || ((its->small_mask >> k) & 1u)) {
+        const bool has_cw = pl->weighted || pl->interacted[k];
+        meta += N * (4.0 + (has_cw ? sT : 0));
+        meta64 += N * (4.0 + (has_cw ? 8.0 : 0.0));
+      }
+    rowsum = meta + N * C * sT + Pf * C * sT;
+    rowsum64 = meta64 + N * C * 8.0 + Pf * C * 8.0;
+  }
+  b.expand = refs + cw + 2.0 * N * C * sT + P * C * sT;
+  b.segsum = posmeta + cwp + pos * C * sT + (P - Pf) * C * sT;
+  b.rowsum = rowsum;
+  b.rowsum64 = rowsum64;
   b.pupdate = 9.0 * P * C * sT;
-  b.resid64 = refs + cw64 + N * C * (8.0 + 8.0 + 4.0) + P * C * 12.0 + Pprim * C * 8.0;
-  b.segsum64 = posmeta + cwp64 + pos * C * 8.0 + (P - Pprim) * C * 8.0;
+  b.resid64 = refs + cw64 + N * C * (8.0 + 8.0 + 4.0) + P * C * 12.0;
+  b.segsum64 = posmeta + cwp64 + pos * C * 8.0 + (P - Pf) * C * 8.0;
   b.grad64 = P * C * (8.0 + 4.0 + 8.0 + 4.0 + 8.0);
   return b;
 }
@@ -411,6 +508,9 @@ static int prepare(fe_plan* pl, int C, int sT, bool mixed, Ctx& c) {
   if ((st = w.block_part.ensure((size_t)std::max<int64_t>(its->n_blocks, 1) * nC * 8))) return st;
   if ((st = w.ex_block_part.ensure((size_t)std::max<int64_t>(its->ex_n_blocks, 1) * nC * 8))) return st;
   if ((st = w.inst.ensure((size_t)pl->nprob * nC * sizeof(Inst)))) return st;
+  // at most 8 resident CTAs of 256 threads per SM
+  if ((st = w.small_part.ensure((size_t)its->sms * 8 * std::max(its->small_rows, 1) * nC * 8)))
+    return st;
   if ((st = w.counters.ensure(64))) return st;
   if (!pl->host_pinned) FE_CK(cudaMallocHost(&pl->host_pinned, 64));
   c.pl = pl;
@@ -431,6 +531,8 @@ static int prepare(fe_plan* pl, int C, int sT, bool mixed, Ctx& c) {
   c.block = w.block_part.as<double>();
   c.ex_block = w.ex_block_part.as<double>();
   c.S = w.S.p;
+  c.small_part = w.small_part.as<double>();
+  c.rowsum = use_rowsum(pl, C);
   // coefficient-side slabs start at zero (levels without observations and
   // the null levels are never written afterwards)
   FE_CK(cudaMemsetAsync(w.V.p, 0, P * nC * (size_t)sT, c.s));
@@ -525,9 +627,10 @@ static int run_loop(fe_plan* pl, Ctx& c, int prec, int64_t cap, int32_t nact0, B
     size_t key = (size_t)c.C * 1000003u ^ (size_t)m;
     const void* ptrs[] = {c.inst, c.part_e, c.part_a, c.part_b, c.piece, c.ex_piece, c.S,
                           c.block, c.ex_block, pl->ws.U.p, pl->ws.V.p, pl->ws.H.p, pl->ws.Hb.p,
-                          pl->ws.X.p, c.its, c.counters, c.s};
+                          pl->ws.X.p, c.its, c.counters, c.s, c.small_part};
     for (const void* p : ptrs) key = key * 1315423911u + (size_t)p;
     key = key * 31 + (size_t)cur_tune().ex * 7 + (size_t)cur_tune().seg;
+    key = key * 3 + (c.rowsum ? 1u : 0u);
     lg = &pl->graphs[{c.C, prec}];
     if (!lg->exec || lg->key != key) {
       if (lg->exec) {
@@ -644,7 +747,7 @@ static int autotune(fe_plan* pl, Ctx& c) {
     for (int rep = 0; rep < 3 && !st; ++rep) {
       cudaEventRecord(e0, c.s);
       st = launch_segsum<T, C>(c, LoadIn<T, T, vec_of<T, C>()>{w.U.as<T>()}, static_cast<T*>(c.S), "tune",
-                               0.0, !use_fuse(pl, C));
+                               0.0, c.rowsum);
       cudaEventRecord(e1, c.s);
       cudaEventSynchronize(e1);
       float t = 0.f;
@@ -703,7 +806,7 @@ static int solve_plain_tile(fe_plan* pl, const SolveReq& rq, int64_t col0, int n
   if (st) return st;
   if ((st = autotune<T, C>(pl, c))) return st;
   Workspace& w = pl->ws;
-  const Bytes by = alg_bytes(pl, C, (int)sizeof(T));
+  const Bytes by = alg_bytes(pl, c.its, C, (int)sizeof(T));
   std::vector<Inst> h;
   init_insts(pl, rq, C, ncols, h);
   FE_CK(cudaMemcpyAsync(c.inst, h.data(), h.size() * sizeof(Inst), cudaMemcpyHostToDevice, c.s));
@@ -716,17 +819,17 @@ static int solve_plain_tile(fe_plan* pl, const SolveReq& rq, int64_t col0, int n
   T* ST = static_cast<T*>(c.S);
   // warm start x = A'b (src/AbstractFixedEffectSolver.jl:56); solve_coefficients! starts at 0
   if (rq.residuals) {
-    if ((st = launch_segsum<double, C>(c, LoadIn<double, double, vec_of<double, C>()>{B64}, S64, "segsum_warm", 0.0)))
+    if ((st = launch_segsum<double, C>(c, LoadIn<double, double, vec_of<double, C>()>{B64}, S64, "segsum_warm", 0.0,
+                                        c.rowsum, "rowsum_warm", 0.0)))
       return st;
     if ((st = launch_pupdate<C>(c, S64, PEpiStoreX<T, vec_of<double, C>()>{X, true}, nullptr, nullptr, "pupdate_warm", 0.0)))
       return st;
   }
   // u = b - A x, beta (lsmr.jl:63-64)
-  const bool fuse = use_fuse(pl, C);
-  void* fs = fuse ? c.S : nullptr;
+  const bool fuse = c.rowsum;
   if ((st = launch_expand<T, C>(c, TabOne<T, T, vec_of<T, C>()>{X},
                                 EpiBminusAx<T, T, vec_of<T, C>()>{B64, U, nullptr, c.inst, 0}, c.part_e,
-                                "expand_init", by.expand, fs)))
+                                "expand_init", by.expand)))
     return st;
   if ((st = launch_scalar_phase(c, PH_INIT_BETA, 0))) return st;
   PEpiLsmr<T, vec_of<T, C>()> pe{};
@@ -735,7 +838,8 @@ static int solve_plain_tile(fe_plan* pl, const SolveReq& rq, int64_t col0, int n
   pe.Hb = w.Hb.as<T>();
   pe.X = X;
   pe.inst = c.inst;
-  if ((st = launch_segsum<T, C>(c, LoadIn<T, T, vec_of<T, C>()>{U}, ST, "segsum", by.segsum, !fuse)))
+  if ((st = launch_segsum<T, C>(c, LoadIn<T, T, vec_of<T, C>()>{U}, ST, "segsum", by.segsum, fuse,
+                                "rowsum", by.rowsum)))
     return st;
   if ((st = launch_pupdate<C>(c, ST, pe, c.part_a, c.part_b, "pupdate", by.pupdate))) return st;
   if ((st = launch_scalar_phase(c, PH_INIT_ALPHA, 1))) return st;
@@ -747,11 +851,11 @@ static int solve_plain_tile(fe_plan* pl, const SolveReq& rq, int64_t col0, int n
   const int64_t cap = std::max<int64_t>(rq.maxiter, 1) + 2;
   auto body = [&]() -> int {
     int e;
-    if ((e = launch_expand<T, C>(c, TabOne<T, T, vec_of<T, C>()>{V}, ee, c.part_e, "expand", by.expand,
-                                 fs)))
+    if ((e = launch_expand<T, C>(c, TabOne<T, T, vec_of<T, C>()>{V}, ee, c.part_e, "expand", by.expand)))
       return e;
     if ((e = launch_scalar_phase(c, PH_BETA, 0))) return e;
-    if ((e = launch_segsum<T, C>(c, LoadIn<T, T, vec_of<T, C>()>{U}, ST, "segsum", by.segsum, !fuse)))
+    if ((e = launch_segsum<T, C>(c, LoadIn<T, T, vec_of<T, C>()>{U}, ST, "segsum", by.segsum, fuse,
+                                 "rowsum", by.rowsum)))
       return e;
     if ((e = launch_pupdate<C>(c, ST, pe, c.part_a, c.part_b, "pupdate", by.pupdate))) return e;
     return launch_scalar_phase(c, PH_ALPHA, 0);
@@ -785,7 +889,7 @@ static int solve_mixed_tile(fe_plan* pl, const SolveReq& rq, int64_t col0, int n
   if (st) return st;
   if ((st = autotune<float, C>(pl, c))) return st;
   Workspace& w = pl->ws;
-  const Bytes by = alg_bytes(pl, C, 4);
+  const Bytes by = alg_bytes(pl, c.its, C, 4);
   std::vector<Inst> h;
   init_insts(pl, rq, C, ncols, h);
   FE_CK(cudaMemcpyAsync(c.inst, h.data(), h.size() * sizeof(Inst), cudaMemcpyHostToDevice, c.s));
@@ -799,7 +903,8 @@ static int solve_mixed_tile(fe_plan* pl, const SolveReq& rq, int64_t col0, int n
   double* S64 = static_cast<double*>(c.S);
   float* S32 = static_cast<float*>(c.S);
   if (rq.residuals && pl->opt_mixed_warm) {
-    if ((st = launch_segsum<double, C>(c, LoadIn<double, double, vec_of<double, C>()>{B64}, S64, "segsum_warm", 0.0)))
+    if ((st = launch_segsum<double, C>(c, LoadIn<double, double, vec_of<double, C>()>{B64}, S64, "segsum_warm", 0.0,
+                                        c.rowsum, "rowsum_warm", 0.0)))
       return st;
     if ((st = launch_pupdate<C>(c, S64, PEpiStoreX<double, vec_of<double, C>()>{X64, true}, nullptr, nullptr,
                                 "pupdate_warm", 0.0)))
@@ -821,18 +926,17 @@ static int solve_mixed_tile(fe_plan* pl, const SolveReq& rq, int64_t col0, int n
   pg.inst = c.inst;
   const int64_t cap = std::max<int64_t>(rq.maxiter, 1) + 2;
   int64_t total_it = 0;
-  const bool fuse = use_fuse(pl, C);
-  void* fs = fuse ? c.S : nullptr;
+  const bool fuse = c.rowsum;
   for (int round = 0; round <= pl->opt_max_rounds + 1; ++round) {
     FE_CK(cudaMemsetAsync(c.counters + 1, 0, sizeof(int32_t), c.s));
     // r = b - A (x64 + dx32) in FP64, with the FP32 copy as the next inner u
     if ((st = launch_expand<double, C>(c, TabSum64<vec_of<double, C>()>{X64, X},
                                        EpiBminusAx<double, double, vec_of<double, C>()>{B64, R64, U, c.inst, 2},
-                                       c.part_e, "resid64", by.resid64, fs)))
+                                       c.part_e, "resid64", by.resid64)))
       return st;
     // g = A'r in FP64 (the next inner v), x64 += dx32, ||x64||
     if ((st = launch_segsum<double, C>(c, LoadIn<double, double, vec_of<double, C>()>{R64}, S64, "segsum64",
-                                       by.segsum64, !fuse)))
+                                       by.segsum64, fuse, "rowsum64", by.rowsum64)))
       return st;
     if ((st = launch_pupdate<C>(c, S64, pg, c.part_a, c.part_b, "grad64", by.grad64))) return st;
     if ((st = launch_scalar_phase(c, PH_OUTER, 0))) return st;
@@ -842,11 +946,11 @@ static int solve_mixed_tile(fe_plan* pl, const SolveReq& rq, int64_t col0, int n
     auto body = [&]() -> int {
       int e;
       if ((e = launch_expand<float, C>(c, TabOne<float, float, vec_of<float, C>()>{V}, ee, c.part_e,
-                                       "expand", by.expand, fs)))
+                                       "expand", by.expand)))
         return e;
       if ((e = launch_scalar_phase(c, PH_BETA, 0))) return e;
       if ((e = launch_segsum<float, C>(c, LoadIn<float, float, vec_of<float, C>()>{U}, S32, "segsum",
-                                       by.segsum, !fuse)))
+                                       by.segsum, fuse, "rowsum", by.rowsum)))
         return e;
       if ((e = launch_pupdate<C>(c, S32, pe, c.part_a, c.part_b, "pupdate", by.pupdate))) return e;
       return launch_scalar_phase(c, PH_ALPHA, 0);

@@ -277,22 +277,38 @@ def test_zipf_split_levels(fe, oracle):
 
 
 @pytest.mark.parametrize("prec", ["fp64", "mixed"])
-def test_fused_primary_reduce_matches_unfused(fe, synth, oracle, prec):
-    # the primary FE reduced inside the expand (default) vs by the segsum
-    pb = synth.make(4, scale=0.0003, ncols=6)
-    fes = [fe.FixedEffect.from_refs(r, n, a) for r, n, a in zip(pb.refs, pb.nlev, pb.interaction)]
-    Y = np.asfortranarray(pb.Y.astype(np.float64))
-    R_o, _, _ = oracle.solve_residuals_cols(Y, pb.refs, pb.nlev, pb.interaction, pb.weights, tol=1e-8)
+def test_rowsum_matches_segsum_path(fe, oracle, prec):
+    # 32-column tile: the contiguous row-sum pass reduces the primary FE (one
+    # level holds 30 % of the observations, so it is cut into pieces) and two
+    # small FEs (20 levels with an interaction, 6 levels); weighted.  Compared
+    # with the segsum-only path and the oracle, and bitwise across two calls.
+    rng = np.random.default_rng(12)
+    N = 40_000
+    r1 = rng.integers(1, 3001, N)
+    r1[rng.random(N) < 0.3] = 1
+    r2 = rng.integers(1, 401, N)
+    r3 = rng.integers(1, 21, N)
+    r4 = rng.integers(1, 7, N)
+    refs = [r1, r2, r3, r4]
+    inter = [None, None, rng.uniform(0.5, 1.5, N), None]
+    w = rng.uniform(0.5, 1.5, N)
+    Y = np.asfortranarray(rng.standard_normal((N, 5)))
+    R_o, _, _ = oracle.solve_residuals_cols(Y, refs, None, inter, w, tol=1e-8)
+    fes = [fe.FixedEffect(r, interaction=a) for r, a in zip(refs, inter)]
     out = []
     for fuse in (1, 0):
-        feM = fe.AbstractFixedEffectSolver(fes, pb.weights, "CUDA", np.float64, precision=prec)
+        feM = fe.AbstractFixedEffectSolver(fes, w, "CUDA", np.float64, precision=prec)
+        feM.set_option(fe._lib.FE_OPT_TILE, 32)
         feM.set_option(fe._lib.FE_OPT_FUSE, fuse)
         R, its, cvs = feM.solve_residuals(Y.copy(), tol=1e-8)
+        R2, its2, _ = feM.solve_residuals(Y.copy(), tol=1e-8)
         feM.close()
-        assert cvs.all()
+        assert cvs.all() and np.array_equal(R, R2) and np.array_equal(its, its2)
+        err = max(rel_err(R[:, j], R_o[:, j]) for j in range(Y.shape[1]))
+        assert err < REL, (fuse, err)
         out.append(R)
-    for R in out:
-        assert max(rel_err(R[:, j], R_o[:, j]) for j in range(Y.shape[1])) < REL
+    # the two paths sum in different orders: equal to rounding
+    assert max(rel_err(out[0][:, j], out[1][:, j]) for j in range(Y.shape[1])) < REL
 
 
 def test_autotuner_persists_choice(fe, synth, tmp_path, monkeypatch):
