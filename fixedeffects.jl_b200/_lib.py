@@ -35,6 +35,7 @@ FE_OPT_SEGSUM_VARIANT = 8
 FE_OPT_AUTOTUNE = 9
 FE_OPT_MIXED_WARM_START = 10
 FE_OPT_GRAPH = 11
+FE_OPT_ROWSUM_VARIANT = 12
 
 # every symbol declared in include/fe_b200.h
 EXPORTS = (

@@ -240,6 +240,15 @@ int fe_plan_set_option(fe_plan* plan, int32_t option, double value) {
     case FE_OPT_GRAPH:
       plan->opt_graph = value != 0 ? 1 : 0;
       return FE_OK;
+    case FE_OPT_ROWSUM_VARIANT: {
+      const int v = (int)value;
+      if (v < -1 || v > 1) {
+        set_error("row-sum variant must be -1 (default), 0 or 1");
+        return FE_ERR_INVALID;
+      }
+      plan->opt_rowsum_variant = v;
+      return FE_OK;
+    }
     case FE_OPT_EXPAND_VARIANT:
     case FE_OPT_SEGSUM_VARIANT: {
       const int v = (int)value;

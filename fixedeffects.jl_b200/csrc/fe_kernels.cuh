@@ -552,25 +552,84 @@ struct RowSumArgs {
   int32_t small_rows;         // table rows in use
 };
 
-// rows per step: 4 KB of rows per warp (one buffer of the double buffer)
+// Row ring of one warp: NBUF buffers of STEP rows; NBUF-1 steps are in
+// flight while one is walked.
 template <typename TA> struct RowSumStep {
-  static constexpr int value = sizeof(TA) == 4 ? 32 : 16;
+  static constexpr int value = 16;
+  static constexpr int NBUF = sizeof(TA) == 4 ? 3 : 2;
 };
 
-// One row of the walk: r is the row within the step (a compile-time constant
-// in the unrolled full-step walk).
-template <typename TA, int C, bool W, int NS>
-__device__ __forceinline__ void rowsum_row(int r, const TA* __restrict__ rows, TA& acc,
-                                           uint32_t bmask, int kpr, TA cpv, int k0, TA c0, int k1,
-                                           TA c1, TA* __restrict__ Sf, TA* __restrict__ tbl,
-                                           int lane) {
-  const TA x = rows[r * C];
+// The walk of one step, in groups of 4 rows (r0 a compile-time multiple of 4
+// in the unrolled full-step walk).  Primary FE: a running sum per lane,
+// stored at each level change.  Small FEs: rows of a group with equal keys
+// are added together first (into the group's first row with that key), so the
+// remaining table rows are distinct and their 4 loads, adds and stores are
+// independent: one shared-memory round trip per group instead of per row.
+template <typename TA, int C, bool W>
+__device__ __forceinline__ void rowsum_primary(int r, const TA x, TA& acc, uint32_t bmask,
+                                               int kpr, TA cpv, TA* __restrict__ Sf) {
   acc += W ? x * __shfl_sync(FE_FULL, cpv, r) : x;
   if ((bmask >> r) & 1u) {
     const int kr = __shfl_sync(FE_FULL, kpr, r);
     Sf[(int64_t)kr * C] = acc;
     acc = TA(0);
   }
+}
+
+template <typename TA, int C, bool W>
+__device__ __forceinline__ void rowsum_small4(int r0, TA v0, TA v1, TA v2, TA v3, int kt, TA ct,
+                                              TA* __restrict__ tbl, int lane) {
+  const int t0 = __shfl_sync(FE_FULL, kt, r0);
+  const int t1 = __shfl_sync(FE_FULL, kt, r0 + 1);
+  const int t2 = __shfl_sync(FE_FULL, kt, r0 + 2);
+  const int t3 = __shfl_sync(FE_FULL, kt, r0 + 3);
+  if (W) {
+    v0 *= __shfl_sync(FE_FULL, ct, r0);
+    v1 *= __shfl_sync(FE_FULL, ct, r0 + 1);
+    v2 *= __shfl_sync(FE_FULL, ct, r0 + 2);
+    v3 *= __shfl_sync(FE_FULL, ct, r0 + 3);
+  }
+  // a row whose key appeared earlier in the group is added into that row
+  // (the first with the key); the rows left have distinct keys
+  const bool s1 = t1 != t0;
+  const bool s2 = t2 != t0 && t2 != t1;
+  const bool s3 = t3 != t0 && t3 != t1 && t3 != t2;
+  const int d3 = t3 == t0 ? 0 : (t3 == t1 ? 1 : 2);  // target of row 3 when !s3
+  const int d2 = t2 == t0 ? 0 : 1;                    // target of row 2 when !s2
+  if (!s3) {
+    if (d3 == 0) v0 += v3;
+    else if (d3 == 1) v1 += v3;
+    else v2 += v3;
+  }
+  if (!s2) {
+    if (d2 == 0) v0 += v2;
+    else v1 += v2;
+  }
+  if (!s1) v0 += v1;
+  TA* p0 = tbl + t0 * C + lane;
+  TA* p1 = tbl + t1 * C + lane;
+  TA* p2 = tbl + t2 * C + lane;
+  TA* p3 = tbl + t3 * C + lane;
+  TA a0 = *p0;
+  TA a1 = s1 ? *p1 : TA(0);
+  TA a2 = s2 ? *p2 : TA(0);
+  TA a3 = s3 ? *p3 : TA(0);
+  a0 += v0;
+  a1 += v1;
+  a2 += v2;
+  a3 += v3;
+  *p0 = a0;
+  if (s1) *p1 = a1;
+  if (s2) *p2 = a2;
+  if (s3) *p3 = a3;
+}
+
+// one row at a time (partial steps)
+template <typename TA, int C, bool W, int NS>
+__device__ __forceinline__ void rowsum_row(int r, const TA x, TA& acc, uint32_t bmask, int kpr,
+                                           TA cpv, int k0, TA c0, int k1, TA c1,
+                                           TA* __restrict__ Sf, TA* __restrict__ tbl, int lane) {
+  rowsum_primary<TA, C, W>(r, x, acc, bmask, kpr, cpv, Sf);
   if (NS > 0) {
     const int t0 = __shfl_sync(FE_FULL, k0, r);
     tbl[t0 * C + lane] += W ? x * __shfl_sync(FE_FULL, c0, r) : x;
@@ -581,22 +640,44 @@ __device__ __forceinline__ void rowsum_row(int r, const TA* __restrict__ rows, T
   }
 }
 
+// a full step of STEP rows (a multiple of 4)
+template <typename TA, int C, bool W, int NS, int STEP>
+__device__ __forceinline__ void rowsum_full_step(const TA (&xs)[STEP], TA& acc, uint32_t bmask,
+                                                 int kpr, TA cpv, int k0, TA c0, int k1, TA c1,
+                                                 TA* __restrict__ Sf, TA* __restrict__ tbl,
+                                                 int lane) {
+  static_assert(STEP % 4 == 0, "groups of 4 rows");
+#pragma unroll
+  for (int r0 = 0; r0 < STEP; r0 += 4) {
+    TA x[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      x[j] = xs[r0 + j];
+      rowsum_primary<TA, C, W>(r0 + j, x[j], acc, bmask, kpr, cpv, Sf);
+    }
+    if (NS > 0) rowsum_small4<TA, C, W>(r0, x[0], x[1], x[2], x[3], k0, c0, tbl, lane);
+    if (NS > 1) rowsum_small4<TA, C, W>(r0, x[0], x[1], x[2], x[3], k1, c1, tbl, lane);
+  }
+}
+
 // W: some reduced FE has weights (cw); NS: small FEs reduced in the tables.
 template <typename TA, int C, bool W, int NS>
-__global__ void __launch_bounds__(kThreads, 4)
+__global__ void __launch_bounds__(kThreads, sizeof(TA) == 4 ? 4 : 2)
 k_rowsum(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_items,
          const TA* __restrict__ src, RowSumArgs rs) {
   static_assert(C == 32, "the walk puts one column on each lane");
   constexpr int STEP = RowSumStep<TA>::value;
+  constexpr int NBUF = RowSumStep<TA>::NBUF;
   constexpr int BUF = STEP * C;                               // elements per buffer
   constexpr int CHUNKS = BUF * (int)sizeof(TA) / 16 / 32;     // 16-byte copies per lane
   constexpr int ROWCH = C * (int)sizeof(TA) / 16;             // 16-byte chunks per row
+  static_assert(CHUNKS * 32 * 16 == BUF * (int)sizeof(TA), "whole chunks per lane");
   __shared__ double smt[kWarps][32];
   extern __shared__ __align__(16) unsigned char rowsum_smem[];
   const int lane = threadIdx.x & 31;
   const int wib = threadIdx.x >> 5;
-  TA* wbuf = reinterpret_cast<TA*>(rowsum_smem) + (size_t)wib * 2 * BUF;     // 2 row buffers
-  TA* tbl = reinterpret_cast<TA*>(rowsum_smem) + (size_t)kWarps * 2 * BUF +  // small-FE table
+  TA* wbuf = reinterpret_cast<TA*>(rowsum_smem) + (size_t)wib * NBUF * BUF;     // row ring
+  TA* tbl = reinterpret_cast<TA*>(rowsum_smem) + (size_t)kWarps * NBUF * BUF +  // small-FE table
             (size_t)wib * rs.small_rows * C;
   for (int e = lane; e < rs.small_rows * C; e += 32) tbl[e] = TA(0);
   __syncwarp();
@@ -615,9 +696,11 @@ k_rowsum(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_items,
     const ExpandItem it = items[wi];
     const int64_t ie = it.ie;
     if (ie <= it.ib) continue;
-    // copy the rows of the step at `base` into buffer b (one commit group)
+    // copy the rows of the step at `base` into buffer b (one commit group,
+    // empty past the end of the item)
     auto issue = [=](int64_t base, int b) {
-      const int nv = (int)((ie - base) < STEP ? (ie - base) : STEP);
+      const int64_t left = ie - base;
+      const int nv = (int)(left < STEP ? (left > 0 ? left : 0) : STEP);
       const unsigned char* g = reinterpret_cast<const unsigned char*>(src + base * C);
       unsigned char* sp = reinterpret_cast<unsigned char*>(wbuf + b * BUF);
 #pragma unroll
@@ -646,23 +729,20 @@ k_rowsum(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_items,
         if (W) c1_n = (ok && cw1) ? __ldg(cw1 + p) : TA(1);
       }
     };
-    issue(it.ib, 0);
+#pragma unroll
+    for (int q = 0; q < NBUF - 1; ++q) issue(it.ib + (int64_t)q * STEP, q);
     keys(it.ib);
     int ckey = -1;  // primary level of the open run (warp-uniform)
     TA acc = TA(0);
     int b = 0;
-    for (int64_t base = it.ib; base < ie; base += STEP, b ^= 1) {
+    for (int64_t base = it.ib; base < ie; base += STEP, b = (b + 1 == NBUF ? 0 : b + 1)) {
       const int kpr = kpr_n, k0 = k0_n, k1 = k1_n;
       const TA cpv = cp_n, c0 = c0_n, c1 = c1_n;
       const int nvalid = (int)((ie - base) < STEP ? (ie - base) : STEP);
-      if (base + STEP < ie) {
-        issue(base + STEP, b ^ 1);
-        keys(base + STEP);
-        cp_async_wait<1>();
-      } else {
-        cp_async_wait<0>();
-      }
-      __syncwarp();  // every lane's copies of this step are visible
+      issue(base + (int64_t)(NBUF - 1) * STEP, b == 0 ? NBUF - 1 : b - 1);
+      if (base + STEP < ie) keys(base + STEP);
+      cp_async_wait<NBUF - 1>();  // this step's group is complete
+      __syncwarp();               // every lane's copies of this step are visible
       const int kn = __shfl_down_sync(FE_FULL, kpr, 1);
       const uint32_t bmask = __ballot_sync(FE_FULL, lane + 1 < nvalid && kn != kpr);
       const int kfirst = __shfl_sync(FE_FULL, kpr, 0);
@@ -672,16 +752,19 @@ k_rowsum(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_items,
       }
       const TA* __restrict__ rows = wbuf + b * BUF + lane;
       if (nvalid == STEP) {
+        TA xs[STEP];
 #pragma unroll
-        for (int r = 0; r < STEP; ++r)
-          rowsum_row<TA, C, W, NS>(r, rows, acc, bmask, kpr, cpv, k0, c0, k1, c1, Sf, tbl, lane);
+        for (int r = 0; r < STEP; ++r) xs[r] = rows[r * C];
+        rowsum_full_step<TA, C, W, NS, STEP>(xs, acc, bmask, kpr, cpv, k0, c0, k1, c1, Sf, tbl,
+                                             lane);
       } else {
 #pragma unroll 1
         for (int r = 0; r < nvalid; ++r)
-          rowsum_row<TA, C, W, NS>(r, rows, acc, bmask, kpr, cpv, k0, c0, k1, c1, Sf, tbl, lane);
+          rowsum_row<TA, C, W, NS>(r, rows[r * C], acc, bmask, kpr, cpv, k0, c0, k1, c1, Sf, tbl,
+                                   lane);
       }
       ckey = __shfl_sync(FE_FULL, kpr, nvalid - 1);
-      __syncwarp();  // buffer b is free for the copies of step + 2
+      __syncwarp();  // buffer b is free for the copies of step + NBUF
     }
     // the open run: a whole level, or one piece of a long one
     SegRun<TA, 1, 32, 1> run;
@@ -695,7 +778,111 @@ k_rowsum(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_items,
     __syncthreads();
     const int n = rs.small_rows * C;
     double* __restrict__ out = rs.small_part + (int64_t)blockIdx.x * n;
-    const TA* t0 = reinterpret_cast<const TA*>(rowsum_smem) + (size_t)kWarps * 2 * BUF;
+    const TA* t0 = reinterpret_cast<const TA*>(rowsum_smem) + (size_t)kWarps * NBUF * BUF;
+    for (int e = threadIdx.x; e < n; e += kThreads) {
+      double t = 0.0;
+#pragma unroll
+      for (int w = 0; w < kWarps; ++w) t += (double)t0[(size_t)w * n + e];
+      out[e] = t;
+    }
+  }
+}
+
+// The same pass with the rows staged in registers instead of shared memory:
+// STEP loads per lane for the next step are issued before the current step is
+// walked.  Shared memory then carries only the small-FE table traffic (two
+// wavefronts per row instead of four), at the price of 2 x STEP registers.
+template <typename TA, int C, bool W, int NS>
+__global__ void __launch_bounds__(kThreads, sizeof(TA) == 4 ? 3 : 2)
+k_rowsum_reg(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_items,
+             const TA* __restrict__ src, RowSumArgs rs) {
+  static_assert(C == 32, "the walk puts one column on each lane");
+  constexpr int STEP = sizeof(TA) == 4 ? 16 : 8;
+  __shared__ double smt[kWarps][32];
+  extern __shared__ __align__(16) unsigned char rowsum_smem[];
+  const int lane = threadIdx.x & 31;
+  const int wib = threadIdx.x >> 5;
+  TA* tbl = reinterpret_cast<TA*>(rowsum_smem) + (size_t)wib * rs.small_rows * C;
+  for (int e = lane; e < rs.small_rows * C; e += 32) tbl[e] = TA(0);
+  __syncwarp();
+  const int kp = d.primary;
+  TA* __restrict__ Sf = reinterpret_cast<TA*>(rs.sum) + d.lev_base[kp] * C + lane;
+  const int32_t* __restrict__ refp = d.refs[kp];
+  const TA* __restrict__ cwp = cw_of<TA>(d, kp);
+  const int32_t* __restrict__ ref0 = NS > 0 ? d.refs[rs.small_fe[0]] : nullptr;
+  const int32_t* __restrict__ ref1 = NS > 1 ? d.refs[rs.small_fe[1]] : nullptr;
+  const TA* __restrict__ cw0 = NS > 0 ? cw_of<TA>(d, rs.small_fe[0]) : nullptr;
+  const TA* __restrict__ cw1 = NS > 1 ? cw_of<TA>(d, rs.small_fe[1]) : nullptr;
+  const int off0 = rs.small_off[0], off1 = rs.small_off[1];
+  const int64_t w0 = (int64_t)blockIdx.x * n_items / gridDim.x;
+  const int64_t w1 = (int64_t)(blockIdx.x + 1) * n_items / gridDim.x;
+  for (int64_t wi = w0 + wib; wi < w1; wi += kWarps) {
+    const ExpandItem it = items[wi];
+    const int64_t ie = it.ie;
+    if (ie <= it.ib) continue;
+    TA xn[STEP];
+    int kpr_n = kSentinel, k0_n = 0, k1_n = 0;
+    TA cp_n = TA(1), c0_n = TA(1), c1_n = TA(1);
+    auto fetch = [&](int64_t base) {
+      const int64_t left = ie - base;
+      const int nv = (int)(left < STEP ? left : STEP);
+      const TA* __restrict__ row = src + base * C + lane;
+#pragma unroll
+      for (int r = 0; r < STEP; ++r) xn[r] = r < nv ? __ldcs(row + (int64_t)r * C) : TA(0);
+      const int64_t p = base + lane;
+      const bool ok = lane < nv;
+      kpr_n = ok ? __ldg(refp + p) : kSentinel;
+      if (W) cp_n = (ok && cwp) ? __ldg(cwp + p) : TA(1);
+      if (NS > 0) {
+        k0_n = ok ? off0 + __ldg(ref0 + p) : 0;
+        if (W) c0_n = (ok && cw0) ? __ldg(cw0 + p) : TA(1);
+      }
+      if (NS > 1) {
+        k1_n = ok ? off1 + __ldg(ref1 + p) : 0;
+        if (W) c1_n = (ok && cw1) ? __ldg(cw1 + p) : TA(1);
+      }
+    };
+    fetch(it.ib);
+    int ckey = -1;  // primary level of the open run (warp-uniform)
+    TA acc = TA(0);
+    for (int64_t base = it.ib; base < ie; base += STEP) {
+      TA x[STEP];
+#pragma unroll
+      for (int r = 0; r < STEP; ++r) x[r] = xn[r];
+      const int kpr = kpr_n, k0 = k0_n, k1 = k1_n;
+      const TA cpv = cp_n, c0 = c0_n, c1 = c1_n;
+      const int nvalid = (int)((ie - base) < STEP ? (ie - base) : STEP);
+      if (base + STEP < ie) fetch(base + STEP);
+      const int kn = __shfl_down_sync(FE_FULL, kpr, 1);
+      const uint32_t bmask = __ballot_sync(FE_FULL, lane + 1 < nvalid && kn != kpr);
+      const int kfirst = __shfl_sync(FE_FULL, kpr, 0);
+      if (ckey >= 0 && ckey != kfirst) {
+        Sf[(int64_t)ckey * C] = acc;
+        acc = TA(0);
+      }
+      if (nvalid == STEP) {
+        rowsum_full_step<TA, C, W, NS, STEP>(x, acc, bmask, kpr, cpv, k0, c0, k1, c1, Sf, tbl,
+                                             lane);
+      } else {
+#pragma unroll
+        for (int r = 0; r < STEP; ++r)
+          if (r < nvalid)  // warp-uniform
+            rowsum_row<TA, C, W, NS>(r, x[r], acc, bmask, kpr, cpv, k0, c0, k1, c1, Sf, tbl, lane);
+      }
+      ckey = __shfl_sync(FE_FULL, kpr, nvalid - 1);
+    }
+    SegRun<TA, 1, 32, 1> run;
+    run.ckey = ckey;
+    run.carry.v[0] = acc;
+    run.acc.v[0] = TA(0);
+    run.pend = false;
+    run.finish(it.split, it.piece, rs.sa, 0, lane, C, Sf, smt[wib]);
+  }
+  if (NS > 0) {
+    __syncthreads();
+    const int n = rs.small_rows * C;
+    double* __restrict__ out = rs.small_part + (int64_t)blockIdx.x * n;
+    const TA* t0 = reinterpret_cast<const TA*>(rowsum_smem);
     for (int e = threadIdx.x; e < n; e += kThreads) {
       double t = 0.0;
 #pragma unroll

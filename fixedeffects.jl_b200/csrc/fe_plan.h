@@ -138,6 +138,7 @@ struct fe_plan {
   int32_t opt_autotune = 1;     // time the variants on first use of a tile shape
   int32_t opt_mixed_warm = 1;   // mixed precision starts from x0 = A'b (else x0 = 0)
   int32_t opt_graph = 1;        // replay the LSMR iterations from a CUDA graph
+  int32_t opt_rowsum_variant = -1; // row-sum pass: 0 shared-memory ring, 1 registers
   std::map<std::pair<int, int>, fe::LoopGraph> graphs;  // by (C, precision)
   // tuned variants per (tile width C, element size): {expand, segsum}
   std::map<std::pair<int, int>, std::pair<int, int>> tuned;

@@ -231,29 +231,32 @@ static int launch_expand(Ctx& c, Tab tab, Epi epi, double* part, const char* nam
 template <typename TA, int C, bool W, int NS>
 static int rowsum_launch(Ctx& c, const TA* src, TA* out) {
   if constexpr (C == 32) {
-    auto kern = k_rowsum<TA, C, W, NS>;
-    constexpr int STEP = RowSumStep<TA>::value;
-    const size_t smem =
-        (size_t)kWarps * (2 * STEP + c.its->small_rows) * C * sizeof(TA);
+    // default: rows in registers for FP32, the shared-memory ring for FP64
+    const bool regs = c.pl->opt_rowsum_variant == 1 ||
+                      (c.pl->opt_rowsum_variant < 0 && sizeof(TA) == 4);
+    auto kern = regs ? k_rowsum_reg<TA, C, W, NS> : k_rowsum<TA, C, W, NS>;
+    const int RING = regs ? 0 : RowSumStep<TA>::value * RowSumStep<TA>::NBUF;
+    const size_t smem = (size_t)kWarps * (RING + c.its->small_rows) * C * sizeof(TA);
     // per instantiation: the opt-in shared-memory limit (set once) and the
     // resident CTAs per SM for the last shared-memory size seen
-    static bool attr_set = false;
-    static size_t occ_smem = (size_t)-1;
-    static int occ = 1;
-    if (!attr_set) {
+    static bool attr_set[2] = {false, false};
+    static size_t occ_smem[2] = {(size_t)-1, (size_t)-1};
+    static int occ[2] = {1, 1};
+    const int vi = regs ? 1 : 0;
+    if (!attr_set[vi]) {
       FE_CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)(kWarps * (2 * STEP + kSmallRows) * C * sizeof(TA))));
-      attr_set = true;
+                                 (int)(kWarps * (RING + kSmallRows) * C * sizeof(TA))));
+      attr_set[vi] = true;
     }
-    if (occ_smem != smem) {
+    if (occ_smem[vi] != smem) {
       int o = 0;
       FE_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, kern, kThreads, smem));
-      occ = std::max(o, 1);
-      occ_smem = smem;
+      occ[vi] = std::max(o, 1);
+      occ_smem[vi] = smem;
     }
     const int64_t n = (int64_t)c.its->ex.size();
     const int64_t grid =
-        std::max<int64_t>(1, std::min<int64_t>(c.its->Se, (int64_t)occ * c.its->sms));
+        std::max<int64_t>(1, std::min<int64_t>(c.its->Se, (int64_t)occ[vi] * c.its->sms));
     RowSumArgs rs{};
     rs.sum = out;
     rs.sa = c.ex_split();
@@ -631,6 +634,7 @@ static int run_loop(fe_plan* pl, Ctx& c, int prec, int64_t cap, int32_t nact0, B
     for (const void* p : ptrs) key = key * 1315423911u + (size_t)p;
     key = key * 31 + (size_t)cur_tune().ex * 7 + (size_t)cur_tune().seg;
     key = key * 3 + (c.rowsum ? 1u : 0u);
+    key = key * 5 + (size_t)(pl->opt_rowsum_variant + 1);
     lg = &pl->graphs[{c.C, prec}];
     if (!lg->exec || lg->key != key) {
       if (lg->exec) {

@@ -57,7 +57,10 @@ extern "C" {
 #define FE_OPT_MAX_ROUNDS 3  /* FP64 refinement rounds (FE_PREC_MIXED) */
 #define FE_OPT_PROFILE 4     /* 1: time every launch with CUDA events */
 #define FE_OPT_INNER_RHO 5   /* FP32 inner-solve floor (relative ||A'r|| drop) */
-#define FE_OPT_FUSE 6        /* 1: reduce the primary FE inside the expand (default 0) */
+#define FE_OPT_FUSE 6        /* 1 (default): 32-column tiles of single-problem plans
+                                reduce the primary FE and up to two small FEs in one
+                                contiguous row-sum pass; 0: every FE by the
+                                level-order segsum */
 #define FE_OPT_EXPAND_VARIANT 7 /* expand kernel variant 0..3, -1 = default */
 #define FE_OPT_SEGSUM_VARIANT 8 /* segsum kernel variant 0..5, -1 = default */
 #define FE_OPT_AUTOTUNE 9    /* 1 (default): time the kernel variants on the first
@@ -69,6 +72,8 @@ extern "C" {
                                       or from x0 = 0 (0) */
 #define FE_OPT_GRAPH 11      /* 1 (default): replay the LSMR iterations between host
                                 convergence checks from a captured CUDA graph */
+#define FE_OPT_ROWSUM_VARIANT 12 /* row-sum pass: -1 default, 0 rows staged in shared
+                                    memory (cp.async ring), 1 rows in registers */
 
 typedef struct fe_plan fe_plan;
 

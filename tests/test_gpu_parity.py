@@ -296,19 +296,22 @@ def test_rowsum_matches_segsum_path(fe, oracle, prec):
     R_o, _, _ = oracle.solve_residuals_cols(Y, refs, None, inter, w, tol=1e-8)
     fes = [fe.FixedEffect(r, interaction=a) for r, a in zip(refs, inter)]
     out = []
-    for fuse in (1, 0):
+    # (row-sum pass, its variant): shared-memory ring, registers, segsum only
+    for fuse, var in ((1, 0), (1, 1), (0, -1)):
         feM = fe.AbstractFixedEffectSolver(fes, w, "CUDA", np.float64, precision=prec)
         feM.set_option(fe._lib.FE_OPT_TILE, 32)
         feM.set_option(fe._lib.FE_OPT_FUSE, fuse)
+        feM.set_option(fe._lib.FE_OPT_ROWSUM_VARIANT, var)
         R, its, cvs = feM.solve_residuals(Y.copy(), tol=1e-8)
         R2, its2, _ = feM.solve_residuals(Y.copy(), tol=1e-8)
         feM.close()
         assert cvs.all() and np.array_equal(R, R2) and np.array_equal(its, its2)
         err = max(rel_err(R[:, j], R_o[:, j]) for j in range(Y.shape[1]))
-        assert err < REL, (fuse, err)
+        assert err < REL, (fuse, var, err)
         out.append(R)
-    # the two paths sum in different orders: equal to rounding
-    assert max(rel_err(out[0][:, j], out[1][:, j]) for j in range(Y.shape[1])) < REL
+    # the two row-sum variants sum in the same order; the segsum in another
+    assert np.array_equal(out[0], out[1])
+    assert max(rel_err(out[0][:, j], out[2][:, j]) for j in range(Y.shape[1])) < REL
 
 
 def test_autotuner_persists_choice(fe, synth, tmp_path, monkeypatch):
