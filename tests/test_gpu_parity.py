@@ -326,7 +326,7 @@ def test_autotuner_persists_choice(fe, synth, tmp_path, monkeypatch):
     lines = cache.read_text().strip().splitlines()
     assert len(lines) == 1
     sig, C, sT, ex, seg = lines[0].split()
-    assert (int(C), int(sT)) == (8, 4) and 0 <= int(ex) < 4 and 0 <= int(seg) < 4
+    assert (int(C), int(sT)) == (8, 4) and 0 <= int(ex) < 4 and 0 <= int(seg) < 6
     # a second plan of the same shape reuses the cached choice (no new line)
     feM = fe.AbstractFixedEffectSolver(fes, None, "CUDA", np.float32)
     R2, _, _ = feM.solve_residuals(Y.copy(), tol=1e-8)
