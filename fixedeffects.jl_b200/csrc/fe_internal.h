@@ -100,6 +100,11 @@ struct FeDev {
   const double* cwp_d[kMaxFE];
   int64_t lev_base[kMaxFE];      // first row of FE k in a [P][C] slab
   int32_t primary;               // FE whose levels order the observations
+  // set inside the LSMR loop only: the number of instances still running
+  // (written by the scalar kernel's beta phase); the reductions return at
+  // once when it is 0, so the iterations that finish a replayed chunk after
+  // every instance has stopped cost launches only
+  const int32_t* active;
 };
 
 // LSMR state of one instance (problem p, column j).  Scalars are FP64 in every

@@ -674,6 +674,7 @@ k_rowsum(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_items,
   static_assert(CHUNKS * 32 * 16 == BUF * (int)sizeof(TA), "whole chunks per lane");
   __shared__ double smt[kWarps][32];
   extern __shared__ __align__(16) unsigned char rowsum_smem[];
+  if (d.active && *d.active == 0) return;  // the whole CTA
   const int lane = threadIdx.x & 31;
   const int wib = threadIdx.x >> 5;
   TA* wbuf = reinterpret_cast<TA*>(rowsum_smem) + (size_t)wib * NBUF * BUF;     // row ring
@@ -800,6 +801,7 @@ k_rowsum_reg(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_item
   constexpr int STEP = sizeof(TA) == 4 ? 16 : 8;
   __shared__ double smt[kWarps][32];
   extern __shared__ __align__(16) unsigned char rowsum_smem[];
+  if (d.active && *d.active == 0) return;  // the whole CTA
   const int lane = threadIdx.x & 31;
   const int wib = threadIdx.x >> 5;
   TA* tbl = reinterpret_cast<TA*>(rowsum_smem) + (size_t)wib * rs.small_rows * C;
@@ -901,7 +903,8 @@ struct SmallRows {
 template <typename TA, int C>
 __global__ void __launch_bounds__(kThreads)
 k_small_combine(const double* __restrict__ part, int nparts, int small_rows, SmallRows m,
-                TA* __restrict__ out) {
+                TA* __restrict__ out, const int32_t* __restrict__ active) {
+  if (active && *active == 0) return;
   constexpr int Q = kThreads / C;
   __shared__ double sm[Q][C];
   const int row = blockIdx.x;
@@ -969,6 +972,7 @@ k_segsum(const FeDev d, const ReduceItem* __restrict__ items, int64_t n_items, L
   const int g = lane / CL, jl = lane - g * CL;
   const int64_t w = (int64_t)blockIdx.x * kWarps + (threadIdx.x >> 5);
   if (w >= n_items) return;
+  if (d.active && *d.active == 0) return;
   const ReduceItem it = items[w];
   if (it.pe <= it.pb) return;
   const int k = it.fe;
@@ -1066,6 +1070,7 @@ k_segsum_async(const FeDev d, const ReduceItem* __restrict__ items, int64_t n_it
   const int g = lane / CL, jl = lane - g * CL;
   const int64_t w = (int64_t)blockIdx.x * kWarps + wib;
   if (w >= n_items) return;
+  if (d.active && *d.active == 0) return;
   const ReduceItem it = items[w];
   if (it.pe <= it.pb) return;
   unsigned char* ring = dyn_smem + (size_t)wib * L::kWarpBytes;

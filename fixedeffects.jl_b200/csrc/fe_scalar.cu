@@ -195,7 +195,12 @@ __global__ void __launch_bounds__(kScalarThreads) k_scalar(ScalarArgs a) {
       break;
     }
     case PH_BETA: {
-      if (id == 0) a.counters[0] = 0;
+      // counters[2]: instances running in this iteration (read by the
+      // reductions that follow); counters[0] collects the next count
+      if (id == 0) {
+        a.counters[2] = a.counters[0];
+        a.counters[0] = 0;
+      }
       if (!s.active) break;
       // beta = ||u||; if beta > 0: u /= beta, v = A'u - beta v  (lsmr.jl:104-108)
       s.beta = sqrt(s0);
@@ -281,7 +286,8 @@ __global__ void __launch_bounds__(kScalarThreads) k_scalar(ScalarArgs a) {
       s.s_v = 1.0 / ng;
       lsmr_init(s, 3);
       s.normAr0 = s.normAr;
-      atomicAdd(a.counters + 1, 1);
+      atomicAdd(a.counters, 1);      // LSMR running (read by the first beta phase)
+      atomicAdd(a.counters + 1, 1);  // refinement running
       break;
     }
     default:

@@ -274,7 +274,7 @@ static int rowsum_launch(Ctx& c, const TA* src, TA* out) {
       SmallRows m{};
       for (int r = 0; r < c.its->small_rows; ++r) m.slab_row[r] = c.its->small_slab_row[(size_t)r];
       k_small_combine<TA, C><<<(unsigned)c.its->small_rows, kThreads, 0, c.s>>>(
-          c.small_part, (int)grid, c.its->small_rows, m, out);
+          c.small_part, (int)grid, c.its->small_rows, m, out, c.d.active);
       FE_CK(cudaGetLastError());
     }
     return 0;
@@ -864,7 +864,10 @@ static int solve_plain_tile(fe_plan* pl, const SolveReq& rq, int64_t col0, int n
     if ((e = launch_pupdate<C>(c, ST, pe, c.part_a, c.part_b, "pupdate", by.pupdate))) return e;
     return launch_scalar_phase(c, PH_ALPHA, 0);
   };
-  if ((st = run_loop(pl, c, (int)sizeof(T), cap, nact, body, nullptr))) return st;
+  c.d.active = c.counters + 2;
+  st = run_loop(pl, c, (int)sizeof(T), cap, nact, body, nullptr);
+  c.d.active = nullptr;
+  if (st) return st;
   if (rq.residuals) {
     // r = b - A x (src/AbstractFixedEffectSolver.jl:62)
     if ((st = launch_expand<T, C>(c, TabOne<T, T, vec_of<T, C>()>{X},
@@ -932,7 +935,7 @@ static int solve_mixed_tile(fe_plan* pl, const SolveReq& rq, int64_t col0, int n
   int64_t total_it = 0;
   const bool fuse = c.rowsum;
   for (int round = 0; round <= pl->opt_max_rounds + 1; ++round) {
-    FE_CK(cudaMemsetAsync(c.counters + 1, 0, sizeof(int32_t), c.s));
+    FE_CK(cudaMemsetAsync(c.counters, 0, 2 * sizeof(int32_t), c.s));
     // r = b - A (x64 + dx32) in FP64, with the FP32 copy as the next inner u
     if ((st = launch_expand<double, C>(c, TabSum64<vec_of<double, C>()>{X64, X},
                                        EpiBminusAx<double, double, vec_of<double, C>()>{B64, R64, U, c.inst, 2},
@@ -960,7 +963,10 @@ static int solve_mixed_tile(fe_plan* pl, const SolveReq& rq, int64_t col0, int n
       return launch_scalar_phase(c, PH_ALPHA, 0);
     };
     int64_t done = 0;
-    if ((st = run_loop(pl, c, 1, cap - total_it, nout, body, &done))) return st;
+    c.d.active = c.counters + 2;
+    st = run_loop(pl, c, 1, cap - total_it, nout, body, &done);
+    c.d.active = nullptr;
+    if (st) return st;
     total_it += done;
   }
   if (rq.residuals) {
