@@ -252,9 +252,9 @@ int fe_plan_set_option(fe_plan* plan, int32_t option, double value) {
     case FE_OPT_EXPAND_VARIANT:
     case FE_OPT_SEGSUM_VARIANT: {
       const int v = (int)value;
-      const int vmax = option == FE_OPT_EXPAND_VARIANT ? 3 : 5;
+      const int vmax = 5;
       if (v < -1 || v > vmax) {
-        set_error("kernel variant must be -1 (default) or 0..3 (expand), 0..5 (segsum)");
+        set_error("kernel variant must be -1 (default) or 0..5");
         return FE_ERR_INVALID;
       }
       (option == FE_OPT_EXPAND_VARIANT ? plan->opt_ex_variant : plan->opt_seg_variant) = v;

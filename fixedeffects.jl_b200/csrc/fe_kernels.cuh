@@ -421,10 +421,11 @@ struct SegRun {
 // k_expand: one warp per ExpandItem (a range of sorted observations); U row
 // slots per lane group per step, KB >= number of FEs (compile-time bound so
 // that every index and row load of a step can be issued before the first is
-// consumed).  The next step's refs and weights are prefetched while the
-// current step's rows are in flight.
+// consumed).  PF = 1: the next step's refs and weights are prefetched while
+// the current step's rows are in flight; PF = 2: its old rows as well, so a
+// step waits only for its coefficient-row gathers.
 // ---------------------------------------------------------------------------
-template <typename TA, int C, int U, int KB, bool PF, class Tab, class Epi>
+template <typename TA, int C, int U, int KB, int PF, class Tab, class Epi>
 __global__ void __launch_bounds__(kThreads)
 k_expand(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_items, Tab tab, Epi epi,
          double* __restrict__ part, int64_t S) {
@@ -432,16 +433,17 @@ k_expand(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_items, T
   constexpr int VEC = Sh::VEC, CL = Sh::CL, G = Sh::G;
   constexpr int STEP = G * U;                     // observations per step
   constexpr int NI = STEP >= 32 ? STEP / 32 : 1;  // index registers per lane
+  static_assert(STEP <= 32 || STEP % 32 == 0, "a step's indices fill whole index registers");
   using TP = typename Epi::TP;
   using TN = typename Epi::TN;
   __shared__ double sm[kWarps][32];
   const int lane = threadIdx.x & 31;
   const int wib = threadIdx.x >> 5;
   const int g = lane / CL, jl = lane - g * CL;
-  const int64_t w = (int64_t)blockIdx.x * kWarps + wib;
   double nrm[VEC];
 #pragma unroll
   for (int v = 0; v < VEC; ++v) nrm[v] = 0.0;
+  const int64_t w = (int64_t)blockIdx.x * kWarps + wib;
   if (w < n_items) {
     const ExpandItem it = items[w];
     epi.begin(it.prob, jl, C);
@@ -466,6 +468,14 @@ k_expand(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_items, T
         }
       };
       if (PF) fetch(it.ib);
+      VA<TP, VEC> oldn[U];  // PF == 2: the next step's old rows
+      if (PF == 2) {
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          const int64_t i = it.ib + u * G + g;
+          if (i < it.ie && epi.act) oldn[u] = epi.pre(i * C + jl * VEC);
+        }
+      }
       for (int64_t base = it.ib; base < it.ie; base += STEP) {
         if (!PF) fetch(base);
         int rc[KB][NI];
@@ -485,21 +495,34 @@ k_expand(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_items, T
           const int64_t i = base + u * G + g;
 #pragma unroll
           for (int v = 0; v < VEC; ++v) s[u].v[v] = TA(0);
-          if (i < it.ie && epi.act) old[u] = epi.pre(i * C + jl * VEC);
+          if (PF == 2) {
+            old[u] = oldn[u];
+          } else if (i < it.ie && epi.act) {
+            old[u] = epi.pre(i * C + jl * VEC);
+          }
+        }
+        if (PF == 2 && base + STEP < it.ie) {
+#pragma unroll
+          for (int u = 0; u < U; ++u) {
+            const int64_t i = base + STEP + u * G + g;
+            if (i < it.ie && epi.act) oldn[u] = epi.pre(i * C + jl * VEC);
+          }
         }
 #pragma unroll
         for (int k = 0; k < KB; ++k) {
           if (k < K) {
             const TA* __restrict__ sc = scale_of<TA>(d, k);
             const int64_t lb = d.lev_base[k];
+            const bool wk = cw_of<TA>(d, k) != nullptr;  // uniform
 #pragma unroll
             for (int u = 0; u < U; ++u) {
               const int q = u * G;  // + g: the same index register (G divides 32)
               const int ref = __shfl_sync(FE_FULL, rc[k][q >> 5], (q & 31) + g);
-              const TA c = __shfl_sync(FE_FULL, cc[k][q >> 5], (q & 31) + g);
+              const TA c = wk ? __shfl_sync(FE_FULL, cc[k][q >> 5], (q & 31) + g) : TA(1);
               const int64_t i = base + u * G + g;
               if (i < it.ie && epi.act) {
-                const TA cs = c * __ldg(sc + ref);
+                const TA scl = __ldg(sc + ref);
+                const TA cs = wk ? c * scl : scl;
                 const VA<TA, VEC> t = tab.load((lb + ref) * C + jl * VEC);
 #pragma unroll
                 for (int v = 0; v < VEC; ++v) s[u].v[v] += cs * t.v[v];
@@ -535,10 +558,10 @@ k_expand(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_items, T
 // primary level is stored at each key change, and every row is added into the
 // small-FE tables.  The segsum then gathers only the remaining (large) FEs.
 //
-// Work split: CTA b takes the contiguous item range
-// [b n / grid, (b+1) n / grid) of the expand items (whole primary levels, or
-// pieces of long ones) and its warps take every 8th item of it, so the
-// tables' summation order depends only on the grid size.  At the end the 8
+// Work split: warp wib of CTA b takes the expand items (whole primary levels,
+// or pieces of long ones) b*8 + wib + j*grid*8, so the warps in flight work
+// on neighbouring rows and the tables' summation order depends only on the
+// grid size.  At the end the 8
 // warp tables are summed (warp order, FP64) into the CTA's partial slot;
 // k_small_combine sums the slots in CTA order into the [P][C] slab.
 // ---------------------------------------------------------------------------
@@ -691,9 +714,8 @@ k_rowsum(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_items,
   const TA* __restrict__ cw0 = NS > 0 ? cw_of<TA>(d, rs.small_fe[0]) : nullptr;
   const TA* __restrict__ cw1 = NS > 1 ? cw_of<TA>(d, rs.small_fe[1]) : nullptr;
   const int off0 = rs.small_off[0], off1 = rs.small_off[1];
-  const int64_t w0 = (int64_t)blockIdx.x * n_items / gridDim.x;
-  const int64_t w1 = (int64_t)(blockIdx.x + 1) * n_items / gridDim.x;
-  for (int64_t wi = w0 + wib; wi < w1; wi += kWarps) {
+  const int64_t wstride = (int64_t)gridDim.x * kWarps;
+  for (int64_t wi = (int64_t)blockIdx.x * kWarps + wib; wi < n_items; wi += wstride) {
     const ExpandItem it = items[wi];
     const int64_t ie = it.ie;
     if (ie <= it.ib) continue;
@@ -816,9 +838,8 @@ k_rowsum_reg(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_item
   const TA* __restrict__ cw0 = NS > 0 ? cw_of<TA>(d, rs.small_fe[0]) : nullptr;
   const TA* __restrict__ cw1 = NS > 1 ? cw_of<TA>(d, rs.small_fe[1]) : nullptr;
   const int off0 = rs.small_off[0], off1 = rs.small_off[1];
-  const int64_t w0 = (int64_t)blockIdx.x * n_items / gridDim.x;
-  const int64_t w1 = (int64_t)(blockIdx.x + 1) * n_items / gridDim.x;
-  for (int64_t wi = w0 + wib; wi < w1; wi += kWarps) {
+  const int64_t wstride = (int64_t)gridDim.x * kWarps;
+  for (int64_t wi = (int64_t)blockIdx.x * kWarps + wib; wi < n_items; wi += wstride) {
     const ExpandItem it = items[wi];
     const int64_t ie = it.ie;
     if (ie <= it.ib) continue;
@@ -967,6 +988,7 @@ k_segsum(const FeDev d, const ReduceItem* __restrict__ items, int64_t n_items, L
   constexpr int VEC = Sh::VEC, CL = Sh::CL, G = Sh::G;
   constexpr int STEP = G * U;
   constexpr int NI = STEP >= 32 ? STEP / 32 : 1;
+  static_assert(STEP <= 32 || STEP % 32 == 0, "a step's indices fill whole index registers");
   __shared__ double smt[kWarps][32];
   const int lane = threadIdx.x & 31;
   const int g = lane / CL, jl = lane - g * CL;
@@ -1062,6 +1084,7 @@ k_segsum_async(const FeDev d, const ReduceItem* __restrict__ items, int64_t n_it
   using L = AsyncSegLayout<TA, C, U, S>;
   constexpr int STEP = L::STEP;
   constexpr int NI = STEP >= 32 ? STEP / 32 : 1;
+  static_assert(STEP <= 32 || STEP % 32 == 0, "a step's indices fill whole index registers");
   constexpr int CHUNK = VEC * (int)sizeof(TA);  // bytes a lane copies per row
   extern __shared__ __align__(16) unsigned char dyn_smem[];
   __shared__ double smt[kWarps][32];
@@ -1168,6 +1191,7 @@ k_segsum_async(const FeDev d, const ReduceItem* __restrict__ items, int64_t n_it
 template <typename T, int VEC>
 struct PEpiLsmr {
   using TS = T;
+  using TN = T;  // norm accumulation within an item
   T* __restrict__ V;
   T* __restrict__ H;
   T* __restrict__ Hb;
@@ -1197,8 +1221,7 @@ struct PEpiLsmr {
     }
   }
   __device__ __forceinline__ void update(const FeDev& d, int k, int64_t l, int64_t o,
-                                         const VA<T, VEC>& sum, double (&na)[VEC],
-                                         double (&nb)[VEC]) {
+                                         const VA<T, VEC>& sum, TN (&na)[VEC], TN (&nb)[VEC]) {
     VA<T, VEC> vv = vld<T, VEC>(V + o);
     if (upd_bits) {
       VA<T, VEC> hh = vld<T, VEC>(H + o);
@@ -1219,7 +1242,7 @@ struct PEpiLsmr {
           hb.v[v] = T(0);
           if (m == 3) xx.v[v] = T(0);
         }
-        if (m != 0) nb[v] += (double)xx.v[v] * (double)xx.v[v];
+        if (m != 0) nb[v] += xx.v[v] * xx.v[v];
       }
       vst<T, VEC>(H + o, hh);
       vst<T, VEC>(Hb + o, hb);
@@ -1232,7 +1255,7 @@ struct PEpiLsmr {
         if ((v_bits >> v) & 1u) {
           const T vn = sum.v[v] * sc * rd_acc[v] - rd_v[v] * vv.v[v];
           vv.v[v] = vn;
-          na[v] += (double)vn * (double)vn;
+          na[v] += vn * vn;
         }
       }
       vst<T, VEC>(V + o, vv);
@@ -1244,6 +1267,7 @@ struct PEpiLsmr {
 template <typename TOut, int VEC>
 struct PEpiStoreX {
   using TS = double;
+  using TN = double;
   TOut* __restrict__ X;
   bool act;
   __device__ __forceinline__ void begin(int, int, int) { act = true; }
@@ -1263,6 +1287,7 @@ struct PEpiStoreX {
 template <int VEC>
 struct PEpiGrad64 {
   using TS = double;
+  using TN = double;
   float* __restrict__ V32;
   double* __restrict__ X64;
   const float* __restrict__ X32;
@@ -1303,6 +1328,7 @@ struct PEpiGrad64 {
 // (src/SolverCPU.jl:84-88, issue #97 of the reference).  C = 1.
 struct PEpiScale {
   using TS = double;
+  using TN = double;
   double* sd[kMaxFE];
   float* sf[kMaxFE];
   bool act;
@@ -1327,6 +1353,7 @@ k_pupdate(const FeDev d, const PItem* __restrict__ items, int64_t n_items,
   using TS = typename Epi::TS;
   using Sh = Shape<TS, C>;
   constexpr int VEC = Sh::VEC, CL = Sh::CL, G = Sh::G;
+  using TN = typename Epi::TN;
   __shared__ double sm[kWarps][32];
   const int lane = threadIdx.x & 31;
   const int g = lane / CL, jl = lane - g * CL;
@@ -1343,6 +1370,12 @@ k_pupdate(const FeDev d, const PItem* __restrict__ items, int64_t n_items,
     if (__any_sync(FE_FULL, epi.act)) {
       const int k = it.fe;
       const int64_t lb = d.lev_base[k];
+      TN ia[VEC], ib[VEC];  // norms of this item, flushed below
+#pragma unroll
+      for (int v = 0; v < VEC; ++v) {
+        ia[v] = TN(0);
+        ib[v] = TN(0);
+      }
       for (int64_t base = it.rb; base < it.re; base += (int64_t)G * U) {
         VA<TS, VEC> sv[U];
 #pragma unroll
@@ -1353,8 +1386,13 @@ k_pupdate(const FeDev d, const PItem* __restrict__ items, int64_t n_items,
 #pragma unroll
         for (int u = 0; u < U; ++u) {
           const int64_t row = base + u * G + g;
-          if (row < it.re && epi.act) epi.update(d, k, row - lb, row * C + jl * VEC, sv[u], na, nb);
+          if (row < it.re && epi.act) epi.update(d, k, row - lb, row * C + jl * VEC, sv[u], ia, ib);
         }
+      }
+#pragma unroll
+      for (int v = 0; v < VEC; ++v) {
+        na[v] = (double)ia[v];
+        nb[v] = (double)ib[v];
       }
     }
   }

@@ -68,6 +68,7 @@ k_segsum_scale_one_fe(const FeDev d, const ReduceItem* __restrict__ items, int64
   constexpr int VEC = Sh::VEC, CL = Sh::CL, G = Sh::G;
   constexpr int STEP = G * U;
   constexpr int NI = STEP >= 32 ? STEP / 32 : 1;
+  static_assert(STEP <= 32 || STEP % 32 == 0, "a step's indices fill whole index registers");
   __shared__ double smt[kWarps][32];
   const int lane = threadIdx.x & 31;
   const int g = lane / CL, jl = lane - g * CL;

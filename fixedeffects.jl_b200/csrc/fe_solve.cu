@@ -76,7 +76,7 @@ static const std::string& tune_signature(fe_plan* pl) {
       (void)cudaGetLastError();
       os << "unknown";
     }
-    os << "/kv2/N" << pl->N << "/P" << pl->nprob << "/K" << pl->K << "/w" << (pl->weighted ? 1 : 0);
+    os << "/kv3/N" << pl->N << "/P" << pl->nprob << "/K" << pl->K << "/w" << (pl->weighted ? 1 : 0);
     for (int k = 0; k < pl->K; ++k) os << "/" << pl->nlev[k] << (pl->interacted[k] ? "i" : "");
     pl->tune_signature = os.str();
   }

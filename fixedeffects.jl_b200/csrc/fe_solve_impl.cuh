@@ -172,10 +172,11 @@ struct Ctx {
 // whether the next step's indices are prefetched).  Variant 0 is the default;
 // fe_plan_set_option(FE_OPT_EXPAND_VARIANT / FE_OPT_SEGSUM_VARIANT) selects
 // another, which is how the tuner compares them.
-//   expand: 0 U=2 PF, 1 U=4 PF, 2 U=2 no-PF, 3 U=4 no-PF
+//   expand: 0 U=2 PF, 1 U=4 PF, 2 U=2 no-PF, 3 U=4 no-PF,
+//           4 U=2 PF of refs and old rows, 5 U=4 PF of refs and old rows
 //   segsum: 0 U=8 no-PF, 1 U=4 PF, 2 U=8 PF, 3 U=4 no-PF,
 //           4 cp.async ring U=4 x 4 stages, 5 cp.async ring U=2 x 6 stages
-constexpr int kVariants = 4;
+constexpr int kVariants = 6;
 constexpr int kSegVariants = 6;
 template <int C> struct Tune {
   static constexpr int kPU = 4;
@@ -196,7 +197,7 @@ inline int pick_seg(const fe_plan* pl) {
 }
 template <typename T, int C> constexpr int vec_of() { return Shape<T, C>::VEC; }
 
-template <int KB, int U, bool PF, typename TA, int C, class Tab, class Epi>
+template <int KB, int U, int PF, typename TA, int C, class Tab, class Epi>
 static int expand_kbu(Ctx& c, Tab tab, Epi epi, double* part) {
   const unsigned grid = (unsigned)(c.its->ex.size() / kWarps);
   const ExpandItem* items = c.its->d_ex.as<ExpandItem>();
@@ -211,10 +212,12 @@ template <int KB, typename TA, int C, class Tab, class Epi>
 static int expand_kb(Ctx& c, Tab tab, Epi epi, double* part) {
   const int var = pick_ex(c.pl);
   switch (var) {
-    case 1: return expand_kbu<KB, 4, true, TA, C>(c, tab, epi, part);
-    case 2: return expand_kbu<KB, 2, false, TA, C>(c, tab, epi, part);
-    case 3: return expand_kbu<KB, 4, false, TA, C>(c, tab, epi, part);
-    default: return expand_kbu<KB, 2, true, TA, C>(c, tab, epi, part);
+    case 1: return expand_kbu<KB, 4, 1, TA, C>(c, tab, epi, part);
+    case 2: return expand_kbu<KB, 2, 0, TA, C>(c, tab, epi, part);
+    case 3: return expand_kbu<KB, 4, 0, TA, C>(c, tab, epi, part);
+    case 4: return expand_kbu<KB, 2, 2, TA, C>(c, tab, epi, part);
+    case 5: return expand_kbu<KB, 4, 2, TA, C>(c, tab, epi, part);
+    default: return expand_kbu<KB, 2, 1, TA, C>(c, tab, epi, part);
   }
 }
 

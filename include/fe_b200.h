@@ -61,7 +61,7 @@ extern "C" {
                                 reduce the primary FE and up to two small FEs in one
                                 contiguous row-sum pass; 0: every FE by the
                                 level-order segsum */
-#define FE_OPT_EXPAND_VARIANT 7 /* expand kernel variant 0..3, -1 = default */
+#define FE_OPT_EXPAND_VARIANT 7 /* expand kernel variant 0..5, -1 = default */
 #define FE_OPT_SEGSUM_VARIANT 8 /* segsum kernel variant 0..5, -1 = default */
 #define FE_OPT_AUTOTUNE 9    /* 1 (default): time the kernel variants on the first
                                 solve of a tile shape; the choice is kept in the
