@@ -2,12 +2,11 @@
 // fixed effect recomputed without any device allocation.
 //
 // Who needs it: code that must not call cudaMalloc at that moment.  Examples
-// are a stream that is being captured into a CUDA graph (an allocation
-// invalidates the capture), a caller whose device memory is owned by its own
-// pool or by another runtime (Julia's CUDA.jl allocator, for instance), and a
-// host callback.  fe_plan_update_weights allocates its level-sum and
-// piece-partial scratch on every call; this entry point keeps that scratch in
-// one file-scope device array instead.
+// are a caller whose device memory is owned by its own pool or by another
+// runtime (Julia's CUDA.jl allocator, for instance), and a host callback.
+// fe_plan_update_weights allocates its level-sum and piece-partial scratch on
+// every call; this entry point keeps that scratch in one file-scope device
+// array instead.
 //
 // The array is a fixed kNoAllocScratchBytes (8 MiB) per device, held from the
 // moment the library is loaded until the process exits.  Every call shares

@@ -194,9 +194,10 @@ int fe_plan_reset_stats(fe_plan* plan);
  * (the values fe_plan_get_scales returns, src/SolverCPU.jl:78-89) into
  * `scale_out_dev`, n_levels[fe_index] doubles of DEVICE memory, enqueued on
  * `stream` (NULL: the plan's stream), without allocating any memory.  It is
- * for callers that cannot call cudaMalloc at that point: a stream being
- * captured into a CUDA graph, a caller whose device memory belongs to its own
- * pool or runtime (e.g. Julia's CUDA.jl), a host callback.
+ * for callers that cannot call cudaMalloc at that point: a caller whose device
+ * memory belongs to its own pool or runtime (e.g. Julia's CUDA.jl allocator,
+ * which owns the device heap it hands out), or code on a path where a
+ * cudaMalloc would stall or is not allowed, such as a host callback.
  *
  * Its scratch is one file-scope device array of FE_NOALLOC_SCRATCH_BYTES
  * (8 MiB) that every GPU which loads the library holds until the process

@@ -1,6 +1,6 @@
 """fe_plan_scales_noalloc: the allocation-free recomputation of one fixed
-effect's Jacobi scales, for callers that cannot call cudaMalloc (a stream
-under CUDA-graph capture, a caller with its own device-memory pool).  Its
+effect's Jacobi scales, for callers that cannot call cudaMalloc (a caller
+whose device memory belongs to its own pool, a host callback).  Its
 output must equal what fe_plan_get_scales returns for the same plan.
 
 This file is collected last on purpose: it exercises a shared, fixed-size
