@@ -392,22 +392,23 @@ def run_sweep(args):
     for prec, tile, ncols in (("mixed", 0, pb.Y.shape[1]), ("fp64", 1, min(4, pb.Y.shape[1]))):
         feM = fe.AbstractFixedEffectSolver(fes, pb.weights, "CUDA", np.float64, precision=prec)
         feM.set_option(fe._lib.FE_OPT_TILE, tile)
-        for e in range(4):
-            for sv in range(4):
-                feM.set_option(fe._lib.FE_OPT_EXPAND_VARIANT, e)
-                feM.set_option(fe._lib.FE_OPT_SEGSUM_VARIANT, sv)
-                best = 1e30
-                for _ in range(3):
-                    Y = Y0[:, :ncols].clone().t().contiguous().t()
-                    if prec == "fp64":
-                        Y = Y.double().t().contiguous().t()
-                    torch.cuda.synchronize()
-                    t = time.perf_counter()
-                    feM.solve_residuals(Y, tol=1e-8, maxiter=10000)
-                    torch.cuda.synchronize()
-                    best = min(best, time.perf_counter() - t)
-                mode = f"{prec} C={'32' if tile == 0 else '1'}"
-                print(f"| {mode} | {e} | {sv} | {best * 1e3:.1f} | {ncols / best:.1f} |", flush=True)
+        combos = [(e, sv) for e in range(6) for sv in range(6)] + [(-1, -1)]  # last: tuned
+        for e, sv in combos:
+            feM.set_option(fe._lib.FE_OPT_EXPAND_VARIANT, e)
+            feM.set_option(fe._lib.FE_OPT_SEGSUM_VARIANT, sv)
+            best = 1e30
+            for _ in range(3):
+                Y = Y0[:, :ncols].clone().t().contiguous().t()
+                if prec == "fp64":
+                    Y = Y.double().t().contiguous().t()
+                torch.cuda.synchronize()
+                t = time.perf_counter()
+                feM.solve_residuals(Y, tol=1e-8, maxiter=10000)
+                torch.cuda.synchronize()
+                best = min(best, time.perf_counter() - t)
+            mode = f"{prec} C={'32' if tile == 0 else '1'}"
+            es, ss = ("tuned", "tuned") if e < 0 else (e, sv)
+            print(f"| {mode} | {es} | {ss} | {best * 1e3:.1f} | {ncols / best:.1f} |", flush=True)
         feM.close()
     return 0
 

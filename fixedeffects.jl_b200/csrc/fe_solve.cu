@@ -96,7 +96,7 @@ bool tune_cache_load(fe_plan* pl, int C, int sT, int* ex, int* seg) {
     std::string s;
     int c = 0, t = 0, e = 0, g = 0;
     if (!(is >> s >> c >> t >> e >> g)) continue;
-    if (s == sig && c == C && t == sT && e >= 0 && e < 4 && g >= 0 && g < 6) {
+    if (s == sig && c == C && t == sT && e >= 0 && e < 6 && g >= 0 && g < 6) {
       *ex = e;
       *seg = g;
       found = true;  // the last matching line wins

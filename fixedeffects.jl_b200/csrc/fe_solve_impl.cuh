@@ -182,18 +182,21 @@ template <int C> struct Tune {
   static constexpr int kPU = 4;
 };
 // tuning state of the tile being solved
+// tuning state of the tile being solved, per element size (0: FP32, 1: FP64)
 struct TuneSel {
-  int ex = -1, seg = -1;
+  int ex[2] = {-1, -1}, seg[2] = {-1, -1};
 };
 inline TuneSel& cur_tune() {
   static thread_local TuneSel t;
   return t;
 }
-inline int pick_ex(const fe_plan* pl) {
-  return pl->opt_ex_variant >= 0 ? pl->opt_ex_variant : (cur_tune().ex >= 0 ? cur_tune().ex : 0);
+inline int pick_ex(const fe_plan* pl, size_t elem) {
+  const int t = cur_tune().ex[elem == 8 ? 1 : 0];
+  return pl->opt_ex_variant >= 0 ? pl->opt_ex_variant : (t >= 0 ? t : 0);
 }
-inline int pick_seg(const fe_plan* pl) {
-  return pl->opt_seg_variant >= 0 ? pl->opt_seg_variant : (cur_tune().seg >= 0 ? cur_tune().seg : 0);
+inline int pick_seg(const fe_plan* pl, size_t elem) {
+  const int t = cur_tune().seg[elem == 8 ? 1 : 0];
+  return pl->opt_seg_variant >= 0 ? pl->opt_seg_variant : (t >= 0 ? t : 0);
 }
 template <typename T, int C> constexpr int vec_of() { return Shape<T, C>::VEC; }
 
@@ -210,7 +213,7 @@ static int expand_kbu(Ctx& c, Tab tab, Epi epi, double* part) {
 
 template <int KB, typename TA, int C, class Tab, class Epi>
 static int expand_kb(Ctx& c, Tab tab, Epi epi, double* part) {
-  const int var = pick_ex(c.pl);
+  const int var = pick_ex(c.pl, sizeof(TA));
   switch (var) {
     case 1: return expand_kbu<KB, 4, 1, TA, C>(c, tab, epi, part);
     case 2: return expand_kbu<KB, 2, 0, TA, C>(c, tab, epi, part);
@@ -346,7 +349,7 @@ static int launch_segsum(Ctx& c, Load ld, TA* out, const char* name, double byte
   const unsigned grid = (unsigned)((n + kWarps - 1) / kWarps);
   const ReduceItem* items = c.its->d_rd.as<ReduceItem>();
   const SplitArgs sa = c.seg_split();
-  const int var = pick_seg(c.pl);
+  const int var = pick_seg(c.pl, sizeof(TA));
   if constexpr (Load::kAsyncable) {
     if (var == 4 || var == 5) {
       const int st = var == 4 ? launch_segsum_async<TA, C, 4, 4>(c, ld, out, items, n, grid)
@@ -635,7 +638,9 @@ static int run_loop(fe_plan* pl, Ctx& c, int prec, int64_t cap, int32_t nact0, B
                           c.block, c.ex_block, pl->ws.U.p, pl->ws.V.p, pl->ws.H.p, pl->ws.Hb.p,
                           pl->ws.X.p, c.its, c.counters, c.s, c.small_part};
     for (const void* p : ptrs) key = key * 1315423911u + (size_t)p;
-    key = key * 31 + (size_t)cur_tune().ex * 7 + (size_t)cur_tune().seg;
+    // the variants the captured launches use (tuned, or forced by an option)
+    for (size_t e : {(size_t)4, (size_t)8})
+      key = key * 31 + (size_t)pick_ex(pl, e) * 7 + (size_t)pick_seg(pl, e);
     key = key * 3 + (c.rowsum ? 1u : 0u);
     key = key * 5 + (size_t)(pl->opt_rowsum_variant + 1);
     lg = &pl->graphs[{c.C, prec}];
@@ -687,30 +692,35 @@ static int run_loop(fe_plan* pl, Ctx& c, int prec, int64_t cap, int32_t nact0, B
 bool tune_cache_load(fe_plan* pl, int C, int sT, int* ex, int* seg);
 void tune_cache_store(fe_plan* pl, int C, int sT, int ex, int seg);
 
+// rows: scratch of N x C elements of T; levels: P x C elements of T (their
+// contents are irrelevant to the timing and are left as scratch values)
 template <typename T, int C>
-static int autotune(fe_plan* pl, Ctx& c) {
-  const std::pair<int, int> key(C, (int)sizeof(T));
+static int autotune(fe_plan* pl, Ctx& c, T* rows, T* levels, bool resid_form = false) {
+  // tuning key: element size, + 100 for the mixed mode's FP64 refinement
+  // kernels (a different expand epilogue than the plain FP64 loop)
+  const int kind = (int)sizeof(T) + (resid_form ? 100 : 0);
+  const std::pair<int, int> key(C, kind);
+  const int ti = sizeof(T) == 8 ? 1 : 0;
   auto f = pl->tuned.find(key);
   if (f != pl->tuned.end()) {
-    cur_tune().ex = f->second.first;
-    cur_tune().seg = f->second.second;
+    cur_tune().ex[ti] = f->second.first;
+    cur_tune().seg[ti] = f->second.second;
     return 0;
   }
   int ex = 0, seg = 0;
-  if (tune_cache_load(pl, C, (int)sizeof(T), &ex, &seg)) {
+  if (tune_cache_load(pl, C, kind, &ex, &seg)) {
     pl->tuned[key] = {ex, seg};
-    cur_tune().ex = ex;
-    cur_tune().seg = seg;
+    cur_tune().ex[ti] = ex;
+    cur_tune().seg[ti] = seg;
     return 0;
   }
   if (!pl->opt_autotune) {
-    cur_tune().ex = 0;
-    cur_tune().seg = 0;
+    cur_tune().ex[ti] = 0;
+    cur_tune().seg[ti] = 0;
     return 0;
   }
-  Workspace& w = pl->ws;
   const size_t N = (size_t)pl->N, P = (size_t)pl->P;
-  FE_CK(cudaMemsetAsync(w.U.p, 0, N * C * sizeof(T), c.s));
+  FE_CK(cudaMemsetAsync(rows, 0, N * C * sizeof(T), c.s));
   std::vector<Inst> h((size_t)pl->nprob * C);
   for (Inst& s : h) {
     memset(&s, 0, sizeof(s));
@@ -727,7 +737,7 @@ static int autotune(fe_plan* pl, Ctx& c) {
   pl->prof.on = false;
   const int save_ex = pl->opt_ex_variant, save_seg = pl->opt_seg_variant;
   EpiExpandLsmr<T, vec_of<T, C>()> ee{};
-  ee.U = w.U.as<T>();
+  ee.U = rows;
   ee.inst = c.inst;
   float best_e = 1e30f, best_s = 1e30f;
   int st = 0;
@@ -736,7 +746,20 @@ static int autotune(fe_plan* pl, Ctx& c) {
     float ms = 1e30f;
     for (int rep = 0; rep < 3 && !st; ++rep) {
       cudaEventRecord(e0, c.s);
-      st = launch_expand<T, C>(c, TabOne<T, T, vec_of<T, C>()>{w.V.as<T>()}, ee, c.part_e, "tune", 0.0);
+      if constexpr (std::is_same<T, double>::value) {
+        if (resid_form) {  // the refinement's r = b - A (x64 + x32), all columns
+          Workspace& w = pl->ws;
+          st = launch_expand<double, C>(
+              c, TabSum64<vec_of<double, C>()>{levels, w.X.as<float>()},
+              EpiBminusAx<double, double, vec_of<double, C>()>{w.B64.as<double>(), rows,
+                                                                w.U.as<float>(), c.inst, 0},
+              c.part_e, "tune", 0.0);
+        } else {
+          st = launch_expand<T, C>(c, TabOne<T, T, vec_of<T, C>()>{levels}, ee, c.part_e, "tune", 0.0);
+        }
+      } else {
+        st = launch_expand<T, C>(c, TabOne<T, T, vec_of<T, C>()>{levels}, ee, c.part_e, "tune", 0.0);
+      }
       cudaEventRecord(e1, c.s);
       cudaEventSynchronize(e1);
       float t = 0.f;
@@ -753,7 +776,7 @@ static int autotune(fe_plan* pl, Ctx& c) {
     float ms = 1e30f;
     for (int rep = 0; rep < 3 && !st; ++rep) {
       cudaEventRecord(e0, c.s);
-      st = launch_segsum<T, C>(c, LoadIn<T, T, vec_of<T, C>()>{w.U.as<T>()}, static_cast<T*>(c.S), "tune",
+      st = launch_segsum<T, C>(c, LoadIn<T, T, vec_of<T, C>()>{rows}, static_cast<T*>(c.S), "tune",
                                0.0, c.rowsum);
       cudaEventRecord(e1, c.s);
       cudaEventSynchronize(e1);
@@ -776,9 +799,9 @@ static int autotune(fe_plan* pl, Ctx& c) {
   // back at zero (every split level completed); clear S for the solve
   FE_CK(cudaMemsetAsync(c.S, 0, P * C * 8, c.s));
   pl->tuned[key] = {ex, seg};
-  tune_cache_store(pl, C, (int)sizeof(T), ex, seg);
-  cur_tune().ex = ex;
-  cur_tune().seg = seg;
+  tune_cache_store(pl, C, kind, ex, seg);
+  cur_tune().ex[ti] = ex;
+  cur_tune().seg[ti] = seg;
   return 0;
 }
 
@@ -811,7 +834,7 @@ static int solve_plain_tile(fe_plan* pl, const SolveReq& rq, int64_t col0, int n
   Ctx c;
   int st = prepare(pl, C, (int)sizeof(T), false, c);
   if (st) return st;
-  if ((st = autotune<T, C>(pl, c))) return st;
+  if ((st = autotune<T, C>(pl, c, pl->ws.U.as<T>(), pl->ws.V.as<T>()))) return st;
   Workspace& w = pl->ws;
   const Bytes by = alg_bytes(pl, c.its, C, (int)sizeof(T));
   std::vector<Inst> h;
@@ -897,7 +920,10 @@ static int solve_mixed_tile(fe_plan* pl, const SolveReq& rq, int64_t col0, int n
   Ctx c;
   int st = prepare(pl, C, 4, true, c);
   if (st) return st;
-  if ((st = autotune<float, C>(pl, c))) return st;
+  // FP32 loop kernels on U/V; FP64 refinement kernels on R64/X64 (FP64-sized)
+  if ((st = autotune<float, C>(pl, c, pl->ws.U.as<float>(), pl->ws.V.as<float>()))) return st;
+  if ((st = autotune<double, C>(pl, c, pl->ws.R64.as<double>(), pl->ws.X64.as<double>(), true)))
+    return st;
   Workspace& w = pl->ws;
   const Bytes by = alg_bytes(pl, c.its, C, 4);
   std::vector<Inst> h;

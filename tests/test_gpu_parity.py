@@ -323,15 +323,21 @@ def test_autotuner_persists_choice(fe, synth, tmp_path, monkeypatch):
     feM = fe.AbstractFixedEffectSolver(fes, None, "CUDA", np.float32)
     R1, _, _ = feM.solve_residuals(Y.copy(), tol=1e-8)
     feM.close()
+    # mixed precision tunes its FP32 loop kernels (element size 4) and its
+    # FP64 refinement kernels (recorded as 108): one line each
     lines = cache.read_text().strip().splitlines()
-    assert len(lines) == 1
-    sig, C, sT, ex, seg = lines[0].split()
-    assert (int(C), int(sT)) == (8, 4) and 0 <= int(ex) < 6 and 0 <= int(seg) < 6
-    # a second plan of the same shape reuses the cached choice (no new line)
+    assert len(lines) == 2
+    shapes = set()
+    for line in lines:
+        sig, C, sT, ex, seg = line.split()
+        shapes.add((int(C), int(sT)))
+        assert 0 <= int(ex) < 6 and 0 <= int(seg) < 6
+    assert shapes == {(8, 4), (8, 108)}
+    # a second plan of the same shape reuses the cached choices (no new line)
     feM = fe.AbstractFixedEffectSolver(fes, None, "CUDA", np.float32)
     R2, _, _ = feM.solve_residuals(Y.copy(), tol=1e-8)
     feM.close()
-    assert len(cache.read_text().strip().splitlines()) == 1
+    assert len(cache.read_text().strip().splitlines()) == 2
     assert np.array_equal(R1, R2)
 
 
