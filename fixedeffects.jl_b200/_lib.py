@@ -36,6 +36,7 @@ FE_OPT_AUTOTUNE = 9
 FE_OPT_MIXED_WARM_START = 10
 FE_OPT_GRAPH = 11
 FE_OPT_ROWSUM_VARIANT = 12
+FE_OPT_ABSORB = 14
 
 # every symbol declared in include/fe_b200.h
 EXPORTS = (

@@ -25,6 +25,7 @@ constexpr int kScalarThreads = 256;
 constexpr int kSentinel = 0x7fffffff;  // "no level" key
 constexpr int kSmallRows = 32;         // rows of the row-sum pass's small-FE tables
 constexpr int kRowSumSmallFE = 2;      // small FEs the row-sum pass reduces
+constexpr int64_t kDemeanRows = 64;    // rows per demean item (whole primary levels)
 
 // A contiguous range of observations (sorted order) processed by one warp.
 // Items hold whole levels of the primary FE (the FE that orders the
@@ -101,10 +102,14 @@ struct FeDev {
   int64_t lev_base[kMaxFE];      // first row of FE k in a [P][C] slab
   int32_t primary;               // FE whose levels order the observations
   // set inside the LSMR loop only: the number of instances still running
-  // (written by the scalar kernel's beta phase); the reductions return at
-  // once when it is 0, so the iterations that finish a replayed chunk after
-  // every instance has stopped cost launches only
+  // (written by the scalar kernel's beta phase, and by the refinement phase
+  // that starts an inner solve); the reductions return at once when it is 0,
+  // so the iterations that finish a replayed chunk after every instance has
+  // stopped cost launches only
   const int32_t* active;
+  // absorbed-primary mode: the expand leaves out the primary FE (its effect is
+  // projected out of the rows by the demean pass instead)
+  int32_t absorb;
 };
 
 // LSMR state of one instance (problem p, column j).  Scalars are FP64 in every

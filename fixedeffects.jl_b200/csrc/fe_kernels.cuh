@@ -113,6 +113,27 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
 
+// Streaming (evict-first) variants for data touched once per kernel, so that
+// it does not push reused coefficient rows out of L1/L2.
+template <typename T, int V>
+__device__ __forceinline__ VA<T, V> vld_cs(const T* p) {
+  using IO = VecIO<T, V>;
+  typename IO::Cr c[IO::kN];
+#pragma unroll
+  for (int q = 0; q < IO::kN; ++q) c[q] = __ldcs(reinterpret_cast<const typename IO::Cr*>(p) + q);
+  VA<T, V> a;
+  memcpy(&a, c, sizeof(a));
+  return a;
+}
+template <typename T, int V>
+__device__ __forceinline__ void vst_cs(T* p, const VA<T, V>& a) {
+  using IO = VecIO<T, V>;
+  typename IO::Cr c[IO::kN];
+  memcpy(c, &a, sizeof(a));
+#pragma unroll
+  for (int q = 0; q < IO::kN; ++q) __stcs(reinterpret_cast<typename IO::Cr*>(p) + q, c[q]);
+}
+
 // lane shape for accumulation type TA and tile width C
 template <typename TA, int C>
 struct Shape {
@@ -209,7 +230,7 @@ struct EpiExpandLsmr {
       act = act || s.active != 0;
     }
   }
-  __device__ __forceinline__ VA<T, VEC> pre(int64_t o) const { return vld<T, VEC>(U + o); }
+  __device__ __forceinline__ VA<T, VEC> pre(int64_t o) const { return vld_cs<T, VEC>(U + o); }
   __device__ __forceinline__ VA<T, VEC> apply(int64_t o, const VA<T, VEC>& s,
                                                const VA<T, VEC>& old, TN (&nrm)[VEC]) {
     VA<T, VEC> u;
@@ -218,7 +239,7 @@ struct EpiExpandLsmr {
       u.v[v] = av[v] * s.v[v] + au[v] * old.v[v];
       nrm[v] += u.v[v] * u.v[v];
     }
-    vst<T, VEC>(U + o, u);
+    vst_cs<T, VEC>(U + o, u);
     return u;
   }
 };
@@ -461,7 +482,7 @@ k_expand(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_items, T
           for (int r = 0; r < NI; ++r) {
             const int64_t p = base + r * 32 + lane;
             const bool ok = k < K && p < it.ie && (r * 32 + lane) < STEP;
-            rl[k][r] = ok ? __ldg(d.refs[k] + p) : kSentinel;
+            rl[k][r] = ok ? __ldcs(d.refs[k] + p) : kSentinel;
             const TA* __restrict__ cw = cw_of<TA>(d, k < K ? k : 0);
             cl[k][r] = (ok && cw) ? __ldg(cw + p) : TA(1);
           }
@@ -510,7 +531,7 @@ k_expand(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_items, T
         }
 #pragma unroll
         for (int k = 0; k < KB; ++k) {
-          if (k < K) {
+          if (k < K && !(d.absorb && k == d.primary)) {
             const TA* __restrict__ sc = scale_of<TA>(d, k);
             const int64_t lb = d.lev_base[k];
             const bool wk = cw_of<TA>(d, k) != nullptr;  // uniform
@@ -906,6 +927,163 @@ k_rowsum_reg(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_item
     const int n = rs.small_rows * C;
     double* __restrict__ out = rs.small_part + (int64_t)blockIdx.x * n;
     const TA* t0 = reinterpret_cast<const TA*>(rowsum_smem);
+    for (int e = threadIdx.x; e < n; e += kThreads) {
+      double t = 0.0;
+#pragma unroll
+      for (int w = 0; w < kWarps; ++w) t += (double)t0[(size_t)w * n + e];
+      out[e] = t;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// k_demean: the projection of the absorbed-primary mode.  With the primary FE
+// (whose levels are contiguous row segments, the observations being sorted by
+// it) projected out of the least-squares problem, the solver works with
+// M u = u - a_l (a_l' u) per primary level l, where a_l holds cw_i * scale_l on
+// the rows of level l (a unit vector).  In place on rows [N][32] of T:
+//   pass 1 of an item: z_l = sum_{i in l} cw_i u_i per level -> sum slab
+//                      (the primary FE's rows of the [P][C] slab, free here);
+//   pass 2:            u_i -= cw_i scale_l^2 z_l, ||u||^2 per column into the
+//                      norm slot of the CTA, the small FEs' sums of cw u into
+//                      the per-warp tables (as k_rowsum), optional FP32 copy.
+// Items are whole primary levels (dm list), short enough that the second
+// read of an item's rows hits L1/L2.  Lane = column, STEP rows per step held
+// in registers.  The only cross-lane dependency is the z row of a level,
+// written by all lanes in pass 1 and read in pass 2 after a __syncwarp.
+// ---------------------------------------------------------------------------
+template <typename T, int C, bool W, int NS>
+__global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 3 : 2)
+k_demean(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_items,
+         T* __restrict__ rows, float* __restrict__ rows32, RowSumArgs rs,
+         double* __restrict__ part, int64_t S) {
+  static_assert(C == 32, "one column per lane");
+  constexpr int STEP = sizeof(T) == 4 ? 16 : 8;
+  __shared__ double sm[kWarps][32];
+  extern __shared__ __align__(16) unsigned char demean_smem[];
+  if (d.active && *d.active == 0) return;  // the whole CTA
+  const int lane = threadIdx.x & 31;
+  const int wib = threadIdx.x >> 5;
+  T* tbl = reinterpret_cast<T*>(demean_smem) + (size_t)wib * rs.small_rows * C;
+  for (int e = lane; e < rs.small_rows * C; e += 32) tbl[e] = T(0);
+  __syncwarp();
+  const int kp = d.primary;
+  T* __restrict__ Z = reinterpret_cast<T*>(rs.sum) + d.lev_base[kp] * C + lane;
+  const int32_t* __restrict__ refp = d.refs[kp];
+  const T* __restrict__ cwp = cw_of<T>(d, kp);
+  const T* __restrict__ scp = scale_of<T>(d, kp);
+  const int32_t* __restrict__ ref0 = NS > 0 ? d.refs[rs.small_fe[0]] : nullptr;
+  const int32_t* __restrict__ ref1 = NS > 1 ? d.refs[rs.small_fe[1]] : nullptr;
+  const T* __restrict__ cw0 = NS > 0 ? cw_of<T>(d, rs.small_fe[0]) : nullptr;
+  const T* __restrict__ cw1 = NS > 1 ? cw_of<T>(d, rs.small_fe[1]) : nullptr;
+  const int off0 = rs.small_off[0], off1 = rs.small_off[1];
+  double nrm = 0.0;
+  const int64_t wstride = (int64_t)gridDim.x * kWarps;
+  for (int64_t wi = (int64_t)blockIdx.x * kWarps + wib; wi < n_items; wi += wstride) {
+    const ExpandItem it = items[wi];
+    const int64_t ie = it.ie;
+    if (ie <= it.ib) continue;
+    // pass 1: z_l = sum cw u over each level of the item
+    int ckey = -1;
+    T acc = T(0);
+    for (int64_t base = it.ib; base < ie; base += STEP) {
+      const int nvalid = (int)((ie - base) < STEP ? (ie - base) : STEP);
+      const bool okl = lane < nvalid;
+      const int kpr = okl ? __ldg(refp + base + lane) : kSentinel;
+      const T cpv = (W && okl && cwp) ? __ldg(cwp + base + lane) : T(1);
+      T x[STEP];
+#pragma unroll
+      for (int r = 0; r < STEP; ++r) x[r] = r < nvalid ? rows[(base + r) * C + lane] : T(0);
+      const int kn = __shfl_down_sync(FE_FULL, kpr, 1);
+      const uint32_t bmask = __ballot_sync(FE_FULL, lane + 1 < nvalid && kn != kpr);
+      const int kfirst = __shfl_sync(FE_FULL, kpr, 0);
+      if (ckey >= 0 && ckey != kfirst) {
+        Z[(int64_t)ckey * C] = acc;
+        acc = T(0);
+      }
+#pragma unroll
+      for (int r = 0; r < STEP; ++r)
+        if (r < nvalid) rowsum_primary<T, C, W>(r, x[r], acc, bmask, kpr, cpv, Z);
+      ckey = __shfl_sync(FE_FULL, kpr, nvalid - 1);
+    }
+    if (ckey >= 0) Z[(int64_t)ckey * C] = acc;  // items hold whole levels
+    __syncwarp();  // z rows written by every lane are visible to every lane
+    // pass 2: u -= cw scale^2 z, norms, small-FE sums, FP32 copy
+    for (int64_t base = it.ib; base < ie; base += STEP) {
+      const int nvalid = (int)((ie - base) < STEP ? (ie - base) : STEP);
+      const bool okl = lane < nvalid;
+      const int64_t p = base + lane;
+      const int kpr = okl ? __ldg(refp + p) : 0;
+      T f = T(0);  // cw_i scale_l^2 of row base + lane
+      if (okl) {
+        const T sl = __ldg(scp + kpr);
+        f = sl * sl * ((W && cwp) ? __ldg(cwp + p) : T(1));
+      }
+      int k0 = 0, k1 = 0;
+      T c0 = T(1), c1 = T(1);
+      if (NS > 0 && okl) {
+        k0 = off0 + __ldg(ref0 + p);
+        if (W && cw0) c0 = __ldg(cw0 + p);
+      }
+      if (NS > 1 && okl) {
+        k1 = off1 + __ldg(ref1 + p);
+        if (W && cw1) c1 = __ldg(cw1 + p);
+      }
+      T x[STEP];
+#pragma unroll
+      for (int r = 0; r < STEP; ++r) {
+        if (r < nvalid) {
+          const int kr = __shfl_sync(FE_FULL, kpr, r);
+          const T fr = __shfl_sync(FE_FULL, f, r);
+          const int64_t o = (base + r) * C + lane;
+          const T u = rows[o] - fr * Z[(int64_t)kr * C];
+          rows[o] = u;
+          if (rows32) rows32[o] = (float)u;
+          nrm += (double)u * (double)u;
+          x[r] = u;
+        } else {
+          x[r] = T(0);
+        }
+      }
+      if (NS > 0) {
+        if (nvalid == STEP) {
+#pragma unroll
+          for (int r0 = 0; r0 < STEP; r0 += 4) {
+            rowsum_small4<T, C, W>(r0, x[r0], x[r0 + 1], x[r0 + 2], x[r0 + 3], k0, c0, tbl, lane);
+            if (NS > 1)
+              rowsum_small4<T, C, W>(r0, x[r0], x[r0 + 1], x[r0 + 2], x[r0 + 3], k1, c1, tbl, lane);
+          }
+        } else {
+#pragma unroll
+          for (int r = 0; r < STEP; ++r) {
+            if (r < nvalid) {
+              const int t0 = __shfl_sync(FE_FULL, k0, r);
+              tbl[t0 * C + lane] += W ? x[r] * __shfl_sync(FE_FULL, c0, r) : x[r];
+              if (NS > 1) {
+                const int t1 = __shfl_sync(FE_FULL, k1, r);
+                tbl[t1 * C + lane] += W ? x[r] * __shfl_sync(FE_FULL, c1, r) : x[r];
+              }
+            }
+          }
+        }
+      }
+    }
+  }
+  // ||u||^2: warp -> CTA slot (fixed order); slots beyond the grid hold 0
+  sm[wib][lane] = nrm;
+  __syncthreads();
+  if (part != nullptr && threadIdx.x < C) {
+    double t = 0.0;
+#pragma unroll
+    for (int w = 0; w < kWarps; ++w) t += sm[w][threadIdx.x];
+    part[(int64_t)threadIdx.x * S + blockIdx.x] = t;
+    for (int64_t sl = (int64_t)blockIdx.x + gridDim.x; sl < S; sl += gridDim.x)
+      part[(int64_t)threadIdx.x * S + sl] = 0.0;
+  }
+  if (NS > 0) {
+    const int n = rs.small_rows * C;
+    double* __restrict__ out = rs.small_part + (int64_t)blockIdx.x * n;
+    const T* t0 = reinterpret_cast<const T*>(demean_smem);
     for (int e = threadIdx.x; e < n; e += kThreads) {
       double t = 0.0;
 #pragma unroll

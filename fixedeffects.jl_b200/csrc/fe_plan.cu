@@ -512,12 +512,25 @@ int plan_items(fe_plan* pl, int C, ItemSet** out) {
     if (its->ex.size() == e0)
       for (int w = 0; w < kWarps; ++w) its->ex.push_back({o1, o1, p, -1, 0, 0});
     its->ex_slot_off[p + 1] = (int64_t)(its->ex.size() / kWarps);
-    // P-side items: chunks of the problem's slab rows, per FE, padded likewise
+    // P-side items: chunks of the problem's slab rows, per FE, padded likewise.
+    // Single-problem plans list the non-primary FEs first, padded on their
+    // own, so that the absorbed-primary mode can run just that prefix.
     const size_t q0 = its->pu.size();
-    for (int k = 0; k < K; ++k) {
+    auto pu_fe = [&](int k) {
       const int64_t rb = pl->lev_base[k] + pl->prob_lev_off[(size_t)p * K + k];
       const int64_t re = pl->lev_base[k] + pl->prob_lev_off[(size_t)(p + 1) * K + k];
       for (int64_t b = rb; b < re; b += Tp) its->pu.push_back({b, std::min(re, b + Tp), k, p});
+    };
+    if (nprob == 1) {
+      for (int k = 0; k < K; ++k)
+        if (k != kp) pu_fe(k);
+      while ((its->pu.size() - q0) % kWarps) its->pu.push_back({0, 0, 0, p});
+      if (its->pu.size() == q0)
+        for (int w = 0; w < kWarps; ++w) its->pu.push_back({0, 0, 0, p});
+      its->pu_np = (int64_t)its->pu.size();
+      pu_fe(kp);
+    } else {
+      for (int k = 0; k < K; ++k) pu_fe(k);
     }
     while ((its->pu.size() - q0) % kWarps) its->pu.push_back({0, 0, 0, p});
     if (its->pu.size() == q0)
@@ -571,6 +584,26 @@ int plan_items(fe_plan* pl, int C, ItemSet** out) {
       if (cur_b >= 0) dst.push_back({cur_b, cur_e, k, p, -1, 0});
     }
   }
+  // demean items (absorbed-primary mode: 32-column tiles, one problem, 2+ FEs):
+  // whole primary levels packed up to kDemeanRows rows; a longer level is one
+  // item of its own (the pass walks each item twice, so short items keep the
+  // second read in cache)
+  if (C == 32 && nprob == 1 && K >= 2) {
+    const std::vector<int64_t>& off = pl->seg_off[kp];
+    const int64_t nl = pl->nlev[kp];
+    int64_t cur_b = -1, cur_e = -1;
+    for (int64_t l = 0; l < nl; ++l) {
+      const int64_t b = off[(size_t)l], e = off[(size_t)l + 1];
+      if (e == b) continue;
+      if (cur_b >= 0 && e - cur_b > kDemeanRows) {
+        its->dm.push_back({cur_b, cur_e, 0, -1, 0, 0});
+        cur_b = -1;
+      }
+      if (cur_b < 0) cur_b = b;
+      cur_e = e;
+    }
+    if (cur_b >= 0) its->dm.push_back({cur_b, cur_e, 0, -1, 0, 0});
+  }
   its->rd_large = (int64_t)its->rd.size();
   its->rd.insert(its->rd.end(), rd_small.begin(), rd_small.end());
   its->rd_np = (int64_t)its->rd.size();
@@ -589,6 +622,10 @@ int plan_items(fe_plan* pl, int C, ItemSet** out) {
   if (!st) st = upload(its->d_pu, its->pu.data(), its->pu.size(), s);
   if (!st) st = upload(its->d_ex_off, its->ex_slot_off.data(), its->ex_slot_off.size(), s);
   if (!st) st = upload(its->d_pu_off, its->pu_slot_off.data(), its->pu_slot_off.size(), s);
+  its->Sp_np = its->pu_np / kWarps;
+  const int64_t off_np[2] = {0, its->Sp_np};
+  if (!st) st = upload(its->d_pu_off_np, off_np, 2, s);
+  if (!st) st = upload(its->d_dm, its->dm.data(), its->dm.size(), s);
   if (!st) st = upload(its->d_ex_splits, its->ex_splits.data(), its->ex_splits.size(), s);
   const size_t nsc = std::max<size_t>(its->splits.size(), 1) * 4;
   const size_t nesc = std::max<size_t>(its->ex_splits.size(), 1) * 4;

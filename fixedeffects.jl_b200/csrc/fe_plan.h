@@ -59,6 +59,9 @@ struct ItemSet {
   int sms = 148;                       // multiprocessors of the plan's device
   int64_t ex_n_pieces = 0;
   std::vector<PItem> pu;
+  int64_t pu_np = 0;                   // leading P-side items of the non-primary FEs
+  int64_t Sp_np = 0;                   // their norm slots
+  std::vector<ExpandItem> dm;          // demean items (absorbed-primary mode)
   std::vector<int64_t> ex_slot_off;       // per problem, expand norm slots (CTAs)
   std::vector<int64_t> pu_slot_off;       // per problem, P-side norm slots (CTAs)
   int64_t n_pieces = 0, n_blocks = 0;
@@ -66,6 +69,7 @@ struct ItemSet {
   int64_t Se = 0, Sp = 0;                 // slot counts
   DevBuf d_ex, d_rd, d_splits, d_pu, d_ex_off, d_pu_off, d_split_cnt, d_block_cnt;
   DevBuf d_ex_splits, d_ex_split_cnt, d_ex_block_cnt;
+  DevBuf d_pu_off_np, d_dm;
 };
 
 struct Workspace {
@@ -139,6 +143,7 @@ struct fe_plan {
   int32_t opt_mixed_warm = 1;   // mixed precision starts from x0 = A'b (else x0 = 0)
   int32_t opt_graph = 1;        // replay the LSMR iterations from a CUDA graph
   int32_t opt_rowsum_variant = -1; // row-sum pass: 0 shared-memory ring, 1 registers
+  int32_t opt_absorb = 1;       // mixed residual solves project the primary FE out
   std::map<std::pair<int, int>, fe::LoopGraph> graphs;  // by (C, precision)
   // tuned variants per (tile width C, element size): {expand, segsum}
   std::map<std::pair<int, int>, std::pair<int, int>> tuned;

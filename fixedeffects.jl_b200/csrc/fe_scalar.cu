@@ -288,6 +288,7 @@ __global__ void __launch_bounds__(kScalarThreads) k_scalar(ScalarArgs a) {
       s.normAr0 = s.normAr;
       atomicAdd(a.counters, 1);      // LSMR running (read by the first beta phase)
       atomicAdd(a.counters + 1, 1);  // refinement running
+      atomicAdd(a.counters + 2, 1);  // running, for kernels before the first beta
       break;
     }
     default:

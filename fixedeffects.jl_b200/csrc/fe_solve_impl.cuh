@@ -166,6 +166,7 @@ struct Ctx {
   double* ex_block;
   double* small_part;  // the row-sum pass's CTA partials of the small FEs
   bool rowsum;         // primary and small FEs reduced by the row-sum pass
+  bool absorb = false; // primary FE projected out (demean pass; mixed residual solves)
 };
 
 // Kernel variants (unroll depth = row slots per lane group per step, and
@@ -313,6 +314,85 @@ static int launch_rowsum(Ctx& c, const TA* src, TA* out) {
   }
 }
 
+// The demean pass of the absorbed-primary mode (k_demean) and the combine of
+// its small-FE partials.  rows: [N][32] of T, projected in place; rows32: an
+// optional FP32 copy; out: the [P][C] sum slab (z rows of the primary FE,
+// small-FE sums); ||rows||^2 goes to the expand norm slots.
+template <typename T, int C, bool W, int NS>
+static int demean_launch(Ctx& c, T* rows, float* rows32, T* out) {
+  if constexpr (C == 32) {
+    auto kern = k_demean<T, C, W, NS>;
+    const size_t smem = (size_t)kWarps * c.its->small_rows * C * sizeof(T);
+    static bool attr_set = false;  // per instantiation
+    static size_t occ_smem = (size_t)-1;
+    static int occ = 1;
+    if (!attr_set) {
+      FE_CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)(kWarps * kSmallRows * C * sizeof(T))));
+      attr_set = true;
+    }
+    if (occ_smem != smem) {
+      int o = 0;
+      FE_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, kern, kThreads, smem));
+      occ = std::max(o, 1);
+      occ_smem = smem;
+    }
+    const int64_t n = (int64_t)c.its->dm.size();
+    // norm slots are the expand's: the grid must not exceed their count
+    const int64_t grid =
+        std::max<int64_t>(1, std::min<int64_t>(c.its->Se, (int64_t)occ * c.its->sms));
+    RowSumArgs rs{};
+    rs.sum = out;
+    rs.small_part = c.small_part;
+    rs.small_rows = c.its->small_rows;
+    for (int k = 0; k < c.d.K; ++k)
+      if ((c.its->small_mask >> k) & 1u) {
+        rs.small_fe[rs.n_small] = k;
+        rs.small_off[rs.n_small] = c.its->small_off[k];
+        ++rs.n_small;
+      }
+    kern<<<(unsigned)grid, kThreads, smem, c.s>>>(c.d, c.its->d_dm.as<ExpandItem>(), n, rows, rows32,
+                                                  rs, c.part_e, c.its->Se);
+    FE_CK(cudaGetLastError());
+    if (c.its->small_rows > 0) {
+      SmallRows m{};
+      for (int r = 0; r < c.its->small_rows; ++r) m.slab_row[r] = c.its->small_slab_row[(size_t)r];
+      k_small_combine<T, C><<<(unsigned)c.its->small_rows, kThreads, 0, c.s>>>(
+          c.small_part, (int)grid, c.its->small_rows, m, out, c.d.active);
+      FE_CK(cudaGetLastError());
+    }
+    return 0;
+  } else {
+    (void)c;
+    (void)rows;
+    (void)rows32;
+    (void)out;
+    set_error_cstr("demean pass requested for a tile narrower than 32 columns");
+    return 1;
+  }
+}
+
+template <typename T, int C>
+static int launch_demean(Ctx& c, T* rows, float* rows32, T* out, const char* name, double bytes) {
+  ProfScope ps(c.pl, name, bytes);
+  const fe_plan* pl = c.pl;
+  bool w = false;
+  int ns = 0;
+  for (int k = 0; k < pl->K; ++k) {
+    const bool small = ((c.its->small_mask >> k) & 1u) != 0;
+    if (small) ++ns;
+    if ((small || k == pl->primary) && (pl->weighted || pl->interacted[k])) w = true;
+  }
+  switch (ns * 2 + (w ? 1 : 0)) {
+    case 0: return demean_launch<T, C, false, 0>(c, rows, rows32, out);
+    case 1: return demean_launch<T, C, true, 0>(c, rows, rows32, out);
+    case 2: return demean_launch<T, C, false, 1>(c, rows, rows32, out);
+    case 3: return demean_launch<T, C, true, 1>(c, rows, rows32, out);
+    case 4: return demean_launch<T, C, false, 2>(c, rows, rows32, out);
+    default: return demean_launch<T, C, true, 2>(c, rows, rows32, out);
+  }
+}
+
 template <typename TA, int C, int U, int S, class Load>
 static int launch_segsum_async(Ctx& c, Load ld, TA* out, const ReduceItem* items, int64_t n,
                                unsigned grid) {
@@ -334,9 +414,11 @@ static int launch_segsum_async(Ctx& c, Load ld, TA* out, const ReduceItem* items
 // large non-primary FEs; otherwise the segsum reduces every FE.
 template <typename TA, int C, class Load>
 static int launch_segsum(Ctx& c, Load ld, TA* out, const char* name, double bytes,
-                         bool rowsum = false, const char* rs_name = "rowsum", double rs_bytes = 0.0) {
+                         bool rowsum = false, const char* rs_name = "rowsum", double rs_bytes = 0.0,
+                         bool large_only = false) {
+  if (large_only) rowsum = true;  // the segsum part of the row-sum mode only
   if constexpr (!Load::kSquareWeight) {
-    if (rowsum) {
+    if (rowsum && !large_only) {
       ProfScope ps(c.pl, rs_name, rs_bytes);
       static_assert(std::is_same<typename Load::InType, TA>::value, "rows are summed in their type");
       const int st = launch_rowsum<TA, C>(c, ld.in, out);
@@ -381,9 +463,11 @@ template <int C, class Epi>
 static int launch_pupdate(Ctx& c, const typename Epi::TS* S, Epi epi, double* pa, double* pb,
                           const char* name, double bytes) {
   ProfScope ps(c.pl, name, bytes);
-  const unsigned grid = (unsigned)(c.its->pu.size() / kWarps);
+  // absorbed-primary mode: the non-primary levels only (the leading items)
+  const int64_t n = c.absorb ? c.its->pu_np : (int64_t)c.its->pu.size();
+  const unsigned grid = (unsigned)(n / kWarps);
   k_pupdate<C, Tune<C>::kPU, Epi><<<grid, kThreads, 0, c.s>>>(
-      c.d, c.its->d_pu.as<PItem>(), (int64_t)c.its->pu.size(), S, epi, pa, pb, c.its->Sp);
+      c.d, c.its->d_pu.as<PItem>(), n, S, epi, pa, pb, c.absorb ? c.its->Sp_np : c.its->Sp);
   FE_CK(cudaGetLastError());
   return 0;
 }
@@ -399,8 +483,8 @@ static int launch_scalar_phase(Ctx& c, int phase, int init_mode) {
   a.counters = c.counters;
   a.off0 = c.its->d_ex_off.as<int64_t>();
   a.S0 = c.its->Se;
-  a.off1 = c.its->d_pu_off.as<int64_t>();
-  a.S1 = c.its->Sp;
+  a.off1 = c.absorb ? c.its->d_pu_off_np.as<int64_t>() : c.its->d_pu_off.as<int64_t>();
+  a.S1 = c.absorb ? c.its->Sp_np : c.its->Sp;
   switch (phase) {
     case PH_INIT_BETA:
     case PH_BETA:
@@ -438,10 +522,22 @@ static bool use_rowsum(const fe_plan* pl, int C) {
   return pl->opt_fuse != 0 && C == 32 && pl->nprob == 1;
 }
 
+// Absorbed-primary mode of the mixed-precision residual solve (32-column
+// tiles of single-problem plans with 2+ FEs): the least-squares residual is
+// that of the problem with the primary FE projected out,
+//   min || M (b - A_r x_r) ||,  M u = u - sum_l a_l (a_l' u),
+// a_l the unit columns of the primary FE (contiguous row segments).  LSMR then
+// iterates over the other FEs' levels only, on a better-conditioned operator.
+static bool use_absorb(const fe_plan* pl, const ItemSet* its, int C) {
+  return pl->opt_absorb != 0 && C == 32 && pl->nprob == 1 && pl->K >= 2 && !its->dm.empty();
+}
+
 // algorithmic bytes per launch (the roofline numerators): every index vector
 // and observation row once, every coefficient-table row once
 struct Bytes {
   double expand, segsum, pupdate, resid64, segsum64, grad64, rowsum, rowsum64;
+  // absorbed-primary mode
+  double expand_abs, resid64_abs, demean, demean64, pupdate_np, grad64_np;
 };
 static Bytes alg_bytes(const fe_plan* pl, const ItemSet* its, int C, int sT) {
   Bytes b{};
@@ -486,6 +582,28 @@ static Bytes alg_bytes(const fe_plan* pl, const ItemSet* its, int C, int sT) {
   b.segsum = posmeta + cwp + pos * C * sT + (P - Pf) * C * sT;
   b.rowsum = rowsum;
   b.rowsum64 = rowsum64;
+  {
+    // absorbed-primary mode: the expand leaves out the primary FE; the demean
+    // pass reads the primary (and small-FE) keys, reads and writes the rows
+    // and writes one z row per primary level; the P side covers the other FEs
+    const int kp = pl->primary;
+    const bool cwp = pl->weighted || pl->interacted[kp];
+    const double Pp = (double)pl->nlev[kp], Pnp = P - Pp;
+    double keys = N * (4.0 + (cwp ? sT : 0)), keys64 = N * (4.0 + (cwp ? 8.0 : 0.0));
+    for (int k = 0; k < pl->K; ++k)
+      if ((its->small_mask >> k) & 1u) {
+        const bool hc = pl->weighted || pl->interacted[k];
+        keys += N * (4.0 + (hc ? sT : 0));
+        keys64 += N * (4.0 + (hc ? 8.0 : 0.0));
+      }
+    const double cwnp = cw - (cwp ? N * sT : 0.0), cwnp64 = cw64 - (cwp ? N * 8.0 : 0.0);
+    b.expand_abs = N * 4.0 * (pl->K - 1) + cwnp + 2.0 * N * C * sT + Pnp * C * sT;
+    b.resid64_abs = N * 4.0 * (pl->K - 1) + cwnp64 + N * C * 16.0 + Pnp * C * 12.0;
+    b.demean = keys + 2.0 * N * C * sT + Pp * C * sT;
+    b.demean64 = keys64 + 2.0 * N * C * 8.0 + N * C * 4.0 + Pp * C * 8.0;
+    b.pupdate_np = 9.0 * Pnp * C * sT;
+    b.grad64_np = Pnp * C * (8.0 + 4.0 + 8.0 + 4.0 + 8.0);
+  }
   b.pupdate = 9.0 * P * C * sT;
   b.resid64 = refs + cw64 + N * C * (8.0 + 8.0 + 4.0) + P * C * 12.0;
   b.segsum64 = posmeta + cwp64 + pos * C * 8.0 + (P - Pf) * C * 8.0;
@@ -643,6 +761,7 @@ static int run_loop(fe_plan* pl, Ctx& c, int prec, int64_t cap, int32_t nact0, B
       key = key * 31 + (size_t)pick_ex(pl, e) * 7 + (size_t)pick_seg(pl, e);
     key = key * 3 + (c.rowsum ? 1u : 0u);
     key = key * 5 + (size_t)(pl->opt_rowsum_variant + 1);
+    key = key * 3 + (c.absorb ? 1u : 0u);
     lg = &pl->graphs[{c.C, prec}];
     if (!lg->exec || lg->key != key) {
       if (lg->exec) {
@@ -938,7 +1057,12 @@ static int solve_mixed_tile(fe_plan* pl, const SolveReq& rq, int64_t col0, int n
   double* R64 = w.R64.as<double>();
   double* S64 = static_cast<double*>(c.S);
   float* S32 = static_cast<float*>(c.S);
-  if (rq.residuals && pl->opt_mixed_warm) {
+  // absorbed-primary mode (residual solves): LSMR over the other FEs, from
+  // x0 = 0 (the reference's warm start A'b belongs to the full problem)
+  const bool absorb = rq.residuals && use_absorb(pl, c.its, C);
+  c.absorb = absorb;
+  c.d.absorb = absorb ? 1 : 0;
+  if (rq.residuals && pl->opt_mixed_warm && !absorb) {
     if ((st = launch_segsum<double, C>(c, LoadIn<double, double, vec_of<double, C>()>{B64}, S64, "segsum_warm", 0.0,
                                         c.rowsum, "rowsum_warm", 0.0)))
       return st;
@@ -964,23 +1088,47 @@ static int solve_mixed_tile(fe_plan* pl, const SolveReq& rq, int64_t col0, int n
   int64_t total_it = 0;
   const bool fuse = c.rowsum;
   for (int round = 0; round <= pl->opt_max_rounds + 1; ++round) {
-    FE_CK(cudaMemsetAsync(c.counters, 0, 2 * sizeof(int32_t), c.s));
+    FE_CK(cudaMemsetAsync(c.counters, 0, 3 * sizeof(int32_t), c.s));
     // r = b - A (x64 + dx32) in FP64, with the FP32 copy as the next inner u
-    if ((st = launch_expand<double, C>(c, TabSum64<vec_of<double, C>()>{X64, X},
-                                       EpiBminusAx<double, double, vec_of<double, C>()>{B64, R64, U, c.inst, 2},
-                                       c.part_e, "resid64", by.resid64)))
+    // (absorbed: r = M (b - A_r x), projected and copied by the demean pass)
+    if ((st = launch_expand<double, C>(
+             c, TabSum64<vec_of<double, C>()>{X64, X},
+             EpiBminusAx<double, double, vec_of<double, C>()>{B64, R64, absorb ? nullptr : U, c.inst, 2},
+             absorb ? nullptr : c.part_e, "resid64", absorb ? by.resid64_abs : by.resid64)))
       return st;
     // g = A'r in FP64 (the next inner v), x64 += dx32, ||x64||
-    if ((st = launch_segsum<double, C>(c, LoadIn<double, double, vec_of<double, C>()>{R64}, S64, "segsum64",
-                                       by.segsum64, fuse, "rowsum64", by.rowsum64)))
+    if (absorb) {
+      if ((st = launch_demean<double, C>(c, R64, U, S64, "demean64", by.demean64))) return st;
+      if ((st = launch_segsum<double, C>(c, LoadIn<double, double, vec_of<double, C>()>{R64}, S64,
+                                         "segsum64", by.segsum64, true, "", 0.0, true)))
+        return st;
+    } else if ((st = launch_segsum<double, C>(c, LoadIn<double, double, vec_of<double, C>()>{R64}, S64,
+                                              "segsum64", by.segsum64, fuse, "rowsum64", by.rowsum64))) {
       return st;
-    if ((st = launch_pupdate<C>(c, S64, pg, c.part_a, c.part_b, "grad64", by.grad64))) return st;
+    }
+    if ((st = launch_pupdate<C>(c, S64, pg, c.part_a, c.part_b, "grad64",
+                                absorb ? by.grad64_np : by.grad64)))
+      return st;
     if ((st = launch_scalar_phase(c, PH_OUTER, 0))) return st;
     int32_t nout = 0;
     if ((st = read_counter(c, 1, &nout))) return st;
     if (nout == 0) break;
     auto body = [&]() -> int {
       int e;
+      if (absorb) {
+        // u = M (av A_r v + au u): the expand without the primary FE, then the
+        // projection (which also gives ||u|| and the small FEs' sums)
+        if ((e = launch_expand<float, C>(c, TabOne<float, float, vec_of<float, C>()>{V}, ee, nullptr,
+                                         "expand", by.expand_abs)))
+          return e;
+        if ((e = launch_demean<float, C>(c, U, nullptr, S32, "demean", by.demean))) return e;
+        if ((e = launch_scalar_phase(c, PH_BETA, 0))) return e;
+        if ((e = launch_segsum<float, C>(c, LoadIn<float, float, vec_of<float, C>()>{U}, S32, "segsum",
+                                         by.segsum, true, "", 0.0, true)))
+          return e;
+        if ((e = launch_pupdate<C>(c, S32, pe, c.part_a, c.part_b, "pupdate", by.pupdate_np))) return e;
+        return launch_scalar_phase(c, PH_ALPHA, 0);
+      }
       if ((e = launch_expand<float, C>(c, TabOne<float, float, vec_of<float, C>()>{V}, ee, c.part_e,
                                        "expand", by.expand)))
         return e;

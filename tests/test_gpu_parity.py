@@ -381,3 +381,40 @@ def test_graph_replay_matches_direct_launches(fe, synth, prec):
         assert cvs.all() and np.array_equal(R, R2) and np.array_equal(its, its2)
         out.append((R, its))
     assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
+
+
+@pytest.mark.parametrize("case", ["weighted4", "two_fe_small", "unweighted3"])
+def test_absorbed_primary_matches_oracle(fe, oracle, case):
+    # mixed residual solves of a 32-column tile with the primary FE projected
+    # out (FE_OPT_ABSORB, the default) against the oracle's full LSMR and the
+    # non-absorbed path; bitwise identical across two calls
+    rng = np.random.default_rng(21)
+    N = 60_000
+    r1 = rng.integers(1, 5001, N)
+    r1[rng.random(N) < 0.2] = 7  # one long primary level
+    r2 = rng.integers(1, 801, N)  # large FE: gathered by the segsum
+    r3 = rng.integers(1, 21, N)   # small FEs: shared-memory tables
+    r4 = rng.integers(1, 5, N)
+    if case == "weighted4":
+        refs, inter, w = [r1, r2, r3, r4], [None, None, rng.uniform(0.5, 1.5, N), None], rng.uniform(0.5, 1.5, N)
+    elif case == "two_fe_small":
+        refs, inter, w = [r1, r3], [None, None], None
+    else:
+        refs, inter, w = [r1, r2, r3], [None, None, None], None
+    Y = np.asfortranarray(rng.standard_normal((N, 5)))
+    R_o, _, _ = oracle.solve_residuals_cols(Y, refs, None, inter, w, tol=1e-8)
+    fes = [fe.FixedEffect(r, interaction=a) for r, a in zip(refs, inter)]
+    out = []
+    for absorb in (1, 0):
+        feM = fe.AbstractFixedEffectSolver(fes, w, "CUDA", np.float64, precision="mixed")
+        feM.set_option(fe._lib.FE_OPT_TILE, 32)
+        feM.set_option(fe._lib.FE_OPT_ABSORB, absorb)
+        R, its, cvs = feM.solve_residuals(Y.copy(), tol=1e-8)
+        R2, its2, _ = feM.solve_residuals(Y.copy(), tol=1e-8)
+        feM.close()
+        assert cvs.all(), (absorb, its)
+        assert np.array_equal(R, R2) and np.array_equal(its, its2)
+        err = max(rel_err(R[:, j], R_o[:, j]) for j in range(Y.shape[1]))
+        assert err < REL, (absorb, err)
+        out.append(R)
+    assert max(rel_err(out[0][:, j], out[1][:, j]) for j in range(Y.shape[1])) < REL
