@@ -953,18 +953,22 @@ k_rowsum_reg(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_item
 // written by all lanes in pass 1 and read in pass 2 after a __syncwarp.
 // ---------------------------------------------------------------------------
 template <typename T, int C, bool W, int NS>
-__global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 3 : 2)
+__global__ void __launch_bounds__(kThreads, 2)
 k_demean(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_items,
          T* __restrict__ rows, float* __restrict__ rows32, RowSumArgs rs,
          double* __restrict__ part, int64_t S) {
   static_assert(C == 32, "one column per lane");
   constexpr int STEP = sizeof(T) == 4 ? 16 : 8;
+  constexpr int RC = (int)kDemeanRows;  // rows of an item held in registers
+  static_assert(RC == 32, "one item row per lane for the keys");
   __shared__ double sm[kWarps][32];
   extern __shared__ __align__(16) unsigned char demean_smem[];
   if (d.active && *d.active == 0) return;  // the whole CTA
   const int lane = threadIdx.x & 31;
   const int wib = threadIdx.x >> 5;
-  T* tbl = reinterpret_cast<T*>(demean_smem) + (size_t)wib * rs.small_rows * C;
+  // per warp: RC z rows (levels of a short item), then the small-FE table
+  T* zs = reinterpret_cast<T*>(demean_smem) + (size_t)wib * (RC + rs.small_rows) * C;
+  T* tbl = zs + RC * C;
   for (int e = lane; e < rs.small_rows * C; e += 32) tbl[e] = T(0);
   __syncwarp();
   const int kp = d.primary;
@@ -983,7 +987,80 @@ k_demean(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_items,
     const ExpandItem it = items[wi];
     const int64_t ie = it.ie;
     if (ie <= it.ib) continue;
-    // pass 1: z_l = sum cw u over each level of the item
+    if (ie - it.ib <= RC) {
+      // ---- short item: rows in registers, z rows in shared memory ----
+      const int n = (int)(ie - it.ib);
+      const bool okl = lane < n;
+      const int64_t p = it.ib + lane;
+      const int kpr = okl ? __ldg(refp + p) : kSentinel;
+      const T cwv = (W && okl && cwp) ? __ldg(cwp + p) : T(1);
+      T f = T(0);  // cw_i scale_l^2 of row ib + lane
+      if (okl) {
+        const T sl = __ldg(scp + kpr);
+        f = sl * sl * cwv;
+      }
+      int k0 = 0, k1 = 0;
+      T c0 = T(1), c1 = T(1);
+      if (NS > 0 && okl) {
+        k0 = off0 + __ldg(ref0 + p);
+        if (W && cw0) c0 = __ldg(cw0 + p);
+      }
+      if (NS > 1 && okl) {
+        k1 = off1 + __ldg(ref1 + p);
+        if (W && cw1) c1 = __ldg(cw1 + p);
+      }
+      T x[RC];
+      const T* __restrict__ src = rows + it.ib * C + lane;
+#pragma unroll
+      for (int r = 0; r < RC; ++r) x[r] = r < n ? src[(int64_t)r * C] : T(0);
+      const int kn = __shfl_down_sync(FE_FULL, kpr, 1);
+      // level ends after row r: a key change, or the item's last row
+      const uint32_t ends = __ballot_sync(FE_FULL, okl && (lane + 1 == n || kn != kpr));
+      // pass 1: z of each level of the item, in level order
+      T acc = T(0);
+      int li = 0;
+#pragma unroll
+      for (int r = 0; r < RC; ++r) {
+        if (r < n) {  // warp-uniform
+          acc += W ? x[r] * __shfl_sync(FE_FULL, cwv, r) : x[r];
+          if ((ends >> r) & 1u) {
+            zs[li * C + lane] = acc;
+            acc = T(0);
+            ++li;
+          }
+        }
+      }
+      __syncwarp();
+      // pass 2: u -= cw scale^2 z, stored, ||u||^2; padded rows stay 0
+      T* __restrict__ dst = rows + it.ib * C + lane;
+      li = 0;
+#pragma unroll
+      for (int r = 0; r < RC; ++r) {
+        if (r < n) {
+          const T u = x[r] - __shfl_sync(FE_FULL, f, r) * zs[li * C + lane];
+          dst[(int64_t)r * C] = u;
+          if (rows32) rows32[(it.ib + r) * C + lane] = (float)u;
+          nrm += (double)u * (double)u;
+          x[r] = u;
+          if ((ends >> r) & 1u) ++li;
+        }
+      }
+      __syncwarp();  // zs is rewritten by the next item
+      // small FEs: tables += cw u, 4 rows at a time (padded rows add 0)
+      if (NS > 0) {
+#pragma unroll
+        for (int r0 = 0; r0 < RC; r0 += 4) {
+          if (r0 < n) {
+            rowsum_small4<T, C, W>(r0, x[r0], x[r0 + 1], x[r0 + 2], x[r0 + 3], k0, c0, tbl, lane);
+            if (NS > 1)
+              rowsum_small4<T, C, W>(r0, x[r0], x[r0 + 1], x[r0 + 2], x[r0 + 3], k1, c1, tbl, lane);
+          }
+        }
+      }
+      continue;
+    }
+    // ---- long item (one level longer than RC rows): two passes over memory ----
+    // pass 1: z_l = sum cw u over the level
     int ckey = -1;
     T acc = T(0);
     for (int64_t base = it.ib; base < ie; base += STEP) {
@@ -1046,24 +1123,12 @@ k_demean(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_items,
         }
       }
       if (NS > 0) {
-        if (nvalid == STEP) {
 #pragma unroll
-          for (int r0 = 0; r0 < STEP; r0 += 4) {
+        for (int r0 = 0; r0 < STEP; r0 += 4) {
+          if (r0 < nvalid) {
             rowsum_small4<T, C, W>(r0, x[r0], x[r0 + 1], x[r0 + 2], x[r0 + 3], k0, c0, tbl, lane);
             if (NS > 1)
               rowsum_small4<T, C, W>(r0, x[r0], x[r0 + 1], x[r0 + 2], x[r0 + 3], k1, c1, tbl, lane);
-          }
-        } else {
-#pragma unroll
-          for (int r = 0; r < STEP; ++r) {
-            if (r < nvalid) {
-              const int t0 = __shfl_sync(FE_FULL, k0, r);
-              tbl[t0 * C + lane] += W ? x[r] * __shfl_sync(FE_FULL, c0, r) : x[r];
-              if (NS > 1) {
-                const int t1 = __shfl_sync(FE_FULL, k1, r);
-                tbl[t1 * C + lane] += W ? x[r] * __shfl_sync(FE_FULL, c1, r) : x[r];
-              }
-            }
           }
         }
       }
@@ -1083,11 +1148,12 @@ k_demean(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_items,
   if (NS > 0) {
     const int n = rs.small_rows * C;
     double* __restrict__ out = rs.small_part + (int64_t)blockIdx.x * n;
-    const T* t0 = reinterpret_cast<const T*>(demean_smem);
+    const T* t0 = reinterpret_cast<const T*>(demean_smem) + (size_t)kDemeanRows * C;
+    const size_t wstep = (size_t)(kDemeanRows + rs.small_rows) * C;
     for (int e = threadIdx.x; e < n; e += kThreads) {
       double t = 0.0;
 #pragma unroll
-      for (int w = 0; w < kWarps; ++w) t += (double)t0[(size_t)w * n + e];
+      for (int w = 0; w < kWarps; ++w) t += (double)t0[(size_t)w * wstep + e];
       out[e] = t;
     }
   }

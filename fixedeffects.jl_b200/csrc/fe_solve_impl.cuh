@@ -322,13 +322,13 @@ template <typename T, int C, bool W, int NS>
 static int demean_launch(Ctx& c, T* rows, float* rows32, T* out) {
   if constexpr (C == 32) {
     auto kern = k_demean<T, C, W, NS>;
-    const size_t smem = (size_t)kWarps * c.its->small_rows * C * sizeof(T);
+    const size_t smem = (size_t)kWarps * (kDemeanRows + c.its->small_rows) * C * sizeof(T);
     static bool attr_set = false;  // per instantiation
     static size_t occ_smem = (size_t)-1;
     static int occ = 1;
     if (!attr_set) {
       FE_CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)(kWarps * kSmallRows * C * sizeof(T))));
+                                 (int)(kWarps * (kDemeanRows + kSmallRows) * C * sizeof(T))));
       attr_set = true;
     }
     if (occ_smem != smem) {
@@ -584,8 +584,9 @@ static Bytes alg_bytes(const fe_plan* pl, const ItemSet* its, int C, int sT) {
   b.rowsum64 = rowsum64;
   {
     // absorbed-primary mode: the expand leaves out the primary FE; the demean
-    // pass reads the primary (and small-FE) keys, reads and writes the rows
-    // and writes one z row per primary level; the P side covers the other FEs
+    // pass reads the primary (and small-FE) keys and scales and reads and
+    // writes the rows once (z rows stay on chip except for levels longer than
+    // kDemeanRows); the P side covers the other FEs
     const int kp = pl->primary;
     const bool cwp = pl->weighted || pl->interacted[kp];
     const double Pp = (double)pl->nlev[kp], Pnp = P - Pp;
@@ -599,8 +600,8 @@ static Bytes alg_bytes(const fe_plan* pl, const ItemSet* its, int C, int sT) {
     const double cwnp = cw - (cwp ? N * sT : 0.0), cwnp64 = cw64 - (cwp ? N * 8.0 : 0.0);
     b.expand_abs = N * 4.0 * (pl->K - 1) + cwnp + 2.0 * N * C * sT + Pnp * C * sT;
     b.resid64_abs = N * 4.0 * (pl->K - 1) + cwnp64 + N * C * 16.0 + Pnp * C * 12.0;
-    b.demean = keys + 2.0 * N * C * sT + Pp * C * sT;
-    b.demean64 = keys64 + 2.0 * N * C * 8.0 + N * C * 4.0 + Pp * C * 8.0;
+    b.demean = keys + 2.0 * N * C * sT + Pp * sT;
+    b.demean64 = keys64 + 2.0 * N * C * 8.0 + N * C * 4.0 + Pp * 8.0;
     b.pupdate_np = 9.0 * Pnp * C * sT;
     b.grad64_np = Pnp * C * (8.0 + 4.0 + 8.0 + 4.0 + 8.0);
   }
