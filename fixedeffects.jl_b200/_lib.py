@@ -37,6 +37,7 @@ FE_OPT_MIXED_WARM_START = 10
 FE_OPT_GRAPH = 11
 FE_OPT_ROWSUM_VARIANT = 12
 FE_OPT_ABSORB = 14
+FE_OPT_FUSED_DEMEAN = 15
 
 # every symbol declared in include/fe_b200.h
 EXPORTS = (

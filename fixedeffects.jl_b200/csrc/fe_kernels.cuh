@@ -1159,6 +1159,282 @@ k_demean(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_items,
   }
 }
 
+// ---------------------------------------------------------------------------
+// k_expand_demean: the expand and the demean of the absorbed-primary mode in
+// one pass over the rows (32-column tiles).  Per demean item (whole primary
+// levels, at most kDemeanRows rows):
+//   phase A: the new rows without the primary FE, in the expand's lane layout
+//            (Shape<T, 32>):  LSMR   w = av * (A_r v) + au * u_old
+//                             RESID  w = b - A_r x            (FP64)
+//            staged in a per-warp shared buffer;
+//   phase B: one column per lane: the level sums z_l = sum cw w, then
+//            u = w - cw scale_l^2 z_l stored once (LSMR: u in place; RESID:
+//            the FP64 residual and its FP32 copy), ||u||^2 per column into
+//            the CTA's norm slot, and the small FEs' sums of cw u into the
+//            per-warp tables (as k_rowsum).
+// A level longer than kDemeanRows rows is processed in chunks: phase A writes
+// w to the row buffer and accumulates z, then a second walk finalizes it.
+// RESID, mask: columns whose refinement has stopped keep their stored rows.
+// ---------------------------------------------------------------------------
+template <typename T, int VEC>
+struct ExDmCoef {
+  T av[VEC], au[VEC];
+  bool act[VEC];  // the column's rows may be written
+};
+
+template <typename T, int C, int U, int KB, bool RESID, bool W, int NS, class Tab>
+__global__ void __launch_bounds__(kThreads, 2)
+k_expand_demean(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_items, Tab tab,
+                T* __restrict__ rows, const double* __restrict__ B, float* __restrict__ rows32,
+                const Inst* __restrict__ inst, int mask, RowSumArgs rs,
+                double* __restrict__ part, int64_t S) {
+  static_assert(C == 32, "one column per lane in phase B");
+  using Sh = Shape<T, C>;
+  constexpr int VEC = Sh::VEC, CL = Sh::CL, G = Sh::G;
+  constexpr int STEP = G * U;
+  constexpr int RC = (int)kDemeanRows;
+  static_assert(STEP <= 32 && RC % STEP == 0, "steps tile an item's row buffer");
+  __shared__ double sm[kWarps][32];
+  extern __shared__ __align__(16) unsigned char exdm_smem[];
+  if (d.active && *d.active == 0) return;  // the whole CTA
+  const int lane = threadIdx.x & 31;
+  const int wib = threadIdx.x >> 5;
+  const int g = lane / CL, jl = lane - g * CL;
+  const size_t wstride_smem = (size_t)(2 * RC + rs.small_rows) * C;
+  T* ub = reinterpret_cast<T*>(exdm_smem) + (size_t)wib * wstride_smem;  // staged rows
+  T* zs = ub + RC * C;                                                   // level sums
+  T* tbl = zs + RC * C;                                                  // small-FE table
+  for (int e = lane; e < rs.small_rows * C; e += 32) tbl[e] = T(0);
+  const int K = d.K;
+  const int kp = d.primary;
+  const int32_t* __restrict__ refp = d.refs[kp];
+  const T* __restrict__ cwp = cw_of<T>(d, kp);
+  const T* __restrict__ scp = scale_of<T>(d, kp);
+  const int32_t* __restrict__ ref0 = NS > 0 ? d.refs[rs.small_fe[0]] : nullptr;
+  const int32_t* __restrict__ ref1 = NS > 1 ? d.refs[rs.small_fe[1]] : nullptr;
+  const T* __restrict__ cw0 = NS > 0 ? cw_of<T>(d, rs.small_fe[0]) : nullptr;
+  const T* __restrict__ cw1 = NS > 1 ? cw_of<T>(d, rs.small_fe[1]) : nullptr;
+  const int off0 = rs.small_off[0], off1 = rs.small_off[1];
+  // per-column coefficients (phase A, lane group layout) and activity (phase B)
+  ExDmCoef<T, VEC> cf;
+  bool act_any = false;
+#pragma unroll
+  for (int v = 0; v < VEC; ++v) {
+    const Inst& st = inst[jl * VEC + v];
+    cf.av[v] = (T)st.ex_av;
+    cf.au[v] = (T)st.ex_au;
+    cf.act[v] = RESID ? (mask != 2 || st.outer_active != 0) : true;
+    act_any = act_any || (RESID ? cf.act[v] : st.active != 0);
+  }
+  const bool col_act = RESID ? (mask != 2 || inst[lane].outer_active != 0) : inst[lane].active != 0;
+  act_any = __any_sync(FE_FULL, act_any);
+  double nrm = 0.0;
+  __syncwarp();
+
+  // phase A on rows [cb, cb + cn) (cn <= RC): w rows into ub (and, for a
+  // chunk of a long level, into the row buffer)
+  auto phase_a = [&](int64_t cb, int cn, bool to_global) {
+    for (int b0 = 0; b0 < cn; b0 += STEP) {
+      const int64_t base = cb + b0;
+      int rl[KB];
+      T cl[KB];
+#pragma unroll
+      for (int k = 0; k < KB; ++k) {
+        const bool ok = k < K && k != kp && lane < STEP && b0 + lane < cn;
+        rl[k] = ok ? __ldg(d.refs[k] + base + lane) : 0;
+        const T* __restrict__ cw = cw_of<T>(d, k < K ? k : 0);
+        cl[k] = (ok && cw) ? __ldg(cw + base + lane) : T(1);
+      }
+      VA<T, VEC> old[U];
+      VA<T, VEC> sacc[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int r = b0 + u * G + g;
+#pragma unroll
+        for (int v = 0; v < VEC; ++v) sacc[u].v[v] = T(0);
+        if (r < cn) {
+          const int64_t o = (cb + r) * C + jl * VEC;
+          if (RESID) {
+            const VA<double, VEC> bb = vldg<double, VEC>(B + o);
+#pragma unroll
+            for (int v = 0; v < VEC; ++v) old[u].v[v] = (T)bb.v[v];
+          } else {
+            old[u] = vld<T, VEC>(rows + o);
+          }
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < KB; ++k) {
+        if (k < K && k != kp) {
+          const T* __restrict__ sc = scale_of<T>(d, k);
+          const int64_t lb = d.lev_base[k];
+          const bool wk = cw_of<T>(d, k) != nullptr;
+#pragma unroll
+          for (int u = 0; u < U; ++u) {
+            const int q = u * G + g;
+            const int ref = __shfl_sync(FE_FULL, rl[k], q);
+            const T c = wk ? __shfl_sync(FE_FULL, cl[k], q) : T(1);
+            if (b0 + q < cn) {
+              const T scl = __ldg(sc + ref);
+              const T cs = wk ? c * scl : scl;
+              const VA<T, VEC> t = tab.load((lb + ref) * C + jl * VEC);
+#pragma unroll
+              for (int v = 0; v < VEC; ++v) sacc[u].v[v] += cs * t.v[v];
+            }
+          }
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int r = b0 + u * G + g;
+        if (r < cn) {
+          VA<T, VEC> w;
+#pragma unroll
+          for (int v = 0; v < VEC; ++v)
+            w.v[v] = RESID ? old[u].v[v] - sacc[u].v[v] : cf.av[v] * sacc[u].v[v] + cf.au[v] * old[u].v[v];
+          vst<T, VEC>(ub + r * C + jl * VEC, w);
+          if (to_global) {
+#pragma unroll
+            for (int v = 0; v < VEC; ++v)
+              if (cf.act[v]) rows[(cb + r) * C + jl * VEC + v] = w.v[v];
+          }
+        }
+      }
+    }
+    __syncwarp();
+  };
+  // per-row data of rows [cb, cb + cn), one row per lane
+  struct RowData {
+    int kpr, k0, k1;
+    T cwv, f, c0, c1;
+  };
+  auto row_data = [&](int64_t cb, int cn) {
+    RowData rd;
+    const bool okl = lane < cn;
+    const int64_t p = cb + lane;
+    rd.kpr = okl ? __ldg(refp + p) : kSentinel;
+    rd.cwv = (W && okl && cwp) ? __ldg(cwp + p) : T(1);
+    rd.f = T(0);
+    if (okl) {
+      const T sl = __ldg(scp + rd.kpr);
+      rd.f = sl * sl * rd.cwv;
+    }
+    rd.k0 = 0;
+    rd.k1 = 0;
+    rd.c0 = T(1);
+    rd.c1 = T(1);
+    if (NS > 0 && okl) {
+      rd.k0 = off0 + __ldg(ref0 + p);
+      if (W && cw0) rd.c0 = __ldg(cw0 + p);
+    }
+    if (NS > 1 && okl) {
+      rd.k1 = off1 + __ldg(ref1 + p);
+      if (W && cw1) rd.c1 = __ldg(cw1 + p);
+    }
+    return rd;
+  };
+  // finalize rows [cb, cb + cn) whose w is in ub: u = w - f z (z of row r's
+  // level: zrow(r)), stored, norms, small-FE tables
+  auto finalize = [&](int64_t cb, int cn, const RowData& rd, uint32_t ends, bool zs_local, T zlong) {
+    int li = 0;
+#pragma unroll 8
+    for (int r = 0; r < cn; ++r) {
+      const T z = zs_local ? zs[li * C + lane] : zlong;
+      const T u = ub[r * C + lane] - __shfl_sync(FE_FULL, rd.f, r) * z;
+      ub[r * C + lane] = u;
+      if (col_act) {
+        const int64_t o = (cb + r) * C + lane;
+        rows[o] = u;
+        if (RESID && rows32) rows32[o] = (float)u;
+        nrm += (double)u * (double)u;
+      }
+      if ((ends >> r) & 1u) ++li;
+    }
+    if (NS > 0) {
+      for (int r0 = 0; r0 < cn; r0 += 4) {
+        T x0 = ub[r0 * C + lane];
+        T x1 = r0 + 1 < cn ? ub[(r0 + 1) * C + lane] : T(0);
+        T x2 = r0 + 2 < cn ? ub[(r0 + 2) * C + lane] : T(0);
+        T x3 = r0 + 3 < cn ? ub[(r0 + 3) * C + lane] : T(0);
+        rowsum_small4<T, C, W>(r0, x0, x1, x2, x3, rd.k0, rd.c0, tbl, lane);
+        if (NS > 1) rowsum_small4<T, C, W>(r0, x0, x1, x2, x3, rd.k1, rd.c1, tbl, lane);
+      }
+    }
+    __syncwarp();  // ub and zs are rewritten next
+  };
+
+  const int64_t wstride = (int64_t)gridDim.x * kWarps;
+  for (int64_t wi = (int64_t)blockIdx.x * kWarps + wib; wi < n_items; wi += wstride) {
+    const ExpandItem it = items[wi];
+    const int64_t ie = it.ie;
+    if (ie <= it.ib || !act_any) continue;
+    if (ie - it.ib <= RC) {
+      const int n = (int)(ie - it.ib);
+      phase_a(it.ib, n, false);
+      const RowData rd = row_data(it.ib, n);
+      const int kn = __shfl_down_sync(FE_FULL, rd.kpr, 1);
+      const uint32_t ends = __ballot_sync(FE_FULL, lane < n && (lane + 1 == n || kn != rd.kpr));
+      // level sums in level order
+      T acc = T(0);
+      int li = 0;
+#pragma unroll 8
+      for (int r = 0; r < n; ++r) {
+        const T w = ub[r * C + lane];
+        acc += W ? w * __shfl_sync(FE_FULL, rd.cwv, r) : w;
+        if ((ends >> r) & 1u) {
+          zs[li * C + lane] = acc;
+          acc = T(0);
+          ++li;
+        }
+      }
+      __syncwarp();
+      finalize(it.ib, n, rd, ends, true, T(0));
+      continue;
+    }
+    // one level longer than RC rows: w through the row buffer, then finalize
+    T zl = T(0);
+    for (int64_t cb = it.ib; cb < ie; cb += RC) {
+      const int cn = (int)((ie - cb) < RC ? (ie - cb) : RC);
+      phase_a(cb, cn, true);
+      const T cwr = (W && lane < cn && cwp) ? __ldg(cwp + cb + lane) : T(1);
+      for (int r = 0; r < cn; ++r) {
+        const T w = ub[r * C + lane];
+        zl += W ? w * __shfl_sync(FE_FULL, cwr, r) : w;
+      }
+      __syncwarp();
+    }
+    for (int64_t cb = it.ib; cb < ie; cb += RC) {
+      const int cn = (int)((ie - cb) < RC ? (ie - cb) : RC);
+      for (int r = 0; r < cn; ++r) ub[r * C + lane] = rows[(cb + r) * C + lane];
+      __syncwarp();
+      const RowData rd = row_data(cb, cn);
+      finalize(cb, cn, rd, 0u, false, zl);
+    }
+  }
+  // ||u||^2: warp -> CTA slot (fixed order); slots beyond the grid hold 0
+  sm[wib][lane] = nrm;
+  __syncthreads();
+  if (part != nullptr && threadIdx.x < C) {
+    double t = 0.0;
+#pragma unroll
+    for (int w = 0; w < kWarps; ++w) t += sm[w][threadIdx.x];
+    part[(int64_t)threadIdx.x * S + blockIdx.x] = t;
+    for (int64_t sl = (int64_t)blockIdx.x + gridDim.x; sl < S; sl += gridDim.x)
+      part[(int64_t)threadIdx.x * S + sl] = 0.0;
+  }
+  if (NS > 0) {
+    const int n = rs.small_rows * C;
+    double* __restrict__ out = rs.small_part + (int64_t)blockIdx.x * n;
+    const T* t0 = reinterpret_cast<const T*>(exdm_smem) + (size_t)2 * RC * C;
+    for (int e = threadIdx.x; e < n; e += kThreads) {
+      double t = 0.0;
+#pragma unroll
+      for (int w = 0; w < kWarps; ++w) t += (double)t0[(size_t)w * wstride_smem + e];
+      out[e] = t;
+    }
+  }
+}
+
 // Small-FE level sums = the row-sum CTA partials summed in CTA order.  One
 // CTA per table row; thread t sums the slots q, q + Q, ... of column t % C
 // (Q = kThreads / C groups), and the groups are added in group order.

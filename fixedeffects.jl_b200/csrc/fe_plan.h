@@ -144,6 +144,7 @@ struct fe_plan {
   int32_t opt_graph = 1;        // replay the LSMR iterations from a CUDA graph
   int32_t opt_rowsum_variant = -1; // row-sum pass: 0 shared-memory ring, 1 registers
   int32_t opt_absorb = 1;       // mixed residual solves project the primary FE out
+  int32_t opt_exdm = 1;         // absorbed loop: fused expand + demean kernel
   std::map<std::pair<int, int>, fe::LoopGraph> graphs;  // by (C, precision)
   // tuned variants per (tile width C, element size): {expand, segsum}
   std::map<std::pair<int, int>, std::pair<int, int>> tuned;

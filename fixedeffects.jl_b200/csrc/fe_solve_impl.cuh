@@ -393,6 +393,103 @@ static int launch_demean(Ctx& c, T* rows, float* rows32, T* out, const char* nam
   }
 }
 
+// The fused expand + demean of the absorbed-primary loop (k_expand_demean):
+// u = M (av A_r v + au u), in place on rows, ||u||^2 to the expand norm slots,
+// small-FE sums to the slab (through the CTA partials).
+template <typename T, int C, int U, int KB, bool W, int NS, class Tab>
+static int exdm_launch(Ctx& c, Tab tab, T* rows) {
+  if constexpr (C == 32) {
+    auto kern = k_expand_demean<T, C, U, KB, false, W, NS, Tab>;
+    const size_t smem = (size_t)kWarps * (2 * kDemeanRows + c.its->small_rows) * C * sizeof(T);
+    static bool attr_set = false;  // per instantiation
+    static size_t occ_smem = (size_t)-1;
+    static int occ = 1;
+    if (!attr_set) {
+      FE_CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)(kWarps * (2 * kDemeanRows + kSmallRows) * C * sizeof(T))));
+      attr_set = true;
+    }
+    if (occ_smem != smem) {
+      int o = 0;
+      FE_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, kern, kThreads, smem));
+      occ = std::max(o, 1);
+      occ_smem = smem;
+    }
+    const int64_t n = (int64_t)c.its->dm.size();
+    const int64_t grid =
+        std::max<int64_t>(1, std::min<int64_t>(c.its->Se, (int64_t)occ * c.its->sms));
+    RowSumArgs rs{};
+    rs.sum = c.S;
+    rs.small_part = c.small_part;
+    rs.small_rows = c.its->small_rows;
+    for (int k = 0; k < c.d.K; ++k)
+      if ((c.its->small_mask >> k) & 1u) {
+        rs.small_fe[rs.n_small] = k;
+        rs.small_off[rs.n_small] = c.its->small_off[k];
+        ++rs.n_small;
+      }
+    kern<<<(unsigned)grid, kThreads, smem, c.s>>>(c.d, c.its->d_dm.as<ExpandItem>(), n, tab, rows,
+                                                  nullptr, nullptr, c.inst, 0, rs, c.part_e,
+                                                  c.its->Se);
+    FE_CK(cudaGetLastError());
+    if (c.its->small_rows > 0) {
+      SmallRows m{};
+      for (int r = 0; r < c.its->small_rows; ++r) m.slab_row[r] = c.its->small_slab_row[(size_t)r];
+      k_small_combine<T, C><<<(unsigned)c.its->small_rows, kThreads, 0, c.s>>>(
+          c.small_part, (int)grid, c.its->small_rows, m, static_cast<T*>(c.S), c.d.active);
+      FE_CK(cudaGetLastError());
+    }
+    return 0;
+  } else {
+    (void)c;
+    (void)tab;
+    (void)rows;
+    set_error_cstr("fused expand-demean requested for a tile narrower than 32 columns");
+    return 1;
+  }
+}
+
+template <typename T, int C, int U, class Tab>
+static int exdm_u(Ctx& c, Tab tab, T* rows) {
+  const fe_plan* pl = c.pl;
+  bool w = false;
+  int ns = 0;
+  for (int k = 0; k < pl->K; ++k) {
+    const bool small = ((c.its->small_mask >> k) & 1u) != 0;
+    if (small) ++ns;
+    if ((small || k == pl->primary) && (pl->weighted || pl->interacted[k])) w = true;
+  }
+  const int sel = ns * 2 + (w ? 1 : 0);
+  if (c.d.K <= 4) {
+    switch (sel) {
+      case 0: return exdm_launch<T, C, U, 4, false, 0>(c, tab, rows);
+      case 1: return exdm_launch<T, C, U, 4, true, 0>(c, tab, rows);
+      case 2: return exdm_launch<T, C, U, 4, false, 1>(c, tab, rows);
+      case 3: return exdm_launch<T, C, U, 4, true, 1>(c, tab, rows);
+      case 4: return exdm_launch<T, C, U, 4, false, 2>(c, tab, rows);
+      default: return exdm_launch<T, C, U, 4, true, 2>(c, tab, rows);
+    }
+  }
+  switch (sel) {
+    case 0: return exdm_launch<T, C, U, kMaxFE, false, 0>(c, tab, rows);
+    case 1: return exdm_launch<T, C, U, kMaxFE, true, 0>(c, tab, rows);
+    case 2: return exdm_launch<T, C, U, kMaxFE, false, 1>(c, tab, rows);
+    case 3: return exdm_launch<T, C, U, kMaxFE, true, 1>(c, tab, rows);
+    case 4: return exdm_launch<T, C, U, kMaxFE, false, 2>(c, tab, rows);
+    default: return exdm_launch<T, C, U, kMaxFE, true, 2>(c, tab, rows);
+  }
+}
+
+template <typename T, int C, class Tab>
+static int launch_expand_demean(Ctx& c, Tab tab, T* rows, const char* name, double bytes) {
+  ProfScope ps(c.pl, name, bytes);
+  // unroll depth 4 (measured fastest on the worker/firm/year workload), or
+  // that of a forced expand variant
+  const int var = c.pl->opt_ex_variant >= 0 ? c.pl->opt_ex_variant : 3;
+  if (var == 1 || var == 3 || var == 5) return exdm_u<T, C, 4>(c, tab, rows);
+  return exdm_u<T, C, 2>(c, tab, rows);
+}
+
 template <typename TA, int C, int U, int S, class Load>
 static int launch_segsum_async(Ctx& c, Load ld, TA* out, const ReduceItem* items, int64_t n,
                                unsigned grid) {
@@ -537,7 +634,7 @@ static bool use_absorb(const fe_plan* pl, const ItemSet* its, int C) {
 struct Bytes {
   double expand, segsum, pupdate, resid64, segsum64, grad64, rowsum, rowsum64;
   // absorbed-primary mode
-  double expand_abs, resid64_abs, demean, demean64, pupdate_np, grad64_np;
+  double expand_abs, resid64_abs, demean, demean64, pupdate_np, grad64_np, expand_demean;
 };
 static Bytes alg_bytes(const fe_plan* pl, const ItemSet* its, int C, int sT) {
   Bytes b{};
@@ -603,6 +700,8 @@ static Bytes alg_bytes(const fe_plan* pl, const ItemSet* its, int C, int sT) {
     b.demean = keys + 2.0 * N * C * sT + Pp * sT;
     b.demean64 = keys64 + 2.0 * N * C * 8.0 + N * C * 4.0 + Pp * 8.0;
     b.pupdate_np = 9.0 * Pnp * C * sT;
+    // fused: the expand's bytes plus the primary and small-FE keys and scales
+    b.expand_demean = b.expand_abs + keys + Pp * sT;
     b.grad64_np = Pnp * C * (8.0 + 4.0 + 8.0 + 4.0 + 8.0);
   }
   b.pupdate = 9.0 * P * C * sT;
@@ -763,6 +862,7 @@ static int run_loop(fe_plan* pl, Ctx& c, int prec, int64_t cap, int32_t nact0, B
     key = key * 3 + (c.rowsum ? 1u : 0u);
     key = key * 5 + (size_t)(pl->opt_rowsum_variant + 1);
     key = key * 3 + (c.absorb ? 1u : 0u);
+    key = key * 3 + (size_t)pl->opt_exdm;
     lg = &pl->graphs[{c.C, prec}];
     if (!lg->exec || lg->key != key) {
       if (lg->exec) {
@@ -1119,10 +1219,16 @@ static int solve_mixed_tile(fe_plan* pl, const SolveReq& rq, int64_t col0, int n
       if (absorb) {
         // u = M (av A_r v + au u): the expand without the primary FE, then the
         // projection (which also gives ||u|| and the small FEs' sums)
-        if ((e = launch_expand<float, C>(c, TabOne<float, float, vec_of<float, C>()>{V}, ee, nullptr,
-                                         "expand", by.expand_abs)))
-          return e;
-        if ((e = launch_demean<float, C>(c, U, nullptr, S32, "demean", by.demean))) return e;
+        if (pl->opt_exdm) {
+          if ((e = launch_expand_demean<float, C>(c, TabOne<float, float, vec_of<float, C>()>{V}, U,
+                                                  "expand_demean", by.expand_demean)))
+            return e;
+        } else {
+          if ((e = launch_expand<float, C>(c, TabOne<float, float, vec_of<float, C>()>{V}, ee, nullptr,
+                                           "expand", by.expand_abs)))
+            return e;
+          if ((e = launch_demean<float, C>(c, U, nullptr, S32, "demean", by.demean))) return e;
+        }
         if ((e = launch_scalar_phase(c, PH_BETA, 0))) return e;
         if ((e = launch_segsum<float, C>(c, LoadIn<float, float, vec_of<float, C>()>{U}, S32, "segsum",
                                          by.segsum, true, "", 0.0, true)))

@@ -79,6 +79,8 @@ extern "C" {
                                 primary FE out of the least-squares problem and run
                                 LSMR over the other FEs' levels (same residuals, fewer
                                 and cheaper iterations); 0: LSMR over all FEs */
+#define FE_OPT_FUSED_DEMEAN 15 /* 1 (default): the absorbed loop computes and projects
+                                  the rows in one kernel; 0: expand, then demean */
 
 typedef struct fe_plan fe_plan;
 
