@@ -941,7 +941,9 @@ k_rowsum_reg(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_item
 // (whose levels are contiguous row segments, the observations being sorted by
 // it) projected out of the least-squares problem, the solver works with
 // M u = u - a_l (a_l' u) per primary level l, where a_l holds cw_i * scale_l on
-// the rows of level l (a unit vector).  In place on rows [N][32] of T:
+// the rows of level l (a unit vector).  From rows `in` to rows `rows` ([N][32]
+// of T; the same buffer for the in-place projection, every element being read
+// before the same thread stores it):
 //   pass 1 of an item: z_l = sum_{i in l} cw_i u_i per level -> sum slab
 //                      (the primary FE's rows of the [P][C] slab, free here);
 //   pass 2:            u_i -= cw_i scale_l^2 z_l, ||u||^2 per column into the
@@ -954,9 +956,9 @@ k_rowsum_reg(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_item
 // ---------------------------------------------------------------------------
 template <typename T, int C, bool W, int NS>
 __global__ void __launch_bounds__(kThreads, 2)
-k_demean(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_items,
-         T* __restrict__ rows, float* __restrict__ rows32, RowSumArgs rs,
-         double* __restrict__ part, int64_t S) {
+k_demean(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_items, const T* in,
+         T* rows, float* __restrict__ rows32, RowSumArgs rs, double* __restrict__ part,
+         int64_t S) {
   static_assert(C == 32, "one column per lane");
   constexpr int STEP = sizeof(T) == 4 ? 16 : 8;
   constexpr int RC = (int)kDemeanRows;  // rows of an item held in registers
@@ -1010,7 +1012,7 @@ k_demean(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_items,
         if (W && cw1) c1 = __ldg(cw1 + p);
       }
       T x[RC];
-      const T* __restrict__ src = rows + it.ib * C + lane;
+      const T* src = in + it.ib * C + lane;
 #pragma unroll
       for (int r = 0; r < RC; ++r) x[r] = r < n ? src[(int64_t)r * C] : T(0);
       const int kn = __shfl_down_sync(FE_FULL, kpr, 1);
@@ -1032,7 +1034,7 @@ k_demean(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_items,
       }
       __syncwarp();
       // pass 2: u -= cw scale^2 z, stored, ||u||^2; padded rows stay 0
-      T* __restrict__ dst = rows + it.ib * C + lane;
+      T* dst = rows + it.ib * C + lane;
       li = 0;
 #pragma unroll
       for (int r = 0; r < RC; ++r) {
@@ -1070,7 +1072,7 @@ k_demean(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_items,
       const T cpv = (W && okl && cwp) ? __ldg(cwp + base + lane) : T(1);
       T x[STEP];
 #pragma unroll
-      for (int r = 0; r < STEP; ++r) x[r] = r < nvalid ? rows[(base + r) * C + lane] : T(0);
+      for (int r = 0; r < STEP; ++r) x[r] = r < nvalid ? in[(base + r) * C + lane] : T(0);
       const int kn = __shfl_down_sync(FE_FULL, kpr, 1);
       const uint32_t bmask = __ballot_sync(FE_FULL, lane + 1 < nvalid && kn != kpr);
       const int kfirst = __shfl_sync(FE_FULL, kpr, 0);
@@ -1113,7 +1115,7 @@ k_demean(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_items,
           const int kr = __shfl_sync(FE_FULL, kpr, r);
           const T fr = __shfl_sync(FE_FULL, f, r);
           const int64_t o = (base + r) * C + lane;
-          const T u = rows[o] - fr * Z[(int64_t)kr * C];
+          const T u = in[o] - fr * Z[(int64_t)kr * C];
           rows[o] = u;
           if (rows32) rows32[o] = (float)u;
           nrm += (double)u * (double)u;

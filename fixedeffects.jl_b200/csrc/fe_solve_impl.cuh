@@ -319,7 +319,7 @@ static int launch_rowsum(Ctx& c, const TA* src, TA* out) {
 // optional FP32 copy; out: the [P][C] sum slab (z rows of the primary FE,
 // small-FE sums); ||rows||^2 goes to the expand norm slots.
 template <typename T, int C, bool W, int NS>
-static int demean_launch(Ctx& c, T* rows, float* rows32, T* out) {
+static int demean_launch(Ctx& c, const T* in, T* rows, float* rows32, T* out) {
   if constexpr (C == 32) {
     auto kern = k_demean<T, C, W, NS>;
     const size_t smem = (size_t)kWarps * (kDemeanRows + c.its->small_rows) * C * sizeof(T);
@@ -351,8 +351,8 @@ static int demean_launch(Ctx& c, T* rows, float* rows32, T* out) {
         rs.small_off[rs.n_small] = c.its->small_off[k];
         ++rs.n_small;
       }
-    kern<<<(unsigned)grid, kThreads, smem, c.s>>>(c.d, c.its->d_dm.as<ExpandItem>(), n, rows, rows32,
-                                                  rs, c.part_e, c.its->Se);
+    kern<<<(unsigned)grid, kThreads, smem, c.s>>>(c.d, c.its->d_dm.as<ExpandItem>(), n, in, rows,
+                                                  rows32, rs, c.part_e, c.its->Se);
     FE_CK(cudaGetLastError());
     if (c.its->small_rows > 0) {
       SmallRows m{};
@@ -364,6 +364,7 @@ static int demean_launch(Ctx& c, T* rows, float* rows32, T* out) {
     return 0;
   } else {
     (void)c;
+    (void)in;
     (void)rows;
     (void)rows32;
     (void)out;
@@ -372,8 +373,11 @@ static int demean_launch(Ctx& c, T* rows, float* rows32, T* out) {
   }
 }
 
+// in: source rows (nullptr: rows, projected in place)
 template <typename T, int C>
-static int launch_demean(Ctx& c, T* rows, float* rows32, T* out, const char* name, double bytes) {
+static int launch_demean(Ctx& c, T* rows, float* rows32, T* out, const char* name, double bytes,
+                         const T* in = nullptr) {
+  if (!in) in = rows;
   ProfScope ps(c.pl, name, bytes);
   const fe_plan* pl = c.pl;
   bool w = false;
@@ -384,12 +388,12 @@ static int launch_demean(Ctx& c, T* rows, float* rows32, T* out, const char* nam
     if ((small || k == pl->primary) && (pl->weighted || pl->interacted[k])) w = true;
   }
   switch (ns * 2 + (w ? 1 : 0)) {
-    case 0: return demean_launch<T, C, false, 0>(c, rows, rows32, out);
-    case 1: return demean_launch<T, C, true, 0>(c, rows, rows32, out);
-    case 2: return demean_launch<T, C, false, 1>(c, rows, rows32, out);
-    case 3: return demean_launch<T, C, true, 1>(c, rows, rows32, out);
-    case 4: return demean_launch<T, C, false, 2>(c, rows, rows32, out);
-    default: return demean_launch<T, C, true, 2>(c, rows, rows32, out);
+    case 0: return demean_launch<T, C, false, 0>(c, in, rows, rows32, out);
+    case 1: return demean_launch<T, C, true, 0>(c, in, rows, rows32, out);
+    case 2: return demean_launch<T, C, false, 1>(c, in, rows, rows32, out);
+    case 3: return demean_launch<T, C, true, 1>(c, in, rows, rows32, out);
+    case 4: return demean_launch<T, C, false, 2>(c, in, rows, rows32, out);
+    default: return demean_launch<T, C, true, 2>(c, in, rows, rows32, out);
   }
 }
 
@@ -1192,14 +1196,19 @@ static int solve_mixed_tile(fe_plan* pl, const SolveReq& rq, int64_t col0, int n
     FE_CK(cudaMemsetAsync(c.counters, 0, 3 * sizeof(int32_t), c.s));
     // r = b - A (x64 + dx32) in FP64, with the FP32 copy as the next inner u
     // (absorbed: r = M (b - A_r x), projected and copied by the demean pass)
-    if ((st = launch_expand<double, C>(
+    // absorbed: round 0 starts from x = 0, so r0 = M b comes straight from b
+    const bool from_b = absorb && round == 0;
+    if (!from_b &&
+        (st = launch_expand<double, C>(
              c, TabSum64<vec_of<double, C>()>{X64, X},
              EpiBminusAx<double, double, vec_of<double, C>()>{B64, R64, absorb ? nullptr : U, c.inst, 2},
              absorb ? nullptr : c.part_e, "resid64", absorb ? by.resid64_abs : by.resid64)))
       return st;
     // g = A'r in FP64 (the next inner v), x64 += dx32, ||x64||
     if (absorb) {
-      if ((st = launch_demean<double, C>(c, R64, U, S64, "demean64", by.demean64))) return st;
+      if ((st = launch_demean<double, C>(c, R64, U, S64, "demean64", by.demean64,
+                                         from_b ? B64 : nullptr)))
+        return st;
       if ((st = launch_segsum<double, C>(c, LoadIn<double, double, vec_of<double, C>()>{R64}, S64,
                                          "segsum64", by.segsum64, true, "", 0.0, true)))
         return st;
