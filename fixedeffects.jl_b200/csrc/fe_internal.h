@@ -107,6 +107,10 @@ struct FeDev {
   // so the iterations that finish a replayed chunk after every instance has
   // stopped cost launches only
   const int32_t* active;
+  // the same count for kernels that run before the beta phase (the demean
+  // and the fused expand + demean of the absorbed loop): the alpha phase of
+  // the previous iteration, or the refinement phase, has just written it
+  const int32_t* active_pre;
   // absorbed-primary mode: the expand leaves out the primary FE (its effect is
   // projected out of the rows by the demean pass instead)
   int32_t absorb;

@@ -965,7 +965,7 @@ k_demean(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_items, c
   static_assert(RC == 32, "one item row per lane for the keys");
   __shared__ double sm[kWarps][32];
   extern __shared__ __align__(16) unsigned char demean_smem[];
-  if (d.active && *d.active == 0) return;  // the whole CTA
+  if (d.active_pre && *d.active_pre == 0) return;  // the whole CTA
   const int lane = threadIdx.x & 31;
   const int wib = threadIdx.x >> 5;
   // per warp: RC z rows (levels of a short item), then the small-FE table
@@ -1198,7 +1198,7 @@ k_expand_demean(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_i
   static_assert(STEP <= 32 && RC % STEP == 0, "steps tile an item's row buffer");
   __shared__ double sm[kWarps][32];
   extern __shared__ __align__(16) unsigned char exdm_smem[];
-  if (d.active && *d.active == 0) return;  // the whole CTA
+  if (d.active_pre && *d.active_pre == 0) return;  // the whole CTA
   const int lane = threadIdx.x & 31;
   const int wib = threadIdx.x >> 5;
   const int g = lane / CL, jl = lane - g * CL;

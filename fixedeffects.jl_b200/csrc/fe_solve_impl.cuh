@@ -358,7 +358,7 @@ static int demean_launch(Ctx& c, const T* in, T* rows, float* rows32, T* out) {
       SmallRows m{};
       for (int r = 0; r < c.its->small_rows; ++r) m.slab_row[r] = c.its->small_slab_row[(size_t)r];
       k_small_combine<T, C><<<(unsigned)c.its->small_rows, kThreads, 0, c.s>>>(
-          c.small_part, (int)grid, c.its->small_rows, m, out, c.d.active);
+          c.small_part, (int)grid, c.its->small_rows, m, out, c.d.active_pre);
       FE_CK(cudaGetLastError());
     }
     return 0;
@@ -440,7 +440,7 @@ static int exdm_launch(Ctx& c, Tab tab, T* rows) {
       SmallRows m{};
       for (int r = 0; r < c.its->small_rows; ++r) m.slab_row[r] = c.its->small_slab_row[(size_t)r];
       k_small_combine<T, C><<<(unsigned)c.its->small_rows, kThreads, 0, c.s>>>(
-          c.small_part, (int)grid, c.its->small_rows, m, static_cast<T*>(c.S), c.d.active);
+          c.small_part, (int)grid, c.its->small_rows, m, static_cast<T*>(c.S), c.d.active_pre);
       FE_CK(cudaGetLastError());
     }
     return 0;
@@ -1257,8 +1257,10 @@ static int solve_mixed_tile(fe_plan* pl, const SolveReq& rq, int64_t col0, int n
     };
     int64_t done = 0;
     c.d.active = c.counters + 2;
+    c.d.active_pre = c.counters;
     st = run_loop(pl, c, 1, cap - total_it, nout, body, &done);
     c.d.active = nullptr;
+    c.d.active_pre = nullptr;
     if (st) return st;
     total_it += done;
   }
