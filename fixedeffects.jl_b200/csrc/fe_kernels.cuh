@@ -1178,6 +1178,54 @@ k_demean(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_items, c
 // w to the row buffer and accumulates z, then a second walk finalizes it.
 // RESID, mask: columns whose refinement has stopped keep their stored rows.
 // ---------------------------------------------------------------------------
+// Small-FE table update by the G row groups of one warp instruction (row
+// group g holds row r_g's values u, VEC columns per lane): rows whose table
+// row (key) appeared in an earlier group are added into that group first, so
+// the remaining groups hit distinct table rows and update them in one
+// load/add/store.  key >= 0 for a valid row.
+template <typename T, int C, int VEC, int CL, int G>
+__device__ __forceinline__ void vec_table_update(T* tbl, int key, bool valid, VA<T, VEC> u, int g,
+                                                 int jl, int lane) {
+  const int mine = valid ? key : -1 - g;  // invalid rows match nothing
+  int kg[G];
+#pragma unroll
+  for (int h = 0; h < G; ++h) kg[h] = __shfl_sync(FE_FULL, mine, h * CL);
+  int dup[G];
+#pragma unroll
+  for (int h = 0; h < G; ++h) {
+    dup[h] = -1;
+#pragma unroll
+    for (int i = h - 1; i >= 0; --i)
+      if (kg[i] == kg[h]) dup[h] = i;
+  }
+#pragma unroll
+  for (int j = 1; j < G; ++j)
+#pragma unroll
+    for (int i = 0; i < j; ++i)
+      if (dup[j] == i) {  // warp-uniform
+#pragma unroll
+        for (int v = 0; v < VEC; ++v) {
+          const T o = __shfl_sync(FE_FULL, u.v[v], (lane + (j - i) * CL) & 31);
+          if (g == i) u.v[v] += o;
+        }
+      }
+  bool mydup = false;
+#pragma unroll
+  for (int h = 0; h < G; ++h)
+    if (h == g) mydup = dup[h] >= 0;
+  if (valid && !mydup) {
+    T* p = tbl + (int64_t)key * C + jl * VEC;
+    VA<T, VEC> a = vld<T, VEC>(p);
+#pragma unroll
+    for (int v = 0; v < VEC; ++v) a.v[v] += u.v[v];
+    vst<T, VEC>(p, a);
+  }
+}
+
+__device__ __forceinline__ void prefetch_l2(const void* p) {
+  asm volatile("prefetch.global.L2 [%0];\n" ::"l"(p));
+}
+
 template <typename T, int VEC>
 struct ExDmCoef {
   T av[VEC], au[VEC];
@@ -1202,10 +1250,12 @@ k_expand_demean(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_i
   const int lane = threadIdx.x & 31;
   const int wib = threadIdx.x >> 5;
   const int g = lane / CL, jl = lane - g * CL;
-  const size_t wstride_smem = (size_t)(2 * RC + rs.small_rows) * C;
+  // per warp: staged rows, level sums, small-FE table, end row of each level
+  const size_t wstride_smem = (size_t)(2 * RC + rs.small_rows) * C + 32 * sizeof(int) / sizeof(T);
   T* ub = reinterpret_cast<T*>(exdm_smem) + (size_t)wib * wstride_smem;  // staged rows
   T* zs = ub + RC * C;                                                   // level sums
   T* tbl = zs + RC * C;                                                  // small-FE table
+  int* lend = reinterpret_cast<int*>(tbl + rs.small_rows * C);           // last row of level j
   for (int e = lane; e < rs.small_rows * C; e += 32) tbl[e] = T(0);
   const int K = d.K;
   const int kp = d.primary;
@@ -1230,7 +1280,10 @@ k_expand_demean(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_i
   }
   const bool col_act = RESID ? (mask != 2 || inst[lane].outer_active != 0) : inst[lane].active != 0;
   act_any = __any_sync(FE_FULL, act_any);
-  double nrm = 0.0;
+  double nrm = 0.0;      // ||u||^2 of column `lane` (long levels)
+  double nrmv[VEC];      // ||u||^2 of this lane's VEC columns (short items)
+#pragma unroll
+  for (int v = 0; v < VEC; ++v) nrmv[v] = 0.0;
   __syncwarp();
 
   // phase A on rows [cb, cb + cn) (cn <= RC): w rows into ub (and, for a
@@ -1370,27 +1423,112 @@ k_expand_demean(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_i
     const ExpandItem it = items[wi];
     const int64_t ie = it.ie;
     if (ie <= it.ib || !act_any) continue;
+    // the warp's next item: its rows and index lines into L2 while this one
+    // is processed
+    if (wi + wstride < n_items) {
+      const ExpandItem nx = items[wi + wstride];
+      const int64_t nn = nx.ie - nx.ib;
+      if (lane < nn && lane < RC) {
+        const int64_t o = (nx.ib + lane) * C;
+        if (RESID) {
+          prefetch_l2(B + o);
+          if (C * sizeof(double) > 128) prefetch_l2(B + o + 128 / sizeof(double));
+        } else {
+          prefetch_l2(rows + o);
+          if (C * sizeof(T) > 128) prefetch_l2(rows + o + 128 / sizeof(T));
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < KB; ++k)
+        if (k < K && lane == k) prefetch_l2(d.refs[k] + nx.ib);
+    }
     if (ie - it.ib <= RC) {
       const int n = (int)(ie - it.ib);
       phase_a(it.ib, n, false);
       const RowData rd = row_data(it.ib, n);
       const int kn = __shfl_down_sync(FE_FULL, rd.kpr, 1);
-      const uint32_t ends = __ballot_sync(FE_FULL, lane < n && (lane + 1 == n || kn != rd.kpr));
-      // level sums in level order
-      T acc = T(0);
-      int li = 0;
-#pragma unroll 8
-      for (int r = 0; r < n; ++r) {
-        const T w = ub[r * C + lane];
-        acc += W ? w * __shfl_sync(FE_FULL, rd.cwv, r) : w;
-        if ((ends >> r) & 1u) {
-          zs[li * C + lane] = acc;
-          acc = T(0);
-          ++li;
+      const bool is_end = lane < n && (lane + 1 == n || kn != rd.kpr);
+      const uint32_t ends = __ballot_sync(FE_FULL, is_end);
+      const int nlev = __popc(ends);
+      if (is_end) lend[__popc(ends & ((1u << lane) - 1u))] = lane;
+      __syncwarp();
+      // B1: level sums, vector layout; row group g sums levels g, g+G, ...
+      for (int jb = 0; jb < nlev; jb += G) {
+        const int j = jb + g;
+        const bool okj = j < nlev;
+        const int e = okj ? lend[j] : -1;
+        const int st = (okj && j > 0) ? lend[j - 1] + 1 : 0;
+        const int len = okj ? e - st + 1 : 0;
+        const int maxlen = __reduce_max_sync(FE_FULL, (unsigned)len);
+        VA<T, VEC> acc;
+#pragma unroll
+        for (int v = 0; v < VEC; ++v) acc.v[v] = T(0);
+        for (int t = 0; t < maxlen; ++t) {
+          const bool ok = t < len;
+          const int r = ok ? st + t : 0;
+          const T cwr = W ? __shfl_sync(FE_FULL, rd.cwv, r) : T(1);
+          if (ok) {
+            const VA<T, VEC> w = vld<T, VEC>(ub + r * C + jl * VEC);
+#pragma unroll
+            for (int v = 0; v < VEC; ++v) acc.v[v] += cwr * w.v[v];
+          }
         }
+        if (okj) vst<T, VEC>(zs + j * C + jl * VEC, acc);
       }
       __syncwarp();
-      finalize(it.ib, n, rd, ends, true, T(0));
+      // B2: u = w - cw scale^2 z, stored once; norms; small-FE tables
+      VA<T, VEC> nvi;
+#pragma unroll
+      for (int v = 0; v < VEC; ++v) nvi.v[v] = T(0);
+      for (int t = 0; t * G < n; ++t) {
+        const int r = t * G + g;
+        const bool ok = r < n;
+        const T fr = __shfl_sync(FE_FULL, rd.f, r);
+        VA<T, VEC> u;
+        if (ok) {
+          const int li = __popc(ends & ((1u << r) - 1u));
+          const VA<T, VEC> z = vld<T, VEC>(zs + li * C + jl * VEC);
+          u = vld<T, VEC>(ub + r * C + jl * VEC);
+#pragma unroll
+          for (int v = 0; v < VEC; ++v) u.v[v] -= fr * z.v[v];
+          const int64_t o = (it.ib + r) * C + jl * VEC;
+          if (RESID) {
+#pragma unroll
+            for (int v = 0; v < VEC; ++v)
+              if (cf.act[v]) {
+                rows[o + v] = u.v[v];
+                if (rows32) rows32[o + v] = (float)u.v[v];
+                nvi.v[v] += u.v[v] * u.v[v];
+              }
+          } else {
+            vst<T, VEC>(rows + o, u);
+#pragma unroll
+            for (int v = 0; v < VEC; ++v) nvi.v[v] += u.v[v] * u.v[v];
+          }
+        } else {
+#pragma unroll
+          for (int v = 0; v < VEC; ++v) u.v[v] = T(0);
+        }
+        if (NS > 0) {
+          const int k0r = __shfl_sync(FE_FULL, rd.k0, r);
+          const T c0r = W ? __shfl_sync(FE_FULL, rd.c0, r) : T(1);
+          VA<T, VEC> u0 = u;
+#pragma unroll
+          for (int v = 0; v < VEC; ++v) u0.v[v] *= c0r;
+          vec_table_update<T, C, VEC, CL, G>(tbl, k0r, ok, u0, g, jl, lane);
+          if (NS > 1) {
+            const int k1r = __shfl_sync(FE_FULL, rd.k1, r);
+            const T c1r = W ? __shfl_sync(FE_FULL, rd.c1, r) : T(1);
+            VA<T, VEC> u1 = u;
+#pragma unroll
+            for (int v = 0; v < VEC; ++v) u1.v[v] *= c1r;
+            vec_table_update<T, C, VEC, CL, G>(tbl, k1r, ok, u1, g, jl, lane);
+          }
+        }
+      }
+#pragma unroll
+      for (int v = 0; v < VEC; ++v) nrmv[v] += (double)nvi.v[v];
+      __syncwarp();  // ub, zs and lend are rewritten by the next item
       continue;
     }
     // one level longer than RC rows: w through the row buffer, then finalize
@@ -1413,7 +1551,18 @@ k_expand_demean(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_i
       finalize(cb, cn, rd, 0u, false, zl);
     }
   }
-  // ||u||^2: warp -> CTA slot (fixed order); slots beyond the grid hold 0
+  // ||u||^2: the vector-layout sums folded into the per-column ones, then
+  // warp -> CTA slot (fixed order); slots beyond the grid hold 0
+#pragma unroll
+  for (int v = 0; v < VEC; ++v) {
+    double a = nrmv[v];
+#pragma unroll
+    for (int o = CL; o < 32; o <<= 1) a += __shfl_xor_sync(FE_FULL, a, o);
+    if (g == 0) sm[wib][jl * VEC + v] = a;
+  }
+  __syncwarp();
+  nrm += sm[wib][lane];
+  __syncwarp();
   sm[wib][lane] = nrm;
   __syncthreads();
   if (part != nullptr && threadIdx.x < C) {

@@ -404,13 +404,15 @@ template <typename T, int C, int U, int KB, bool W, int NS, class Tab>
 static int exdm_launch(Ctx& c, Tab tab, T* rows) {
   if constexpr (C == 32) {
     auto kern = k_expand_demean<T, C, U, KB, false, W, NS, Tab>;
-    const size_t smem = (size_t)kWarps * (2 * kDemeanRows + c.its->small_rows) * C * sizeof(T);
+    const size_t smem =
+        (size_t)kWarps * ((2 * kDemeanRows + c.its->small_rows) * C * sizeof(T) + 32 * sizeof(int));
     static bool attr_set = false;  // per instantiation
     static size_t occ_smem = (size_t)-1;
     static int occ = 1;
     if (!attr_set) {
       FE_CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)(kWarps * (2 * kDemeanRows + kSmallRows) * C * sizeof(T))));
+                                 (int)(kWarps * ((2 * kDemeanRows + kSmallRows) * C * sizeof(T) +
+                                                 32 * sizeof(int)))));
       attr_set = true;
     }
     if (occ_smem != smem) {
