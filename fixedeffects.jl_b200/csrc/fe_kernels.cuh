@@ -1289,17 +1289,18 @@ k_expand_demean(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_i
   // phase A on rows [cb, cb + cn) (cn <= RC): w rows into ub (and, for a
   // chunk of a long level, into the row buffer)
   auto phase_a = [&](int64_t cb, int cn, bool to_global) {
+    // refs and weights of the chunk's rows (row = lane), loaded once
+    int rl[KB];
+    T cl[KB];
+#pragma unroll
+    for (int k = 0; k < KB; ++k) {
+      const bool ok = k < K && k != kp && lane < cn;
+      rl[k] = ok ? __ldg(d.refs[k] + cb + lane) : 0;
+      const T* __restrict__ cw = cw_of<T>(d, k < K ? k : 0);
+      cl[k] = (ok && cw) ? __ldg(cw + cb + lane) : T(1);
+    }
     for (int b0 = 0; b0 < cn; b0 += STEP) {
       const int64_t base = cb + b0;
-      int rl[KB];
-      T cl[KB];
-#pragma unroll
-      for (int k = 0; k < KB; ++k) {
-        const bool ok = k < K && k != kp && lane < STEP && b0 + lane < cn;
-        rl[k] = ok ? __ldg(d.refs[k] + base + lane) : 0;
-        const T* __restrict__ cw = cw_of<T>(d, k < K ? k : 0);
-        cl[k] = (ok && cw) ? __ldg(cw + base + lane) : T(1);
-      }
       VA<T, VEC> old[U];
       VA<T, VEC> sacc[U];
 #pragma unroll
@@ -1327,8 +1328,8 @@ k_expand_demean(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_i
 #pragma unroll
           for (int u = 0; u < U; ++u) {
             const int q = u * G + g;
-            const int ref = __shfl_sync(FE_FULL, rl[k], q);
-            const T c = wk ? __shfl_sync(FE_FULL, cl[k], q) : T(1);
+            const int ref = __shfl_sync(FE_FULL, rl[k], b0 + q);
+            const T c = wk ? __shfl_sync(FE_FULL, cl[k], b0 + q) : T(1);
             if (b0 + q < cn) {
               const T scl = __ldg(sc + ref);
               const T cs = wk ? c * scl : scl;
@@ -1419,14 +1420,18 @@ k_expand_demean(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_i
   };
 
   const int64_t wstride = (int64_t)gridDim.x * kWarps;
-  for (int64_t wi = (int64_t)blockIdx.x * kWarps + wib; wi < n_items; wi += wstride) {
-    const ExpandItem it = items[wi];
+  int64_t wi0 = (int64_t)blockIdx.x * kWarps + wib;
+  ExpandItem nxt{};  // descriptor of the warp's next item (loaded one item ahead)
+  if (wi0 < n_items) nxt = items[wi0];
+  for (int64_t wi = wi0; wi < n_items; wi += wstride) {
+    const ExpandItem it = nxt;
+    if (wi + wstride < n_items) nxt = items[wi + wstride];
     const int64_t ie = it.ie;
     if (ie <= it.ib || !act_any) continue;
     // the warp's next item: its rows and index lines into L2 while this one
     // is processed
     if (wi + wstride < n_items) {
-      const ExpandItem nx = items[wi + wstride];
+      const ExpandItem nx = nxt;
       const int64_t nn = nx.ie - nx.ib;
       if (lane < nn && lane < RC) {
         const int64_t o = (nx.ib + lane) * C;
@@ -1444,8 +1449,8 @@ k_expand_demean(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_i
     }
     if (ie - it.ib <= RC) {
       const int n = (int)(ie - it.ib);
+      const RowData rd = row_data(it.ib, n);  // loads overlap phase A's
       phase_a(it.ib, n, false);
-      const RowData rd = row_data(it.ib, n);
       const int kn = __shfl_down_sync(FE_FULL, rd.kpr, 1);
       const bool is_end = lane < n && (lane + 1 == n || kn != rd.kpr);
       const uint32_t ends = __ballot_sync(FE_FULL, is_end);
