@@ -294,8 +294,27 @@ class FixedEffectSolverB200:
         _lib.check(_lib.load().fe_solve_coefficients(
             self._h, a.ctypes.data, dt, self.precision, float(tol), int(maxiter), _ptrs(coefs),
             ctypes.byref(it), ctypes.byref(cv)))
-        coefs = [c.astype(a.dtype, copy=False) for c in coefs]
-        return full(normalize(coefs, self.fes), self.fes), int(it.value), bool(cv.value)
+        # normalize! and full on the device (fe_normalize_coefficients,
+        # fe_full_coefficients), in FP64
+        L = _lib.load()
+        _lib.check(L.fe_normalize_coefficients(self._h, _ptrs(coefs), 0))
+        outs = [np.empty(self.N, dtype=np.float64) for _ in self.fes]
+        _lib.check(L.fe_full_coefficients(self._h, _ptrs(coefs), 0, _ptrs(outs), 0))
+        return [o.astype(a.dtype, copy=False) for o in outs], int(it.value), bool(cv.value)
+
+    def normalize_coefficients(self, coefs):
+        """normalize!(fecoefs, fes) on the device (src/FixedEffect.jl:106-135):
+        per-level FP64 coefficient arrays, normalized in place and returned."""
+        coefs = [np.ascontiguousarray(c, dtype=np.float64) for c in coefs]
+        _lib.check(_lib.load().fe_normalize_coefficients(self._h, _ptrs(coefs), 0))
+        return coefs
+
+    def full_coefficients(self, coefs):
+        """full(fecoefs, fes) on the device (src/FixedEffect.jl:137-140)."""
+        coefs = [np.ascontiguousarray(c, dtype=np.float64) for c in coefs]
+        outs = [np.empty(self.N, dtype=np.float64) for _ in self.fes]
+        _lib.check(_lib.load().fe_full_coefficients(self._h, _ptrs(coefs), 0, _ptrs(outs), 0))
+        return outs
 
     # -- diagnostics ----------------------------------------------------------
     def set_option(self, option: int, value: float) -> None:

@@ -155,12 +155,27 @@ int fe_solve_residuals_device(fe_plan* plan, void* Y_dev, int32_t dtype, int64_t
  * solve_coefficients!(y, feM; tol, maxiter) up to, not including, the
  * normalisation: LSMR from x = 0 (src/AbstractFixedEffectSolver.jl:147-157)
  * and coefs[k][l] = x_k[l] * scale_k[l] for l < n_levels[k] (host memory).
- * normalize!/full (src/FixedEffect.jl:106-140) stay in the host binding.
+ * normalize!/full (src/FixedEffect.jl:106-140) follow as
+ * fe_normalize_coefficients and fe_full_coefficients.
  * iterations = div(ch.mvps, 2) as the reference returns.
  */
 int fe_solve_coefficients(fe_plan* plan, const void* y, int32_t dtype, int32_t precision,
                           double tol, int64_t maxiter, double* const* coefs,
                           int64_t* iterations, uint8_t* converged);
+
+/* normalize!(fecoefs, fes) (src/FixedEffect.jl:106-135) on the device: within
+ * each connected component of the observation/level graph of the FEs without
+ * an interaction, every such FE but the first is demeaned and the means are
+ * added to the first.  coefs[k]: n_levels[k] doubles in host memory
+ * (coefs_on_device = 0) or device memory, normalized in place; interacted FEs
+ * are left as they are.  Deterministic (exact fixed-point component sums). */
+int fe_normalize_coefficients(fe_plan* plan, double* const* coefs, int32_t coefs_on_device);
+
+/* full(fecoefs, fes) (src/FixedEffect.jl:137-140): out[k][i] =
+ * coefs[k][refs_k[i]] for every observation i, in the caller's order (N
+ * doubles per FE); host or device memory on either side. */
+int fe_full_coefficients(fe_plan* plan, const double* const* coefs, int32_t coefs_on_device,
+                         double* const* out, int32_t out_on_device);
 
 /* Per-problem iterations/convergence of the last solve: [n_problems][ncols]. */
 int fe_plan_problem_results(fe_plan* plan, int64_t* iterations, uint8_t* converged);
