@@ -341,8 +341,10 @@ def run_ours(args):
             "config": {"workload": WORKLOAD_NAME, "N": N, "fixed_effects": pb.nlev,
                        "columns_per_gpu": ncols, "tol": 1e-8, "precision": "mixed",
                        "parallelism": f"columns sharded over {ws} GPU(s)",
-                       "l2": "inputs larger than L2 (1.28 GB per step)",
-                       "plan_build_s": round(plan_s, 3)},
+                       "l2": "inputs larger than L2 (1.28 GB per step)"},
+            # the solver constructor: refs upload, validation and integer plan
+            # (radix sorts) on the device, weights, preconditioner
+            "plan_build": {"device_s": round(plan_s, 3)},
             "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": N * ncols * 4,
                     "d2h_bytes_per_step": N * ncols * 4, "ms_per_step": e2e_ms},
             "roofline": {"bound": "hbm", "kernel": tname, "achieved": achieved, "peak": peak,
@@ -368,6 +370,12 @@ def run_ours(args):
                 line["max_rel_err_vs_oracle"]["column0_plain_fp64"] = float(
                     np.linalg.norm(plain_result - ro) / np.linalg.norm(ro))
             line["oracle_iterations"] = cb["iterations"]
+            # the host integer plan (stable counting sorts, one core) for scale
+            t0 = time.perf_counter()
+            from oracle import oracle as O
+            O.integer_plan(pb.refs, pb.nlev, feM.primary())
+            line["plan_build"]["oracle_integer_plan_s"] = round(time.perf_counter() - t0, 3)
+            line["plan_build"]["oracle_cores"] = 1
         line["clocks"] = clk.summary()
         print(json.dumps(line), flush=True)
     feM.close()
@@ -413,6 +421,70 @@ def run_sweep(args):
     return 0
 
 
+def run_plan_build(args):
+    """Times plan construction on the device against its host counterparts,
+    on the 10M worker/firm/year workload and the 100M two-FE workload (10M
+    uniform levels, 10K Zipf(1.3) levels):
+      * the solver constructor (refs upload, validation, radix-sort integer
+        plan, weights, preconditioner) vs the oracle's host integer plan
+        (stable counting sorts, one core);
+      * key grouping of raw int64 keys (level ids scattered over the int64
+        range, so the radix-sort path runs) vs numpy's grouping on the host.
+    Prints one JSON line; the device grouping must equal the host one."""
+    import torch
+    torch.cuda.set_device(0)
+    import __graft_entry__ as g
+    fe = g.load_package()
+    import fe_b200.synth as S
+    from oracle import oracle as O
+    O.build()
+
+    def scatter_keys(r):
+        # an injective map of level ids onto sparse int64 keys
+        return (r.astype(np.uint64) * np.uint64(0x9E3779B97F4A7C15)).view(np.int64)
+
+    # load the build kernels once (lazy module loading) on a small case
+    pb = S.config2(scale=0.001, ncols=0)
+    fe.AbstractFixedEffectSolver([fe.FixedEffect.from_refs(r, n) for r, n in zip(pb.refs, pb.nlev)],
+                                 None, "CUDA", np.float32).close()
+    fe.group_keys(scatter_keys(pb.refs[0]), device=0)
+    out = {"metric": "plan construction", "unit": "s", "higher_is_better": False,
+           "data": "synthetic", "workloads": {}}
+    scale = args.scale
+    for name, mk in (("worker_firm_year_10m", lambda: S.config2(scale=scale, ncols=0)),
+                     ("two_fe_100m", lambda: S.config4(scale=scale, ncols=0))):
+        pb = mk()
+        fes = [fe.FixedEffect.from_refs(r, n, a) for r, n, a in zip(pb.refs, pb.nlev, pb.interaction)]
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        feM = fe.AbstractFixedEffectSolver(fes, pb.weights, "CUDA", np.float32, precision="mixed")
+        torch.cuda.synchronize()
+        dev_plan = time.perf_counter() - t
+        t = time.perf_counter()
+        O.integer_plan(pb.refs, pb.nlev, feM.primary())
+        host_plan = time.perf_counter() - t
+        feM.close()
+        dev_group = host_group = 0.0
+        equal = True
+        for r in pb.refs:
+            raw = scatter_keys(r)
+            t = time.perf_counter()
+            dr, dn = fe.group_keys(raw, device=0)
+            dev_group += time.perf_counter() - t
+            t = time.perf_counter()
+            h = fe.FixedEffect(raw)
+            host_group += time.perf_counter() - t
+            equal = equal and dn == h.n and bool(np.array_equal(dr, h.refs))
+        out["workloads"][name] = {
+            "N": pb.N, "fixed_effects": pb.nlev,
+            "device_plan_s": round(dev_plan, 3), "oracle_integer_plan_s": round(host_plan, 3),
+            "device_group_keys_s": round(dev_group, 3), "numpy_group_keys_s": round(host_group, 3),
+            "group_keys_equal_host": equal}
+        log(name, out["workloads"][name])
+    print(json.dumps(out), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -426,7 +498,11 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--sweep-variants", action="store_true",
                     help="time every expand/segsum kernel variant and print a table")
+    ap.add_argument("--plan-build", action="store_true",
+                    help="time plan construction and key grouping, device vs host")
     args = ap.parse_args()
+    if args.plan_build:
+        return run_plan_build(args)
     if args.sweep_variants:
         return run_sweep(args)
     if args.impl == "reference":

@@ -36,7 +36,7 @@ from ._lib import (FE_DTYPE_F32, FE_DTYPE_F64, FE_PREC_FP32, FE_PREC_FP64,
 __all__ = [
     "FixedEffect", "AbstractFixedEffectSolver", "FixedEffectSolverB200", "BatchSolver",
     "solve_residuals", "solve_coefficients", "update_weights", "normalize", "full",
-    "components", "DimensionMismatch", "FEError",
+    "components", "group_keys", "DimensionMismatch", "FEError",
 ]
 
 _METHODS = {"CUDA", "cuda", "gpu", "GPU"}
@@ -62,21 +62,49 @@ def _compact(keys) -> tuple[np.ndarray, int]:
     return (inv.reshape(-1) + 1).astype(np.int64), int(uniq.size)
 
 
+def group_keys(*keys, device: int = 0) -> tuple[np.ndarray, int]:
+    """Level ids of integer key tuples, grouped on the GPU (fe_group_keys):
+    1-based ranks of the distinct tuples in lexicographic ascending order, and
+    their count.  The same ids as the host grouping of ``FixedEffect``."""
+    if not keys:
+        raise ValueError("group_keys needs at least one key vector")
+    cols = []
+    for a in keys:
+        a = np.asarray(a)
+        if a.ndim != 1 or a.dtype.kind not in "iub":
+            raise TypeError("device grouping takes 1-d integer key vectors")
+        if a.dtype.kind == "u" and a.size and int(a.max()) > np.iinfo(np.int64).max:
+            raise TypeError("unsigned keys above 2^63-1 are not supported")
+        cols.append(np.ascontiguousarray(a, dtype=np.int64))
+    n = cols[0].shape[0]
+    if any(c.shape[0] != n for c in cols):
+        raise DimensionMismatch("all key vectors must have the same length")
+    refs = np.empty(n, dtype=np.int64)
+    nl = ctypes.c_int64(0)
+    _lib.check(_lib.load().fe_group_keys(_ptrs(cols), len(cols), n, int(device),
+                                         refs.ctypes.data_as(_lib._i64p), ctypes.byref(nl)))
+    return refs, int(nl.value)
+
+
 class FixedEffect:
     """A fixed effect: 1-based level ids, an optional interaction, level count.
 
     ``FixedEffect(a, b, ...)`` groups observations by the tuple of keys, like
     ``GroupedArray(args..., sort=nothing)`` (src/FixedEffect.jl:18-21); ids
     are assigned in ascending key order.  ``interaction=None`` is the
-    reference's UnitWeights.
+    reference's UnitWeights.  ``device=d`` groups integer keys on GPU ``d``
+    (fe_group_keys: presence flags or a radix sort); otherwise the grouping
+    runs in numpy on the host, where the reference runs it too.
     """
 
     __slots__ = ("refs", "interaction", "n")
 
-    def __init__(self, *args, interaction=None):
+    def __init__(self, *args, interaction=None, device: int | None = None):
         if not args:
             raise ValueError("FixedEffect needs at least one key vector")
-        if len(args) == 1:
+        if device is not None:
+            refs, n = group_keys(*args, device=device)
+        elif len(args) == 1:
             refs, n = _compact(args[0])
         else:
             cols = [_compact(a)[0] for a in args]
@@ -539,6 +567,17 @@ class BatchSolver:
 
     def set_option(self, option: int, value: float) -> None:
         _lib.check(_lib.load().fe_plan_set_option(self._h, option, float(value)))
+
+    def integer_plan(self):
+        """(perm0, offsets[k], segperm[k]) over the concatenated problems;
+        level k ids are numbered problem after problem."""
+        nl = self._nlev.sum(axis=0)
+        perm0 = np.zeros(self.N, dtype=np.int32)
+        offs = [np.zeros(int(n) + 1, dtype=np.int64) for n in nl]
+        segs = [np.zeros(self.N, dtype=np.int32) for _ in range(self.K)]
+        _lib.check(_lib.load().fe_plan_get_integer_plan(
+            self._h, perm0.ctypes.data_as(_lib._i32p), _ptrs(offs), _ptrs(segs)))
+        return perm0, offs, segs
 
     def close(self):
         h = getattr(self, "_h", None)

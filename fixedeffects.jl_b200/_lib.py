@@ -47,7 +47,7 @@ EXPORTS = (
     "fe_solve_coefficients", "fe_plan_problem_results", "fe_plan_last_solve_info",
     "fe_plan_get_integer_plan", "fe_plan_get_scales", "fe_plan_primary",
     "fe_plan_kernel_stat", "fe_plan_reset_stats", "fe_plan_scales_noalloc",
-    "fe_normalize_coefficients", "fe_full_coefficients",
+    "fe_normalize_coefficients", "fe_full_coefficients", "fe_group_keys",
 )
 
 _i64p = ctypes.POINTER(ctypes.c_int64)
@@ -113,6 +113,8 @@ def load(path: Path | str | None = None):
         "fe_plan_scales_noalloc": (ctypes.c_int, [_vp, ctypes.c_int32, _vp, _vp]),
         "fe_normalize_coefficients": (ctypes.c_int, [_vp, _vpp, ctypes.c_int32]),
         "fe_full_coefficients": (ctypes.c_int, [_vp, _vpp, ctypes.c_int32, _vpp, ctypes.c_int32]),
+        "fe_group_keys": (ctypes.c_int, [_vpp, ctypes.c_int32, ctypes.c_int64, ctypes.c_int32,
+                                         _i64p, _i64p]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

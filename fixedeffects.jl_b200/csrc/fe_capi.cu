@@ -383,10 +383,6 @@ int fe_plan_get_integer_plan(fe_plan* plan, int32_t* perm0, int64_t* const* offs
                              int32_t* const* segperm) {
   int st = check_plan(plan);
   if (st) return st;
-  if (plan->nprob != 1) {
-    set_error("integer plan export is defined for single-problem plans");
-    return FE_ERR_INVALID;
-  }
   cudaSetDevice(plan->device);
   const int64_t N = plan->N;
   if (perm0 && N > 0) {

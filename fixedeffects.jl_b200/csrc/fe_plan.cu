@@ -1,5 +1,6 @@
-// fe_plan.cu -- plan construction: validation, the integer plan (stable
-// counting sorts), work items, and the Jacobi preconditioner on the device.
+// fe_plan.cu -- plan construction: argument checks, work items, and the
+// Jacobi preconditioner on the device (the integer plan is built in
+// fe_build.cu).
 //
 // Replaces the solver constructor and update_weights! of the reference's CUDA
 // backend (ext/CUDAExt.jl:99-121) and of the CPU backend
@@ -99,19 +100,8 @@ __global__ void k_cwp(const double* __restrict__ cw_d, const int32_t* __restrict
 static inline unsigned grid1(int64_t n, int b = 256) { return (unsigned)((n + b - 1) / b); }
 
 // ---------------------------------------------------------------------------
-// integer plan
+// the solver constructor
 // ---------------------------------------------------------------------------
-// Stable counting sort of keys[0..n) with values in [0, nb): the restatement
-// of bucketize_refs (ext/MetalExt.jl:40-64) with 0-based positions.
-static void counting_sort(const int32_t* key, int64_t n, int64_t nb, std::vector<int64_t>& off,
-                          int32_t* perm, int64_t base_pos) {
-  off.assign((size_t)nb + 1, 0);
-  for (int64_t i = 0; i < n; ++i) off[(size_t)key[i] + 1] += 1;
-  for (int64_t l = 0; l < nb; ++l) off[(size_t)l + 1] += off[(size_t)l];
-  std::vector<int64_t> next(off.begin(), off.end() - 1);
-  for (int64_t i = 0; i < n; ++i) perm[next[(size_t)key[i]]++] = (int32_t)(base_pos + i);
-}
-
 int plan_build(fe_plan* pl, int32_t nprob, const int64_t* n_obs, int32_t K,
                const int64_t* const* refs, const int64_t* n_levels,
                const double* const* interaction, const double* weights, int32_t device) {
@@ -171,21 +161,6 @@ int plan_build(fe_plan* pl, int32_t nprob, const int64_t* n_obs, int32_t K,
       return 1;
     }
   }
-  for (int p = 0; p < nprob; ++p) {
-    const int64_t o0 = pl->prob_obs_off[p], o1 = pl->prob_obs_off[p + 1];
-    for (int k = 0; k < K; ++k) {
-      const int64_t nl = n_levels[(int64_t)p * K + k];
-      const int64_t* r = refs[k];
-      for (int64_t i = o0; i < o1; ++i) {
-        const int64_t v = r[i];
-        if (nl == 0 ? (v != 0) : (v < 1 || v > nl)) {
-          set_error("plan: refs[" + std::to_string(k) + "][" + std::to_string(i) + "] = " +
-                    std::to_string(v) + " is outside 1.." + std::to_string(nl));
-          return 1;
-        }
-      }
-    }
-  }
   // primary FE: the one with the most levels (its observations become
   // contiguous, so its expand and reduce stream through memory)
   pl->primary = 0;
@@ -197,88 +172,16 @@ int plan_build(fe_plan* pl, int32_t nprob, const int64_t* n_obs, int32_t K,
     FE_CK(cudaStreamCreateWithFlags(&pl->stream, cudaStreamNonBlocking));
     pl->own_stream = true;
   }
-  cudaStream_t s = pl->stream;
 
-  // sorted observation order: stable sort of each problem by its primary level
-  std::vector<int32_t> obs_src((size_t)N), obs_dst((size_t)N);
-  {
-    std::vector<int32_t> key;
-    std::vector<int64_t> off;
-    const int kp = pl->primary;
-    for (int p = 0; p < nprob; ++p) {
-      const int64_t o0 = pl->prob_obs_off[p], o1 = pl->prob_obs_off[p + 1], n = o1 - o0;
-      const int64_t nl = n_levels[(int64_t)p * K + kp];
-      if (nl == 0) {
-        for (int64_t i = 0; i < n; ++i) obs_src[(size_t)(o0 + i)] = (int32_t)(o0 + i);
-        continue;
-      }
-      key.resize((size_t)n);
-      for (int64_t i = 0; i < n; ++i) key[(size_t)i] = (int32_t)(refs[kp][o0 + i] - 1);
-      counting_sort(key.data(), n, nl, off, obs_src.data() + o0, o0);
-    }
-    for (int64_t q = 0; q < N; ++q) obs_dst[(size_t)obs_src[(size_t)q]] = (int32_t)q;
-  }
-  int st = upload(pl->d_obs_src, obs_src.data(), (size_t)N, s);
-  if (!st) st = upload(pl->d_obs_dst, obs_dst.data(), (size_t)N, s);
-  if (st) return st;
-
-  // per-FE sorted refs (global level ids; the null level nlev[k] for problems
-  // without that FE) and the level order over sorted positions
+  // level ids are validated on the device (plan_build_device)
   pl->lev_base.assign(K, 0);
   pl->P = 0;
   for (int k = 0; k < K; ++k) {
     pl->lev_base[k] = pl->P;
     pl->P += pl->nlev[k] + 1;
   }
-  pl->d_refs.resize(K);
-  pl->d_perm.resize(K);
-  pl->d_key.resize(K);
-  pl->perm_identity.assign(K, false);
-  pl->seg_off.assign(K, {});
-  pl->seg_len.assign(K, 0);
-  std::vector<int32_t> rs((size_t)N), perm((size_t)N), keyv((size_t)N);
-  for (int k = 0; k < K; ++k) {
-    for (int p = 0; p < nprob; ++p) {
-      const int64_t o0 = pl->prob_obs_off[p], o1 = pl->prob_obs_off[p + 1];
-      const int64_t nl = n_levels[(int64_t)p * K + k];
-      const int64_t lb = pl->prob_lev_off[(size_t)p * K + k];
-      for (int64_t q = o0; q < o1; ++q) {
-        const int64_t orig = obs_src[(size_t)q];
-        rs[(size_t)q] = nl == 0 ? (int32_t)pl->nlev[k] : (int32_t)(lb + refs[k][orig] - 1);
-      }
-    }
-    // counting sort over nlev+1 buckets; the null bucket comes last and is
-    // excluded from the level order
-    std::vector<int64_t>& off = pl->seg_off[k];
-    counting_sort(rs.data(), N, pl->nlev[k] + 1, off, perm.data(), 0);
-    const int64_t npos = off[(size_t)pl->nlev[k]];
-    pl->seg_len[k] = npos;
-    bool ident = (npos == N);
-    for (int64_t q = 0; q < npos && ident; ++q) ident = (perm[(size_t)q] == (int32_t)q);
-    pl->perm_identity[k] = ident;
-    for (int64_t l = 0; l < pl->nlev[k]; ++l)
-      for (int64_t q = off[(size_t)l]; q < off[(size_t)l + 1]; ++q) keyv[(size_t)q] = (int32_t)l;
-    st = upload(pl->d_refs[k], rs.data(), (size_t)N, s);
-    if (!st) st = upload(pl->d_key[k], keyv.data(), (size_t)npos, s);
-    if (!st && !ident) st = upload(pl->d_perm[k], perm.data(), (size_t)npos, s);
-    if (st) return st;
-    FE_CK(cudaStreamSynchronize(s));  // host vectors are reused
-  }
-
-  // interactions in sorted order
-  pl->interacted.assign(K, false);
-  pl->d_inter_sorted.resize(K);
-  {
-    std::vector<double> tmp((size_t)N);
-    for (int k = 0; k < K; ++k) {
-      if (!interaction || !interaction[k]) continue;
-      pl->interacted[k] = true;
-      for (int64_t q = 0; q < N; ++q) tmp[(size_t)q] = interaction[k][obs_src[(size_t)q]];
-      st = upload(pl->d_inter_sorted[k], tmp.data(), (size_t)N, s);
-      if (st) return st;
-      FE_CK(cudaStreamSynchronize(s));
-    }
-  }
+  int st = plan_build_device(pl, refs, n_levels, interaction);
+  if (st) return st;
   pl->d_scale_d.resize(K);
   pl->d_scale_f.resize(K);
   pl->d_cw_d.resize(K);

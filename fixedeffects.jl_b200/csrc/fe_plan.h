@@ -168,6 +168,9 @@ int plan_build(fe_plan* pl, int32_t nprob, const int64_t* n_obs, int32_t K,
                const int64_t* const* refs, const int64_t* n_levels,
                const double* const* interaction, const double* weights, int32_t device);
 int plan_update_weights(fe_plan* pl, const double* weights);
+// the integer plan and the interactions in sorted order, built on the device
+int plan_build_device(fe_plan* pl, const int64_t* const* refs, const int64_t* n_levels,
+                      const double* const* interaction);
 int plan_items(fe_plan* pl, int C, ItemSet** out);
 int plan_destroy(fe_plan* pl);
 }  // namespace fe

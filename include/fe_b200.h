@@ -91,9 +91,21 @@ int fe_version(void);
 const char* fe_last_error(void);
 
 /*
- * Builds a solver plan on `device`: validates refs, builds the integer plan
- * (stable counting sorts by level), uploads it, and computes the Jacobi
- * preconditioner on the GPU.
+ * Groups observation keys into fixed-effect level ids on `device`: the
+ * GroupedArray compaction behind FixedEffect(keys...) (src/FixedEffect.jl:18-21).
+ * keys[j] holds n int64 keys (host memory); refs_out[i] (host, n values)
+ * becomes the 1-based rank of observation i's key tuple among the distinct
+ * tuples in lexicographic ascending order, and *n_levels_out the number of
+ * distinct tuples.  Dense key ranges use presence flags and a prefix sum,
+ * others a radix sort.
+ */
+int fe_group_keys(const int64_t* const* keys, int32_t n_keys, int64_t n, int32_t device,
+                  int64_t* refs_out, int64_t* n_levels_out);
+
+/*
+ * Builds a solver plan on `device`: uploads the refs, validates them, builds
+ * the integer plan on the GPU (stable radix sorts by level, the same order as
+ * stable counting sorts), and computes the Jacobi preconditioner on the GPU.
  * Replaces AbstractFixedEffectSolver{T}(fes, w, Val{:CUDA})
  * (ext/CUDAExt.jl:99-110) and its update_weights! (ext/CUDAExt.jl:112-121);
  * CPU counterpart src/SolverCPU.jl:55-95.
@@ -186,11 +198,15 @@ int fe_plan_last_solve_info(fe_plan* plan, int64_t ncols, double* test2, int32_t
                             int64_t* lsmr_iters);
 
 /*
- * The integer plan (single-problem plans), for bit-exact checks against the
- * stable counting sort of ext/MetalExt.jl:40-64 (bucketize_refs):
+ * The integer plan, for bit-exact checks against the stable counting sort of
+ * ext/MetalExt.jl:40-64 (bucketize_refs):
  *   perm0[p]      original observation (0-based) at sorted position p
  *   offsets[k]    n_levels[k]+1 level offsets into FE k's level order
  *   segperm[k][q] sorted position of entry q of FE k's level order
+ * For a batch plan the observations are sorted problem by problem (each by
+ * its primary level; a problem without the primary FE keeps its order),
+ * n_levels[k] is the total over problems, levels are numbered problem after
+ * problem, and FE k's level order leaves out the problems without FE k.
  * Any output pointer may be NULL.
  */
 int fe_plan_get_integer_plan(fe_plan* plan, int32_t* perm0, int64_t* const* offsets,
