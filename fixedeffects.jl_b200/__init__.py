@@ -245,19 +245,14 @@ class FixedEffectSolverB200:
         if _is_cuda_tensor(y):
             return self._solve_device(y, tol, maxiter)
         if isinstance(y, (list, tuple)):
-            out_its, out_cv = [], []
-            for col in y:
-                _, it, cv = self.solve_residuals(col, tol=tol, maxiter=maxiter)
-                out_its.append(it)
-                out_cv.append(cv)
-            return y, out_its, out_cv
+            return self._solve_columns(y, tol, maxiter)
         a = np.asarray(y)
         vec = a.ndim == 1
         if a.shape[0] != self.N:
             raise ValueError("FixedEffects must have the same length as y")
         if a.dtype not in (np.float64, np.float32):
             a = a.astype(np.float64)
-        work = a if (a.flags.f_contiguous and a.flags.writeable) else np.asfortranarray(a)
+        work = a if (a.flags.f_contiguous and a.flags.writeable) else np.array(a, order="F")
         if vec:
             work = work.reshape(-1, 1, order="F")
         ncols = work.shape[1]
@@ -274,6 +269,39 @@ class FixedEffectSolverB200:
         if vec:
             return res, int(its[0]), bool(cvs[0])
         return res, its, cvs.astype(bool)
+
+    def _solve_columns(self, ys, tol, maxiter):
+        """The collection method (src/AbstractFixedEffectSolver.jl:74-97): all
+        columns in one batched call (fe_solve_residuals_columns), each solved
+        in place when it is a writable float32/float64 vector."""
+        cols = []
+        for c in ys:
+            a = np.asarray(c)
+            if a.ndim != 1 or a.shape[0] != self.N:
+                raise ValueError("FixedEffects must have the same length as y")
+            cols.append(a)
+        if not cols:
+            return ys, [], []
+        dt = np.float32 if all(a.dtype == np.float32 for a in cols) else np.float64
+        # read-only or non-contiguous columns are solved in a copy
+        work = [a if (a.dtype == dt and a.flags.c_contiguous and a.flags.writeable)
+                else np.array(a, dtype=dt, order="C") for a in cols]
+        its = np.zeros(len(work), dtype=np.int64)
+        cvs = np.zeros(len(work), dtype=np.uint8)
+        _lib.check(_lib.load().fe_solve_residuals_columns(
+            self._h, _ptrs(work), FE_DTYPE_F64 if dt == np.float64 else FE_DTYPE_F32, len(work),
+            self.precision, float(tol), int(maxiter), its.ctypes.data_as(_lib._i64p),
+            cvs.ctypes.data_as(_lib._u8p)))
+        out = list(ys) if isinstance(ys, tuple) else ys
+        for j, (a, w) in enumerate(zip(cols, work)):
+            if w is a:
+                continue
+            if (isinstance(ys[j], np.ndarray) and ys[j].flags.writeable
+                    and ys[j].dtype.kind == "f"):
+                ys[j][...] = w
+            elif isinstance(out, list):
+                out[j] = w
+        return out, [int(i) for i in its], [bool(c) for c in cvs]
 
     def _solve_device(self, y, tol, maxiter):
         import torch
@@ -332,8 +360,11 @@ class FixedEffectSolverB200:
 
     def normalize_coefficients(self, coefs):
         """normalize!(fecoefs, fes) on the device (src/FixedEffect.jl:106-135):
-        per-level FP64 coefficient arrays, normalized in place and returned."""
-        coefs = [np.ascontiguousarray(c, dtype=np.float64) for c in coefs]
+        per-level FP64 coefficient arrays, normalized in place and returned
+        (arrays that cannot be written in place are normalized in a copy)."""
+        coefs = [c if (isinstance(c, np.ndarray) and c.dtype == np.float64
+                       and c.flags.c_contiguous and c.flags.writeable)
+                 else np.array(c, dtype=np.float64) for c in coefs]
         _lib.check(_lib.load().fe_normalize_coefficients(self._h, _ptrs(coefs), 0))
         return coefs
 

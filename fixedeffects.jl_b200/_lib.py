@@ -48,6 +48,7 @@ EXPORTS = (
     "fe_plan_get_integer_plan", "fe_plan_get_scales", "fe_plan_primary",
     "fe_plan_kernel_stat", "fe_plan_reset_stats", "fe_plan_scales_noalloc",
     "fe_normalize_coefficients", "fe_full_coefficients", "fe_group_keys",
+    "fe_solve_residuals_columns",
 )
 
 _i64p = ctypes.POINTER(ctypes.c_int64)
@@ -115,6 +116,9 @@ def load(path: Path | str | None = None):
         "fe_full_coefficients": (ctypes.c_int, [_vp, _vpp, ctypes.c_int32, _vpp, ctypes.c_int32]),
         "fe_group_keys": (ctypes.c_int, [_vpp, ctypes.c_int32, ctypes.c_int64, ctypes.c_int32,
                                          _i64p, _i64p]),
+        "fe_solve_residuals_columns": (ctypes.c_int, [_vp, _vpp, ctypes.c_int32, ctypes.c_int64,
+                                                      ctypes.c_int32, ctypes.c_double,
+                                                      ctypes.c_int64, _i64p, _u8p]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

@@ -55,9 +55,80 @@ int create_common(fe_plan** out, int32_t nprob, const int64_t* n_obs, int32_t K,
   return FE_OK;
 }
 
-int solve_common(fe_plan* plan, void* Y, bool host, int32_t dtype, int64_t ncols, int64_t ld,
-                 int32_t precision, double tol, int64_t maxiter, int64_t* iterations,
-                 uint8_t* converged) {
+// Host columns of a solve, moved through the device staging buffer (the
+// columns side by side, leading dimension N).  Pinned columns: every tile's
+// upload is queued at once on an upload stream with one event per tile, the
+// tile's solve waits for its event, and its download runs on a download
+// stream once the solve is done, so transfers in both directions overlap the
+// solves of the other tiles.  Pageable columns are copied tile by tile on the
+// plan's stream.
+struct HostXfer {
+  fe_plan* pl = nullptr;
+  void* const* cols = nullptr;
+  size_t bytes = 0;  // per column
+  bool pinned = false;
+  cudaStream_t up = nullptr, down = nullptr;
+  std::vector<cudaEvent_t> ev;  // per tile: upload done, then solve done
+  std::vector<int64_t> tile0;   // first column of each tile
+  size_t tile = 0;
+  char* stage() const { return static_cast<char*>(pl->ws.ystage.p); }
+  ~HostXfer() {
+    if (up) cudaStreamSynchronize(up);
+    if (down) cudaStreamSynchronize(down);
+    for (cudaEvent_t e : ev) cudaEventDestroy(e);
+    if (up) cudaStreamDestroy(up);
+    if (down) cudaStreamDestroy(down);
+  }
+};
+
+int xfer_error(const char* what, cudaError_t e) {
+  (void)cudaGetLastError();
+  set_error(std::string(what) + ": " + cudaGetErrorString(e));
+  return FE_ERR_CUDA;
+}
+
+int xfer_before(void* ctx, int64_t col0, int nc) {
+  HostXfer& x = *static_cast<HostXfer*>(ctx);
+  cudaError_t e = cudaSuccess;
+  if (x.pinned) {
+    e = cudaStreamWaitEvent(x.pl->stream, x.ev[2 * x.tile], 0);
+  } else {
+    for (int j = 0; j < nc && e == cudaSuccess; ++j)
+      e = cudaMemcpyAsync(x.stage() + (size_t)(col0 + j) * x.bytes, x.cols[col0 + j], x.bytes,
+                          cudaMemcpyHostToDevice, x.pl->stream);
+  }
+  return e == cudaSuccess ? 0 : xfer_error("host to device copy failed", e);
+}
+
+int xfer_after(void* ctx, int64_t col0, int nc) {
+  HostXfer& x = *static_cast<HostXfer*>(ctx);
+  cudaError_t e = cudaSuccess;
+  cudaStream_t s = x.pl->stream;
+  if (x.pinned) {
+    e = cudaEventRecord(x.ev[2 * x.tile + 1], s);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(x.down, x.ev[2 * x.tile + 1], 0);
+    s = x.down;
+  }
+  for (int j = 0; j < nc && e == cudaSuccess; ++j)
+    e = cudaMemcpyAsync(x.cols[col0 + j], x.stage() + (size_t)(col0 + j) * x.bytes, x.bytes,
+                        cudaMemcpyDeviceToHost, s);
+  ++x.tile;
+  return e == cudaSuccess ? 0 : xfer_error("device to host copy failed", e);
+}
+
+bool is_pinned(const void* p) {
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    (void)cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeHost;
+}
+
+// Y: device matrix (cols == nullptr, leading dimension ld) or host columns.
+int solve_common(fe_plan* plan, void* Y, void* const* cols, int32_t dtype, int64_t ncols,
+                 int64_t ld, int32_t precision, double tol, int64_t maxiter,
+                 int64_t* iterations, uint8_t* converged) {
   int st = check_plan(plan);
   if (st) return st;
   if (dtype != FE_DTYPE_F64 && dtype != FE_DTYPE_F32) {
@@ -68,10 +139,17 @@ int solve_common(fe_plan* plan, void* Y, bool host, int32_t dtype, int64_t ncols
     set_error("precision must be FE_PREC_FP64, FE_PREC_MIXED or FE_PREC_FP32");
     return FE_ERR_INVALID;
   }
-  if (ncols < 0 || (ncols > 0 && !Y && plan->N > 0)) {
+  const bool host = cols != nullptr;
+  if (ncols < 0 || (ncols > 0 && !host && !Y && plan->N > 0)) {
     set_error("Y is NULL or ncols < 0");
     return FE_ERR_INVALID;
   }
+  if (host && plan->N > 0)
+    for (int64_t j = 0; j < ncols; ++j)
+      if (!cols[j]) {
+        set_error("column " + std::to_string(j) + " is NULL");
+        return FE_ERR_INVALID;
+      }
   if (ld < plan->N) {
     set_error("ld must be >= the number of observations");
     return FE_ERR_INVALID;
@@ -100,40 +178,58 @@ int solve_common(fe_plan* plan, void* Y, bool host, int32_t dtype, int64_t ncols
     return FE_ERR_CUDA;
   }
   const int64_t N = plan->N;
+  HostXfer x;
   if (host && N > 0) {
-    // stage through device memory: one 2D copy in, one out
     st = plan->ws.ystage.ensure((size_t)N * ncols * es);
     if (st) return st;
-    cudaError_t e = cudaMemcpy2DAsync(plan->ws.ystage.p, (size_t)N * es, Y, (size_t)ld * es,
-                                      (size_t)N * es, (size_t)ncols, cudaMemcpyHostToDevice,
-                                      plan->stream);
-    if (e != cudaSuccess) {
-      set_error(std::string("host to device copy failed: ") + cudaGetErrorString(e));
-      return FE_ERR_CUDA;
+    x.pl = plan;
+    x.cols = cols;
+    x.bytes = (size_t)N * es;
+    x.pinned = true;
+    for (int64_t j = 0; j < ncols && x.pinned; ++j) x.pinned = is_pinned(cols[j]);
+    if (x.pinned) {
+      for (int64_t c0 = 0; c0 < ncols; c0 += std::min<int64_t>(fe::tile_width(plan, ncols - c0),
+                                                                ncols - c0))
+        x.tile0.push_back(c0);
+      x.tile0.push_back(ncols);
+      cudaError_t e = cudaStreamCreateWithFlags(&x.up, cudaStreamNonBlocking);
+      if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&x.down, cudaStreamNonBlocking);
+      // the uploads must not overtake work already queued on the plan's
+      // stream that reads the staging buffer
+      cudaEvent_t start = nullptr;
+      if (e == cudaSuccess) e = cudaEventCreateWithFlags(&start, cudaEventDisableTiming);
+      if (e == cudaSuccess) e = cudaEventRecord(start, plan->stream);
+      if (e == cudaSuccess) e = cudaStreamWaitEvent(x.up, start, 0);
+      if (start) cudaEventDestroy(start);
+      for (size_t t = 0; t + 1 < x.tile0.size() && e == cudaSuccess; ++t) {
+        cudaEvent_t a = nullptr, b = nullptr;
+        e = cudaEventCreateWithFlags(&a, cudaEventDisableTiming);
+        if (e == cudaSuccess) x.ev.push_back(a);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b, cudaEventDisableTiming);
+        if (e == cudaSuccess) x.ev.push_back(b);
+        for (int64_t j = x.tile0[t]; j < x.tile0[t + 1] && e == cudaSuccess; ++j)
+          e = cudaMemcpyAsync(x.stage() + (size_t)j * x.bytes, cols[j], x.bytes,
+                              cudaMemcpyHostToDevice, x.up);
+        if (e == cudaSuccess) e = cudaEventRecord(a, x.up);
+      }
+      if (e != cudaSuccess) return xfer_error("host to device copy failed", e);
     }
     rq.Y = plan->ws.ystage.p;
     rq.ld = N;
+    rq.before_tile = xfer_before;
+    rq.after_tile = xfer_after;
+    rq.hook_ctx = &x;
   } else {
     rq.Y = Y;
     rq.ld = ld;
   }
   st = fe::solve(plan, rq);
   if (st) return st;
-  if (host && N > 0) {
-    cudaError_t e = cudaMemcpy2DAsync(Y, (size_t)ld * es, plan->ws.ystage.p, (size_t)N * es,
-                                      (size_t)N * es, (size_t)ncols, cudaMemcpyDeviceToHost,
-                                      plan->stream);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(plan->stream);
-    if (e != cudaSuccess) {
-      set_error(std::string("device to host copy failed: ") + cudaGetErrorString(e));
-      return FE_ERR_CUDA;
-    }
-  } else {
-    cudaError_t e = cudaStreamSynchronize(plan->stream);
-    if (e != cudaSuccess) {
-      set_error(std::string("stream synchronize failed: ") + cudaGetErrorString(e));
-      return FE_ERR_CUDA;
-    }
+  cudaError_t e = cudaStreamSynchronize(plan->stream);
+  if (e == cudaSuccess && x.down) e = cudaStreamSynchronize(x.down);
+  if (e != cudaSuccess) {
+    set_error(std::string("stream synchronize failed: ") + cudaGetErrorString(e));
+    return FE_ERR_CUDA;
   }
   return FE_OK;
 }
@@ -280,14 +376,37 @@ int fe_plan_destroy(fe_plan* plan) {
 int fe_solve_residuals(fe_plan* plan, void* Y, int32_t dtype, int64_t ncols, int64_t ld,
                        int32_t precision, double tol, int64_t maxiter, int64_t* iterations,
                        uint8_t* converged) {
-  return solve_common(plan, Y, true, dtype, ncols, ld, precision, tol, maxiter, iterations,
-                      converged);
+  int st = check_plan(plan);
+  if (st) return st;
+  if (ncols < 0 || (ncols > 0 && !Y && plan->N > 0)) {
+    set_error("Y is NULL or ncols < 0");
+    return FE_ERR_INVALID;
+  }
+  const size_t es = dtype == FE_DTYPE_F64 ? 8 : 4;
+  std::vector<void*> cols((size_t)ncols);
+  for (int64_t j = 0; j < ncols; ++j)
+    cols[(size_t)j] = Y ? static_cast<char*>(Y) + (size_t)j * (size_t)ld * es : nullptr;
+  return solve_common(plan, nullptr, cols.data(), dtype, ncols, ld, precision, tol, maxiter,
+                      iterations, converged);
+}
+
+int fe_solve_residuals_columns(fe_plan* plan, void* const* columns, int32_t dtype, int64_t ncols,
+                               int32_t precision, double tol, int64_t maxiter,
+                               int64_t* iterations, uint8_t* converged) {
+  int st = check_plan(plan);
+  if (st) return st;
+  if (ncols < 0 || (ncols > 0 && !columns)) {
+    set_error("columns is NULL or ncols < 0");
+    return FE_ERR_INVALID;
+  }
+  return solve_common(plan, nullptr, columns, dtype, ncols, plan->N, precision, tol, maxiter,
+                      iterations, converged);
 }
 
 int fe_solve_residuals_device(fe_plan* plan, void* Y_dev, int32_t dtype, int64_t ncols,
                               int64_t ld, int32_t precision, double tol, int64_t maxiter,
                               int64_t* iterations, uint8_t* converged) {
-  return solve_common(plan, Y_dev, false, dtype, ncols, ld, precision, tol, maxiter, iterations,
+  return solve_common(plan, Y_dev, nullptr, dtype, ncols, ld, precision, tol, maxiter, iterations,
                       converged);
 }
 

@@ -115,7 +115,7 @@ void tune_cache_store(fe_plan* pl, int C, int sT, int ex, int seg) {
   if (f) f << tune_signature(pl) << " " << C << " " << sT << " " << ex << " " << seg << "\n";
 }
 
-static int tile_width(const fe_plan* pl, int64_t remaining) {
+int tile_width(const fe_plan* pl, int64_t remaining) {
   int cmax = 32;
   if (pl->opt_tile > 0) cmax = pl->opt_tile;
   int64_t want = std::min<int64_t>(remaining, cmax);
@@ -142,6 +142,7 @@ int solve(fe_plan* pl, const SolveReq& rq) {
     const int C = tile_width(pl, ncols - col0);
     const int nc = (int)std::min<int64_t>(C, ncols - col0);
     int st;
+    if (rq.before_tile && (st = rq.before_tile(rq.hook_ctx, col0, nc))) return st;
     switch (C) {
       case 1: st = solve_tile_C<1>(pl, rq, col0, nc, res); break;
       case 2: st = solve_tile_C<2>(pl, rq, col0, nc, res); break;
@@ -151,6 +152,7 @@ int solve(fe_plan* pl, const SolveReq& rq) {
       default: st = solve_tile_C<32>(pl, rq, col0, nc, res); break;
     }
     if (st) return st;
+    if (rq.after_tile && (st = rq.after_tile(rq.hook_ctx, col0, nc))) return st;
     // per-column verdicts: a column's instances are (problem p, column j);
     // with several problems the column aggregates them (max iterations, all
     // converged).  Single-problem plans report the instance itself.

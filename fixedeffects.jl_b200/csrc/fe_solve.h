@@ -21,8 +21,16 @@ struct SolveReq {
   int64_t* prob_iters = nullptr;     // optional [nprob][ncols]
   uint8_t* prob_converged = nullptr; // optional [nprob][ncols]
   double* const* coefs = nullptr;    // host, per FE (coefficients mode)
+  // optional per-tile hooks on the host (transfers of host buffers overlapped
+  // with the solve): before_tile runs before a tile's first launch is
+  // enqueued, after_tile after its last; a non-zero return aborts the solve
+  int (*before_tile)(void* ctx, int64_t col0, int ncols) = nullptr;
+  int (*after_tile)(void* ctx, int64_t col0, int ncols) = nullptr;
+  void* hook_ctx = nullptr;
 };
 
+// column-tile width of the next tile when `remaining` columns are left
+int tile_width(const fe_plan* pl, int64_t remaining);
 int solve(fe_plan* pl, const SolveReq& rq);
 int prof_flush(fe_plan* pl);
 

@@ -153,6 +153,9 @@ int fe_plan_destroy(fe_plan* plan);
  * tests passed).  With several problems a column reports the maximum
  * iterations and the conjunction of convergence flags over problems
  * (fe_plan_problem_results gives them per problem).
+ * Host transfers: with pinned (page-locked) columns the uploads and downloads
+ * of each 32-column tile overlap the solves of the other tiles; pageable
+ * columns are copied tile by tile.
  */
 int fe_solve_residuals(fe_plan* plan, void* Y, int32_t dtype, int64_t ncols, int64_t ld,
                        int32_t precision, double tol, int64_t maxiter, int64_t* iterations,
@@ -162,6 +165,18 @@ int fe_solve_residuals(fe_plan* plan, void* Y, int32_t dtype, int64_t ncols, int
 int fe_solve_residuals_device(fe_plan* plan, void* Y_dev, int32_t dtype, int64_t ncols,
                               int64_t ld, int32_t precision, double tol, int64_t maxiter,
                               int64_t* iterations, uint8_t* converged);
+
+/*
+ * solve_residuals!(xs::AbstractVector{<:AbstractVector}, feM; tol, maxiter)
+ * (src/AbstractFixedEffectSolver.jl:74-97), the collection form that
+ * FixedEffectModels.jl calls: columns[j] is a separate host vector of n_obs
+ * values, solved in place.  The columns are batched like the columns of a
+ * matrix (fe_solve_residuals), with no host-side gathering into one matrix;
+ * results as fe_solve_residuals.
+ */
+int fe_solve_residuals_columns(fe_plan* plan, void* const* columns, int32_t dtype, int64_t ncols,
+                               int32_t precision, double tol, int64_t maxiter,
+                               int64_t* iterations, uint8_t* converged);
 
 /*
  * solve_coefficients!(y, feM; tol, maxiter) up to, not including, the
