@@ -492,6 +492,50 @@ def run_plan_build(args):
     return 0
 
 
+def run_host_columns(args):
+    """Times one host-buffer solve of args.host_columns columns of the 10M
+    workload (several 32-column tiles) from pageable and from pinned host
+    memory (tile-pipelined transfers), next to the device-resident solve.
+    Wall clock per call, best of two after a warm-up; prints one JSON line."""
+    import torch
+    torch.cuda.set_device(0)
+    import __graft_entry__ as g
+    fe = g.load_package()
+    import fe_b200.synth as S
+    ncols = args.host_columns
+    pb = S.config2(scale=args.scale, ncols=ncols)
+    fes = [fe.FixedEffect.from_refs(r, n) for r, n in zip(pb.refs, pb.nlev)]
+    feM = fe.AbstractFixedEffectSolver(fes, None, "CUDA", np.float32, precision="mixed")
+    Y = np.asfortranarray(pb.Y)
+    N = Y.shape[0]
+    P = torch.empty((ncols, N), dtype=torch.float32, pin_memory=True).numpy().T
+    D = torch.from_numpy(np.ascontiguousarray(Y.T)).cuda().t()
+
+    def timed(kind):
+        if kind == "device":
+            A = D.clone().t().contiguous().t()
+        elif kind == "pinned":
+            P[...] = Y
+            A = P
+        else:
+            A = Y.copy(order="F")
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        feM.solve_residuals(A, tol=1e-8, maxiter=10000)
+        torch.cuda.synchronize()
+        return time.perf_counter() - t
+
+    timed("pageable")  # warm-up: tuning, graphs, staging
+    out = {"metric": "host-buffer solve time", "unit": "s", "higher_is_better": False,
+           "data": "synthetic", "config": {"workload": "worker_firm_year_10m", "N": N,
+                                           "columns": ncols, "precision": "mixed", "tol": 1e-8}}
+    for kind in ("device", "pinned", "pageable"):
+        out[kind + "_s"] = round(min(timed(kind) for _ in range(2)), 4)
+    feM.close()
+    print(json.dumps(out), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -507,7 +551,11 @@ def main():
                     help="time every expand/segsum kernel variant and print a table")
     ap.add_argument("--plan-build", action="store_true",
                     help="time plan construction and key grouping, device vs host")
+    ap.add_argument("--host-columns", type=int, default=0,
+                    help="time a host-buffer solve of this many columns: pageable, pinned, device")
     args = ap.parse_args()
+    if args.host_columns:
+        return run_host_columns(args)
     if args.plan_build:
         return run_plan_build(args)
     if args.sweep_variants:
