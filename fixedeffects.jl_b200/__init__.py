@@ -419,7 +419,12 @@ class FixedEffectSolverB200:
             if L.fe_plan_kernel_stat(self._h, i, buf, 64, ctypes.byref(n), ctypes.byref(ms),
                                      ctypes.byref(by)) != 0:
                 break
-            out[buf.value.decode()] = {"launches": n.value, "ms": ms.value, "bytes": by.value}
+            t = np.zeros(max(n.value, 1), dtype=np.float32)
+            m = ctypes.c_int64(0)
+            _lib.check(L.fe_plan_kernel_times(self._h, i, t.ctypes.data_as(ctypes.POINTER(ctypes.c_float)),
+                                              t.size, ctypes.byref(m)))
+            out[buf.value.decode()] = {"launches": n.value, "ms": ms.value, "bytes": by.value,
+                                       "times_ms": t[:m.value].astype(np.float64)}
             i += 1
         return out
 

@@ -48,7 +48,7 @@ EXPORTS = (
     "fe_plan_get_integer_plan", "fe_plan_get_scales", "fe_plan_primary",
     "fe_plan_kernel_stat", "fe_plan_reset_stats", "fe_plan_scales_noalloc",
     "fe_normalize_coefficients", "fe_full_coefficients", "fe_group_keys",
-    "fe_solve_residuals_columns",
+    "fe_solve_residuals_columns", "fe_plan_kernel_times",
 )
 
 _i64p = ctypes.POINTER(ctypes.c_int64)
@@ -111,6 +111,9 @@ def load(path: Path | str | None = None):
         "fe_plan_kernel_stat": (ctypes.c_int, [_vp, ctypes.c_int32, ctypes.c_char_p,
                                                ctypes.c_int64, _i64p, _f64p, _f64p]),
         "fe_plan_reset_stats": (ctypes.c_int, [_vp]),
+        "fe_plan_kernel_times": (ctypes.c_int, [_vp, ctypes.c_int32,
+                                                ctypes.POINTER(ctypes.c_float), ctypes.c_int64,
+                                                _i64p]),
         "fe_plan_scales_noalloc": (ctypes.c_int, [_vp, ctypes.c_int32, _vp, _vp]),
         "fe_normalize_coefficients": (ctypes.c_int, [_vp, _vpp, ctypes.c_int32]),
         "fe_full_coefficients": (ctypes.c_int, [_vp, _vpp, ctypes.c_int32, _vpp, ctypes.c_int32]),

@@ -574,6 +574,24 @@ int fe_plan_kernel_stat(fe_plan* plan, int32_t index, char* name, int64_t name_l
   return FE_OK;
 }
 
+int fe_plan_kernel_times(fe_plan* plan, int32_t index, float* ms, int64_t max_launches,
+                         int64_t* launches) {
+  int st = check_plan(plan);
+  if (st) return st;
+  fe::prof_flush(plan);
+  if (index < 0 || index >= (int32_t)plan->prof.stats.size()) {
+    set_error("kernel stat index out of range");
+    return FE_ERR_INVALID;
+  }
+  auto it = plan->prof.stats.begin();
+  std::advance(it, index);
+  const std::vector<float>& t = it->second.times;
+  if (launches) *launches = (int64_t)t.size();
+  if (ms && max_launches > 0)
+    std::copy(t.begin(), t.begin() + std::min<int64_t>(max_launches, (int64_t)t.size()), ms);
+  return FE_OK;
+}
+
 int fe_plan_reset_stats(fe_plan* plan) {
   int st = check_plan(plan);
   if (st) return st;

@@ -190,6 +190,7 @@ struct KernelStat {
   int64_t launches = 0;
   double ms = 0.0;
   double bytes = 0.0;  // algorithmic bytes
+  std::vector<float> times;  // CUDA-event milliseconds of every launch
 };
 
 }  // namespace fe

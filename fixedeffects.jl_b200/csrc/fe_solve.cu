@@ -35,6 +35,7 @@ int prof_flush(fe_plan* pl) {
     st.name = pr.first;
     st.launches += 1;
     st.ms += ms;
+    st.times.push_back(ms);
     st.bytes += pl->prof.bytes_per_launch[pr.first];
     pl->prof.pool.push_back(pr.second.first);
     pl->prof.pool.push_back(pr.second.second);

@@ -238,6 +238,12 @@ int fe_plan_primary(fe_plan* plan, int32_t* primary);
  * FE_ERR_INVALID past the last kernel. */
 int fe_plan_kernel_stat(fe_plan* plan, int32_t index, char* name, int64_t name_len,
                         int64_t* launches, double* total_ms, double* alg_bytes);
+/* The CUDA-event milliseconds of each launch of kernel `index` (FE_OPT_PROFILE),
+ * in launch order: up to max_launches values into ms, the count in *launches.
+ * Launches that found every instance stopped return at once, so the typical
+ * working launch is read off this list rather than the mean. */
+int fe_plan_kernel_times(fe_plan* plan, int32_t index, float* ms, int64_t max_launches,
+                         int64_t* launches);
 int fe_plan_reset_stats(fe_plan* plan);
 
 /*
