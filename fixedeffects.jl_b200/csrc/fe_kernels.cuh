@@ -1169,59 +1169,17 @@ k_demean(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_items, c
 //            (Shape<T, 32>):  LSMR   w = av * (A_r v) + au * u_old
 //                             RESID  w = b - A_r x            (FP64)
 //            staged in a per-warp shared buffer;
-//   phase B: one column per lane: the level sums z_l = sum cw w, then
+//   phase B: B1 the level sums z_l = sum cw w (vector layout); B2
 //            u = w - cw scale_l^2 z_l stored once (LSMR: u in place; RESID:
-//            the FP64 residual and its FP32 copy), ||u||^2 per column into
-//            the CTA's norm slot, and the small FEs' sums of cw u into the
-//            per-warp tables (as k_rowsum).
+//            the FP64 residual and its FP32 copy) and ||u||^2 per column
+//            into the CTA's norm slot; B3 the small FEs' sums of cw u into
+//            the per-warp tables, one column per lane (as k_rowsum).
 // A level longer than kDemeanRows rows is processed in chunks: phase A writes
 // w to the row buffer and accumulates z, then a second walk finalizes it.
 // RESID, mask: columns whose refinement has stopped keep their stored rows.
+// PRE: tab holds scale_l * v_l (the P-side update stores that copy), so phase
+// A skips the per-row load of the scale.
 // ---------------------------------------------------------------------------
-// Small-FE table update by the G row groups of one warp instruction (row
-// group g holds row r_g's values u, VEC columns per lane): rows whose table
-// row (key) appeared in an earlier group are added into that group first, so
-// the remaining groups hit distinct table rows and update them in one
-// load/add/store.  key >= 0 for a valid row.
-template <typename T, int C, int VEC, int CL, int G>
-__device__ __forceinline__ void vec_table_update(T* tbl, int key, bool valid, VA<T, VEC> u, int g,
-                                                 int jl, int lane) {
-  const int mine = valid ? key : -1 - g;  // invalid rows match nothing
-  int kg[G];
-#pragma unroll
-  for (int h = 0; h < G; ++h) kg[h] = __shfl_sync(FE_FULL, mine, h * CL);
-  int dup[G];
-#pragma unroll
-  for (int h = 0; h < G; ++h) {
-    dup[h] = -1;
-#pragma unroll
-    for (int i = h - 1; i >= 0; --i)
-      if (kg[i] == kg[h]) dup[h] = i;
-  }
-#pragma unroll
-  for (int j = 1; j < G; ++j)
-#pragma unroll
-    for (int i = 0; i < j; ++i)
-      if (dup[j] == i) {  // warp-uniform
-#pragma unroll
-        for (int v = 0; v < VEC; ++v) {
-          const T o = __shfl_sync(FE_FULL, u.v[v], (lane + (j - i) * CL) & 31);
-          if (g == i) u.v[v] += o;
-        }
-      }
-  bool mydup = false;
-#pragma unroll
-  for (int h = 0; h < G; ++h)
-    if (h == g) mydup = dup[h] >= 0;
-  if (valid && !mydup) {
-    T* p = tbl + (int64_t)key * C + jl * VEC;
-    VA<T, VEC> a = vld<T, VEC>(p);
-#pragma unroll
-    for (int v = 0; v < VEC; ++v) a.v[v] += u.v[v];
-    vst<T, VEC>(p, a);
-  }
-}
-
 __device__ __forceinline__ void prefetch_l2(const void* p) {
   asm volatile("prefetch.global.L2 [%0];\n" ::"l"(p));
 }
@@ -1232,7 +1190,7 @@ struct ExDmCoef {
   bool act[VEC];  // the column's rows may be written
 };
 
-template <typename T, int C, int U, int KB, bool RESID, bool W, int NS, class Tab>
+template <typename T, int C, int U, int KB, bool RESID, bool W, int NS, class Tab, bool PRE>
 __global__ void __launch_bounds__(kThreads, 2)
 k_expand_demean(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_items, Tab tab,
                 T* __restrict__ rows, const double* __restrict__ B, float* __restrict__ rows32,
@@ -1331,7 +1289,7 @@ k_expand_demean(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_i
             const int ref = __shfl_sync(FE_FULL, rl[k], b0 + q);
             const T c = wk ? __shfl_sync(FE_FULL, cl[k], b0 + q) : T(1);
             if (b0 + q < cn) {
-              const T scl = __ldg(sc + ref);
+              const T scl = PRE ? T(1) : __ldg(sc + ref);
               const T cs = wk ? c * scl : scl;
               const VA<T, VEC> t = tab.load((lb + ref) * C + jl * VEC);
 #pragma unroll
@@ -1481,7 +1439,7 @@ k_expand_demean(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_i
         if (okj) vst<T, VEC>(zs + j * C + jl * VEC, acc);
       }
       __syncwarp();
-      // B2: u = w - cw scale^2 z, stored once; norms; small-FE tables
+      // B2: u = w - cw scale^2 z, stored once; norms
       VA<T, VEC> nvi;
 #pragma unroll
       for (int v = 0; v < VEC; ++v) nvi.v[v] = T(0);
@@ -1510,29 +1468,25 @@ k_expand_demean(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_i
 #pragma unroll
             for (int v = 0; v < VEC; ++v) nvi.v[v] += u.v[v] * u.v[v];
           }
-        } else {
-#pragma unroll
-          for (int v = 0; v < VEC; ++v) u.v[v] = T(0);
-        }
-        if (NS > 0) {
-          const int k0r = __shfl_sync(FE_FULL, rd.k0, r);
-          const T c0r = W ? __shfl_sync(FE_FULL, rd.c0, r) : T(1);
-          VA<T, VEC> u0 = u;
-#pragma unroll
-          for (int v = 0; v < VEC; ++v) u0.v[v] *= c0r;
-          vec_table_update<T, C, VEC, CL, G>(tbl, k0r, ok, u0, g, jl, lane);
-          if (NS > 1) {
-            const int k1r = __shfl_sync(FE_FULL, rd.k1, r);
-            const T c1r = W ? __shfl_sync(FE_FULL, rd.c1, r) : T(1);
-            VA<T, VEC> u1 = u;
-#pragma unroll
-            for (int v = 0; v < VEC; ++v) u1.v[v] *= c1r;
-            vec_table_update<T, C, VEC, CL, G>(tbl, k1r, ok, u1, g, jl, lane);
-          }
+          if (NS > 0) vst<T, VEC>(ub + r * C + jl * VEC, u);  // for B3
         }
       }
 #pragma unroll
       for (int v = 0; v < VEC; ++v) nrmv[v] += (double)nvi.v[v];
+      // B3: small-FE sums of cw u, one column per lane: a row's table key is
+      // the same in every lane, so rows sharing a key are merged with uniform
+      // branches before the table rows are updated
+      if (NS > 0) {
+        __syncwarp();  // u rows in ub
+        for (int r0 = 0; r0 < n; r0 += 4) {
+          const T x0 = ub[r0 * C + lane];
+          const T x1 = r0 + 1 < n ? ub[(r0 + 1) * C + lane] : T(0);
+          const T x2 = r0 + 2 < n ? ub[(r0 + 2) * C + lane] : T(0);
+          const T x3 = r0 + 3 < n ? ub[(r0 + 3) * C + lane] : T(0);
+          rowsum_small4<T, C, W>(r0, x0, x1, x2, x3, rd.k0, rd.c0, tbl, lane);
+          if (NS > 1) rowsum_small4<T, C, W>(r0, x0, x1, x2, x3, rd.k1, rd.c1, tbl, lane);
+        }
+      }
       __syncwarp();  // ub, zs and lend are rewritten by the next item
       continue;
     }
@@ -1872,6 +1826,7 @@ struct PEpiLsmr {
   T* __restrict__ H;
   T* __restrict__ Hb;
   T* __restrict__ X;
+  T* __restrict__ VS;  // optional: v scaled by the Jacobi scale (the fused loop's table)
   const Inst* __restrict__ inst;
   T rd_acc[VEC], rd_v[VEC], s_v[VEC], c1[VEC], c2[VEC], c3[VEC];
   uint32_t upd_bits;  // 2 bits per column: deferred update mode
@@ -1935,6 +1890,12 @@ struct PEpiLsmr {
         }
       }
       vst<T, VEC>(V + o, vv);
+      if (VS) {
+        VA<T, VEC> vs;
+#pragma unroll
+        for (int v = 0; v < VEC; ++v) vs.v[v] = vv.v[v] * sc;
+        vst<T, VEC>(VS + o, vs);
+      }
     }
   }
 };
@@ -1967,6 +1928,7 @@ struct PEpiGrad64 {
   float* __restrict__ V32;
   double* __restrict__ X64;
   const float* __restrict__ X32;
+  float* __restrict__ VS32;  // optional: v scaled by the FP32 Jacobi scale
   const Inst* __restrict__ inst;
   bool actv[VEC];
   bool act;
@@ -1997,6 +1959,13 @@ struct PEpiGrad64 {
     }
     vst<float, VEC>(V32 + o, g32);
     vst<double, VEC>(X64 + o, x64);
+    if (VS32) {
+      const float sf = __ldg(d.scale_f[k] + l);
+      VA<float, VEC> vs;
+#pragma unroll
+      for (int v = 0; v < VEC; ++v) vs.v[v] = g32.v[v] * sf;
+      vst<float, VEC>(VS32 + o, vs);
+    }
   }
 };
 

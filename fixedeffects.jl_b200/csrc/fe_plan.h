@@ -75,6 +75,7 @@ struct ItemSet {
 struct Workspace {
   int C = 0;
   DevBuf B64, R64, U, V, H, Hb, X, X64, S;
+  DevBuf VS;  // scale * v, the fused absorbed loop's coefficient table (FP32)
   DevBuf part_e, part_a, part_b, piece_part, ex_piece_part, block_part, ex_block_part, inst,
       counters;
   DevBuf small_part;  // the row-sum CTA partials of the small FEs

@@ -403,7 +403,7 @@ static int launch_demean(Ctx& c, T* rows, float* rows32, T* out, const char* nam
 template <typename T, int C, int U, int KB, bool W, int NS, class Tab>
 static int exdm_launch(Ctx& c, Tab tab, T* rows) {
   if constexpr (C == 32) {
-    auto kern = k_expand_demean<T, C, U, KB, false, W, NS, Tab>;
+    auto kern = k_expand_demean<T, C, U, KB, false, W, NS, Tab, true>;
     const size_t smem =
         (size_t)kWarps * ((2 * kDemeanRows + c.its->small_rows) * C * sizeof(T) + 32 * sizeof(int));
     static bool attr_set = false;  // per instantiation
@@ -728,6 +728,7 @@ static int prepare(fe_plan* pl, int C, int sT, bool mixed, Ctx& c) {
   if ((st = w.R64.ensure(N * nC * 8))) return st;
   if ((st = w.U.ensure(N * nC * (size_t)sT))) return st;
   if ((st = w.V.ensure(P * nC * (size_t)sT))) return st;
+  if (mixed && (st = w.VS.ensure(P * nC * 4))) return st;
   if ((st = w.H.ensure(P * nC * (size_t)sT))) return st;
   if ((st = w.Hb.ensure(P * nC * (size_t)sT))) return st;
   if ((st = w.X.ensure(P * nC * (size_t)sT))) return st;
@@ -769,6 +770,7 @@ static int prepare(fe_plan* pl, int C, int sT, bool mixed, Ctx& c) {
   // coefficient-side slabs start at zero (levels without observations and
   // the null levels are never written afterwards)
   FE_CK(cudaMemsetAsync(w.V.p, 0, P * nC * (size_t)sT, c.s));
+  if (mixed) FE_CK(cudaMemsetAsync(w.VS.p, 0, P * nC * 4, c.s));
   FE_CK(cudaMemsetAsync(w.H.p, 0, P * nC * (size_t)sT, c.s));
   FE_CK(cudaMemsetAsync(w.Hb.p, 0, P * nC * (size_t)sT, c.s));
   FE_CK(cudaMemsetAsync(w.X.p, 0, P * nC * (size_t)sT, c.s));
@@ -860,7 +862,7 @@ static int run_loop(fe_plan* pl, Ctx& c, int prec, int64_t cap, int32_t nact0, B
     size_t key = (size_t)c.C * 1000003u ^ (size_t)m;
     const void* ptrs[] = {c.inst, c.part_e, c.part_a, c.part_b, c.piece, c.ex_piece, c.S,
                           c.block, c.ex_block, pl->ws.U.p, pl->ws.V.p, pl->ws.H.p, pl->ws.Hb.p,
-                          pl->ws.X.p, c.its, c.counters, c.s, c.small_part};
+                          pl->ws.X.p, c.its, c.counters, c.s, c.small_part, pl->ws.VS.p};
     for (const void* p : ptrs) key = key * 1315423911u + (size_t)p;
     // the variants the captured launches use (tuned, or forced by an option)
     for (size_t e : {(size_t)4, (size_t)8})
@@ -1191,6 +1193,11 @@ static int solve_mixed_tile(fe_plan* pl, const SolveReq& rq, int64_t col0, int n
   pg.X64 = X64;
   pg.X32 = X;
   pg.inst = c.inst;
+  // the fused absorbed loop gathers scale * v, kept beside v by both P-side
+  // updates
+  float* VS = (absorb && pl->opt_exdm) ? w.VS.as<float>() : nullptr;
+  pe.VS = VS;
+  pg.VS32 = VS;
   const int64_t cap = std::max<int64_t>(rq.maxiter, 1) + 2;
   int64_t total_it = 0;
   const bool fuse = c.rowsum;
@@ -1231,7 +1238,7 @@ static int solve_mixed_tile(fe_plan* pl, const SolveReq& rq, int64_t col0, int n
         // u = M (av A_r v + au u): the expand without the primary FE, then the
         // projection (which also gives ||u|| and the small FEs' sums)
         if (pl->opt_exdm) {
-          if ((e = launch_expand_demean<float, C>(c, TabOne<float, float, vec_of<float, C>()>{V}, U,
+          if ((e = launch_expand_demean<float, C>(c, TabOne<float, float, vec_of<float, C>()>{VS}, U,
                                                   "expand_demean", by.expand_demean)))
             return e;
         } else {
