@@ -38,6 +38,7 @@ FE_OPT_GRAPH = 11
 FE_OPT_ROWSUM_VARIANT = 12
 FE_OPT_ABSORB = 14
 FE_OPT_FUSED_DEMEAN = 15
+FE_OPT_ABSORB_SCALE = 16
 
 # every symbol declared in include/fe_b200.h
 EXPORTS = (

@@ -99,6 +99,102 @@ __global__ void k_cwp(const double* __restrict__ cw_d, const int32_t* __restrict
 
 static inline unsigned grid1(int64_t n, int b = 256) { return (unsigned)((n + b - 1) / b); }
 
+// Column scales of the absorbed operator M A_r: 1 / ||M a_l|| for level l of
+// a non-primary FE, where M projects out the primary FE's columns e_w:
+//   ||M a_l||^2 = ||a_l||^2 - sum_w (e_w' a_l)^2 / ||e_w||^2,
+// e_w' a_l = sum over the rows of level l in primary level w of cw_i cw_p,i,
+// ||a_l||^2 = 1 / scale_l^2 and 1 / ||e_w||^2 = scale_p,w^2 (the Jacobi
+// scales).  Level l's positions in level order are in sorted-row order, and
+// sorted rows are grouped by primary level, so the rows of one (w, l) pair
+// form a run of consecutive positions.  Levels are cut into pieces of at most
+// kAbsPiece positions: one thread per piece sums its runs and reports its
+// first and last run separately (they may continue in the neighbouring
+// pieces); one thread per level then joins the pieces in order.  The order is
+// fixed, so the result does not depend on scheduling.  The ratio
+// ||M a_l||^2 / ||a_l||^2 is floored at 1e-4, so a column that the projection
+// (almost) removes is amplified at most 100-fold; an empty column keeps 0.
+constexpr int64_t kAbsPiece = 1024;
+struct AbsPiece {
+  int64_t q0, q1;   // positions in level order
+  int32_t nruns;    // runs (distinct primary levels) in the piece
+  int32_t w0, w1;   // primary level of the first and of the last run
+  double s0, s1;    // sums of cw cw_p over the first and the last run
+  double mid;       // runs in between: sum of s^2 / ||e_w||^2
+};
+__device__ __forceinline__ double abs_run(double s, int32_t w, const double* scp) {
+  return s * s * scp[w] * scp[w];
+}
+__global__ void k_abs_pieces(AbsPiece* __restrict__ pc, int64_t n, const int32_t* __restrict__ perm,
+                             const int32_t* __restrict__ refp, const double* __restrict__ cwk,
+                             const double* __restrict__ cwp, const double* __restrict__ scp) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  AbsPiece a = pc[i];
+  a.nruns = 0;
+  a.w0 = a.w1 = -1;
+  a.s0 = a.s1 = a.mid = 0.0;
+  int32_t wc = -1;
+  double s = 0.0;
+  for (int64_t q = a.q0; q < a.q1; ++q) {
+    const int64_t p = perm ? (int64_t)perm[q] : q;
+    const int32_t w = refp[p];
+    if (w != wc) {
+      if (a.nruns == 1) {
+        a.w0 = wc;
+        a.s0 = s;
+      } else if (a.nruns > 1) {
+        a.mid += abs_run(s, wc, scp);
+      }
+      ++a.nruns;
+      s = 0.0;
+      wc = w;
+    }
+    s += (cwk ? cwk[p] : 1.0) * (cwp ? cwp[p] : 1.0);
+  }
+  if (a.nruns == 1) {
+    a.w0 = wc;
+    a.s0 = s;
+  } else if (a.nruns > 1) {
+    a.w1 = wc;
+    a.s1 = s;
+  }
+  pc[i] = a;
+}
+__global__ void k_abs_join(const AbsPiece* __restrict__ pc, const int64_t* __restrict__ first,
+                           int64_t nl, const double* __restrict__ scp,
+                           const double* __restrict__ sck, double* __restrict__ out_d,
+                           float* __restrict__ out_f) {
+  const int64_t l = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (l >= nl) return;
+  const double sk = sck[l];
+  double res = 0.0;
+  if (sk > 0.0) {
+    double tot = 0.0, sc = 0.0;
+    int32_t wc = -1;  // the open run
+    for (int64_t i = first[l]; i < first[l + 1]; ++i) {
+      const AbsPiece& a = pc[i];
+      if (a.nruns == 0) continue;
+      if (a.w0 == wc) {
+        sc += a.s0;  // the open run continues
+      } else {
+        if (wc >= 0) tot += abs_run(sc, wc, scp);
+        wc = a.w0;
+        sc = a.s0;
+      }
+      if (a.nruns > 1) {  // the first run ends inside the piece
+        tot += abs_run(sc, wc, scp) + a.mid;
+        wc = a.w1;
+        sc = a.s1;
+      }
+    }
+    if (wc >= 0) tot += abs_run(sc, wc, scp);
+    const double a2 = 1.0 / (sk * sk);
+    res = 1.0 / sqrt(fmax(a2 - tot, 1e-4 * a2));
+  }
+  out_d[l] = res;
+  out_f[l] = (float)res;
+}
+
 // ---------------------------------------------------------------------------
 // the solver constructor
 // ---------------------------------------------------------------------------
@@ -297,6 +393,52 @@ int plan_update_weights(fe_plan* pl, const double* weights) {
                                                            (int64_t)its->pu.size(), sums.as<double>(),
                                                            epi, nullptr, nullptr, 0);
     FE_CK(cudaGetLastError());
+  }
+  // the absorbed operator's column scales (single-problem plans, 2+ FEs)
+  pl->d_abs_scale_d.resize(K);
+  pl->d_abs_scale_f.resize(K);
+  if (pl->nprob == 1 && K >= 2 && N > 0) {
+    const int kp = pl->primary;
+    DevBuf pcs, first;
+    std::vector<AbsPiece> hp;
+    std::vector<int64_t> hf;
+    for (int k = 0; k < K; ++k) {
+      if (k == kp) continue;
+      const int64_t nl = pl->nlev[k];
+      const std::vector<int64_t>& so = pl->seg_off[k];
+      hp.clear();
+      hf.assign((size_t)nl + 1, 0);
+      for (int64_t l = 0; l < nl; ++l) {
+        hf[(size_t)l] = (int64_t)hp.size();
+        for (int64_t q = so[(size_t)l]; q < so[(size_t)l + 1]; q += kAbsPiece) {
+          AbsPiece a{};
+          a.q0 = q;
+          a.q1 = std::min(q + kAbsPiece, so[(size_t)l + 1]);
+          hp.push_back(a);
+        }
+      }
+      hf[(size_t)nl] = (int64_t)hp.size();
+      st = pl->d_abs_scale_d[k].ensure((size_t)(nl + 1) * 8);
+      if (!st) st = pl->d_abs_scale_f[k].ensure((size_t)(nl + 1) * 4);
+      if (!st) st = upload(pcs, hp.data(), hp.size(), s);
+      if (!st) st = upload(first, hf.data(), hf.size(), s);
+      if (st) return st;
+      FE_CK(cudaMemsetAsync(pl->d_abs_scale_d[k].p, 0, (size_t)(nl + 1) * 8, s));
+      FE_CK(cudaMemsetAsync(pl->d_abs_scale_f[k].p, 0, (size_t)(nl + 1) * 4, s));
+      if (!hp.empty()) {
+        k_abs_pieces<<<grid1((int64_t)hp.size(), 128), 128, 0, s>>>(
+            pcs.as<AbsPiece>(), (int64_t)hp.size(), d.perm[k], d.refs[kp], d.cw_d[k], d.cw_d[kp],
+            d.scale_d[kp]);
+        FE_CK(cudaGetLastError());
+      }
+      if (nl > 0) {
+        k_abs_join<<<grid1(nl, 128), 128, 0, s>>>(
+            pcs.as<AbsPiece>(), first.as<int64_t>(), nl, d.scale_d[kp], d.scale_d[k],
+            pl->d_abs_scale_d[k].as<double>(), pl->d_abs_scale_f[k].as<float>());
+        FE_CK(cudaGetLastError());
+      }
+      FE_CK(cudaStreamSynchronize(s));  // the host piece lists are reused
+    }
   }
   FE_CK(cudaStreamSynchronize(s));
   return 0;

@@ -127,6 +127,9 @@ struct fe_plan {
   fe::DevBuf d_sw_orig, d_sw_sorted;
   std::vector<fe::DevBuf> d_inter_sorted;
   std::vector<fe::DevBuf> d_scale_d, d_scale_f, d_cw_d, d_cw_f, d_cwp_d, d_cwp_f;
+  // absorbed-primary mode: per non-primary FE, 1 / ||M a_l|| (the column norms
+  // of the operator the absorbed LSMR runs on; empty for the primary FE)
+  std::vector<fe::DevBuf> d_abs_scale_d, d_abs_scale_f;
 
   fe::FeDev dev{};                     // device view (C patched per launch)
 
@@ -146,6 +149,7 @@ struct fe_plan {
   int32_t opt_rowsum_variant = -1; // row-sum pass: 0 shared-memory ring, 1 registers
   int32_t opt_absorb = 1;       // mixed residual solves project the primary FE out
   int32_t opt_exdm = 1;         // absorbed loop: fused expand + demean kernel
+  int32_t opt_abs_scale = 1;    // absorbed loop: columns scaled by 1 / ||M a_l||
   std::map<std::pair<int, int>, fe::LoopGraph> graphs;  // by (C, precision)
   // tuned variants per (tile width C, element size): {expand, segsum}
   std::map<std::pair<int, int>, std::pair<int, int>> tuned;

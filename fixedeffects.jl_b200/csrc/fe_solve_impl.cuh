@@ -871,6 +871,7 @@ static int run_loop(fe_plan* pl, Ctx& c, int prec, int64_t cap, int32_t nact0, B
     key = key * 5 + (size_t)(pl->opt_rowsum_variant + 1);
     key = key * 3 + (c.absorb ? 1u : 0u);
     key = key * 3 + (size_t)pl->opt_exdm;
+    key = key * 3 + (size_t)pl->opt_abs_scale;
     lg = &pl->graphs[{c.C, prec}];
     if (!lg->exec || lg->key != key) {
       if (lg->exec) {
@@ -1171,6 +1172,15 @@ static int solve_mixed_tile(fe_plan* pl, const SolveReq& rq, int64_t col0, int n
   const bool absorb = rq.residuals && use_absorb(pl, c.its, C);
   c.absorb = absorb;
   c.d.absorb = absorb ? 1 : 0;
+  // the absorbed LSMR runs on M A_r with its own column scales 1 / ||M a_l||
+  // (the projection shrinks the columns unevenly); the primary FE keeps its
+  // Jacobi scale, which the projection itself uses
+  if (absorb && pl->opt_abs_scale)
+    for (int k = 0; k < pl->K; ++k)
+      if (k != pl->primary && pl->d_abs_scale_d[k].p) {
+        c.d.scale_d[k] = pl->d_abs_scale_d[k].as<double>();
+        c.d.scale_f[k] = pl->d_abs_scale_f[k].as<float>();
+      }
   if (rq.residuals && pl->opt_mixed_warm && !absorb) {
     if ((st = launch_segsum<double, C>(c, LoadIn<double, double, vec_of<double, C>()>{B64}, S64, "segsum_warm", 0.0,
                                         c.rowsum, "rowsum_warm", 0.0)))

@@ -81,6 +81,9 @@ extern "C" {
                                 and cheaper iterations); 0: LSMR over all FEs */
 #define FE_OPT_FUSED_DEMEAN 15 /* 1 (default): the absorbed loop computes and projects
                                   the rows in one kernel; 0: expand, then demean */
+#define FE_OPT_ABSORB_SCALE 16 /* 1 (default): the absorbed LSMR scales the other FEs'
+                                  columns by 1 / ||M a_l|| (their norms after the
+                                  projection); 0: by the Jacobi scale 1 / ||a_l|| */
 
 typedef struct fe_plan fe_plan;
 

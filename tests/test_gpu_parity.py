@@ -405,19 +405,21 @@ def test_absorbed_primary_matches_oracle(fe, oracle, case):
     R_o, _, _ = oracle.solve_residuals_cols(Y, refs, None, inter, w, tol=1e-8)
     fes = [fe.FixedEffect(r, interaction=a) for r, a in zip(refs, inter)]
     out = []
-    # (absorb, fused expand + demean): default, separate kernels, full LSMR
-    for absorb, fused in ((1, 1), (1, 0), (0, 1)):
+    # (absorb, fused expand + demean, columns scaled by 1/||M a_l||): default,
+    # separate kernels, Jacobi scales of A_r, full LSMR
+    for absorb, fused, ascale in ((1, 1, 1), (1, 0, 1), (1, 1, 0), (0, 1, 1)):
         feM = fe.AbstractFixedEffectSolver(fes, w, "CUDA", np.float64, precision="mixed")
         feM.set_option(fe._lib.FE_OPT_TILE, 32)
         feM.set_option(fe._lib.FE_OPT_ABSORB, absorb)
         feM.set_option(fe._lib.FE_OPT_FUSED_DEMEAN, fused)
+        feM.set_option(fe._lib.FE_OPT_ABSORB_SCALE, ascale)
         R, its, cvs = feM.solve_residuals(Y.copy(), tol=1e-8)
         R2, its2, _ = feM.solve_residuals(Y.copy(), tol=1e-8)
         feM.close()
-        assert cvs.all(), (absorb, fused, its)
+        assert cvs.all(), (absorb, fused, ascale, its)
         assert np.array_equal(R, R2) and np.array_equal(its, its2)
         err = max(rel_err(R[:, j], R_o[:, j]) for j in range(Y.shape[1]))
-        assert err < REL, (absorb, fused, err)
+        assert err < REL, (absorb, fused, ascale, err)
         out.append(R)
     for R in out[1:]:
         assert max(rel_err(out[0][:, j], R[:, j]) for j in range(Y.shape[1])) < REL
