@@ -383,7 +383,7 @@ def test_graph_replay_matches_direct_launches(fe, synth, prec):
     assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
 
 
-@pytest.mark.parametrize("case", ["weighted4", "two_fe_small", "unweighted3"])
+@pytest.mark.parametrize("case", ["weighted4", "two_fe_small", "unweighted3", "absorbed_levels"])
 def test_absorbed_primary_matches_oracle(fe, oracle, case):
     # mixed residual solves of a 32-column tile with the primary FE projected
     # out (FE_OPT_ABSORB, the default) against the oracle's full LSMR and the
@@ -399,6 +399,17 @@ def test_absorbed_primary_matches_oracle(fe, oracle, case):
         refs, inter, w = [r1, r2, r3, r4], [None, None, rng.uniform(0.5, 1.5, N), None], rng.uniform(0.5, 1.5, N)
     elif case == "two_fe_small":
         refs, inter, w = [r1, r3], [None, None], None
+    elif case == "absorbed_levels":
+        # firms 801.. are each staffed by a single worker (their columns lie in
+        # the span of the worker columns, ||M a_l|| = 0), firm 2000 by two
+        # workers of which one has a single other row (nearly absorbed)
+        r2 = r2.copy()
+        solo = r1 % 7 == 0
+        r2[solo] = 800 + r1[solo]
+        pair = np.flatnonzero(r1 == 5)
+        r2[pair] = 2000 + 5000 + 1
+        r2[np.flatnonzero(r1 == 11)[:1]] = 2000 + 5000 + 1
+        refs, inter, w = [r1, r2, r3], [None, None, None], rng.uniform(0.5, 1.5, N)
     else:
         refs, inter, w = [r1, r2, r3], [None, None, None], None
     Y = np.asfortranarray(rng.standard_normal((N, 5)))
