@@ -62,17 +62,37 @@ def _compact(keys) -> tuple[np.ndarray, int]:
     return (inv.reshape(-1) + 1).astype(np.int64), int(uniq.size)
 
 
+_SIGNLESS = np.int64(0x7FFFFFFFFFFFFFFF)
+
+
+def _order_key(a: np.ndarray) -> np.ndarray:
+    """int64 keys that sort and compare like the float values of ``a``, as
+    ``np.unique`` does: -0.0 equals 0.0, every NaN is one value after +inf.
+    Non-negative doubles keep their bit pattern; negative ones flip every bit
+    but the sign, so a larger magnitude gives a smaller key."""
+    x = np.array(a, dtype=np.float64)
+    x[x == 0.0] = 0.0
+    x[np.isnan(x)] = np.nan
+    bits = x.view(np.int64)
+    return np.where(bits < 0, bits ^ _SIGNLESS, bits)
+
+
 def group_keys(*keys, device: int = 0) -> tuple[np.ndarray, int]:
-    """Level ids of integer key tuples, grouped on the GPU (fe_group_keys):
-    1-based ranks of the distinct tuples in lexicographic ascending order, and
-    their count.  The same ids as the host grouping of ``FixedEffect``."""
+    """Level ids of integer or floating-point key tuples, grouped on the GPU
+    (fe_group_keys): 1-based ranks of the distinct tuples in lexicographic
+    ascending order, and their count.  The same ids as the host grouping of
+    ``FixedEffect``.  Floating-point keys are first mapped to int64 keys of
+    the same order (``_order_key``)."""
     if not keys:
         raise ValueError("group_keys needs at least one key vector")
     cols = []
     for a in keys:
         a = np.asarray(a)
-        if a.ndim != 1 or a.dtype.kind not in "iub":
-            raise TypeError("device grouping takes 1-d integer key vectors")
+        if a.ndim != 1 or a.dtype.kind not in "iubf":
+            raise TypeError("device grouping takes 1-d integer or floating-point key vectors")
+        if a.dtype.kind == "f":
+            cols.append(_order_key(a))
+            continue
         if a.dtype.kind == "u" and a.size and int(a.max()) > np.iinfo(np.int64).max:
             raise TypeError("unsigned keys above 2^63-1 are not supported")
         cols.append(np.ascontiguousarray(a, dtype=np.int64))
@@ -92,9 +112,10 @@ class FixedEffect:
     ``FixedEffect(a, b, ...)`` groups observations by the tuple of keys, like
     ``GroupedArray(args..., sort=nothing)`` (src/FixedEffect.jl:18-21); ids
     are assigned in ascending key order.  ``interaction=None`` is the
-    reference's UnitWeights.  ``device=d`` groups integer keys on GPU ``d``
-    (fe_group_keys: presence flags or a radix sort); otherwise the grouping
-    runs in numpy on the host, where the reference runs it too.
+    reference's UnitWeights.  ``device=d`` groups integer or floating-point
+    keys on GPU ``d`` (fe_group_keys: presence flags or a radix sort);
+    otherwise the grouping runs in numpy on the host, where the reference runs
+    it too.
     """
 
     __slots__ = ("refs", "interaction", "n")

@@ -158,3 +158,27 @@ def test_zipf_sampler(synth):
     p = np.arange(1, 1001, dtype=float) ** -1.1
     p /= p.sum()
     assert abs(c[0] / c.sum() - p[0]) < 0.01
+
+
+# --- order keys of floating-point keys (device grouping, fe_group_keys) --------
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_float_order_keys_group_like_numpy(fe_host, dtype):
+    # the device groups the int64 order keys; their ranks must be the host's
+    # grouping of the float keys (np.unique: -0.0 == 0.0, NaN last and equal)
+    rng = np.random.default_rng(7)
+    x = np.concatenate([rng.standard_normal(5000) * 10.0 ** rng.integers(-30, 30, 5000),
+                        [0.0, -0.0, np.inf, -np.inf, np.nan, -np.nan, 1e-310, -1e-310,
+                         np.finfo(np.float64).max, -np.finfo(np.float64).max]])
+    with np.errstate(over="ignore"):  # float32: values beyond its range become +-inf
+        x = np.concatenate([x, rng.choice(x, 3000)]).astype(dtype)
+    rng.shuffle(x)
+    host = fe_host.FixedEffect(x)
+    k = fe_host._order_key(x)
+    uniq, inv = np.unique(k, return_inverse=True)
+    assert uniq.size == host.n
+    assert np.array_equal(inv.reshape(-1) + 1, host.refs)
+    # multi-key tuples fold the same way
+    y = rng.integers(0, 3, x.size)
+    host2 = fe_host.FixedEffect(x, y)
+    _, inv2 = np.unique(np.stack([k, y], axis=1), axis=0, return_inverse=True)
+    assert np.array_equal(inv2.reshape(-1) + 1, host2.refs)
