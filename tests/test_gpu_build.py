@@ -51,9 +51,16 @@ def test_group_keys_matches_host(fe, case):
         assert f.n == hn and np.array_equal(f.refs, hr)
 
 
-def test_group_keys_rejects_float_keys(fe):
+def test_group_keys_float_keys_and_rejects_strings(fe):
+    rng = np.random.default_rng(9)
+    x = np.concatenate([rng.standard_normal(20_000) * 1e3, [0.0, -0.0, np.inf, -np.inf, np.nan]])
+    x = np.concatenate([x, rng.choice(x, 20_000)])
+    k2 = rng.integers(0, 4, x.size)
+    refs, nl = fe.group_keys(x, k2, device=0)
+    host = fe.FixedEffect(x, k2)  # numpy grouping on the host
+    assert nl == host.n and np.array_equal(refs, host.refs)
     with pytest.raises(TypeError):
-        fe.group_keys(np.array([0.5, 1.5]), device=0)
+        fe.group_keys(np.array(["a", "b"]), device=0)
 
 
 @pytest.mark.parametrize("scale,extra", [(0.1, 0), (0.02, 37)])
