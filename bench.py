@@ -65,6 +65,20 @@ def make_workload(scale: float, rank: int, ncols: int):
     return pb
 
 
+def throughput_figures(n_obs: int, lsmr_iters, stats: dict, ms_total: float, steps: int,
+                       ranks: int) -> dict:
+    """Whole-job observation-iterations/s (N x the LSMR iterations of every
+    column, per second; rank 0's counts times the ranks) and the algorithmic
+    bytes of every kernel of a step per second."""
+    step_s = ms_total * 1e-3 / steps
+    iters = float(np.sum(np.asarray(lsmr_iters, dtype=np.float64)))
+    alg = sum(float(v["bytes"]) for v in stats.values()) / steps
+    return {"observation_iterations_per_s": n_obs * iters * ranks / step_s,
+            "lsmr_iterations_per_step": iters * ranks,
+            "alg_bytes_per_step": alg * ranks,
+            "alg_GBps": alg * ranks / step_s / 1e9}
+
+
 def measured_peak():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -368,6 +382,7 @@ def run_ours(args):
                                         f"({tw.size} of {tv['launches']})"},
             "gpu_launches": launches,
             "kernels": per_kernel,
+            "throughput": throughput_figures(N, info["lsmr_iters"], stats, ms, args.steps, ws),
             "iterations": its_list, "converged": conv_all,
             "refinement_rounds": [int(x) for x in info["rounds"]],
             "fp64_test2": [float(x) for x in info["test2"]],

@@ -182,3 +182,18 @@ def test_float_order_keys_group_like_numpy(fe_host, dtype):
     host2 = fe_host.FixedEffect(x, y)
     _, inv2 = np.unique(np.stack([k, y], axis=1), axis=0, return_inverse=True)
     assert np.array_equal(inv2.reshape(-1) + 1, host2.refs)
+
+
+def test_bench_throughput_figures():
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("bench_mod", ROOT / "bench.py")
+    b = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(b)
+    stats = {"expand": {"bytes": 4e9, "ms": 10.0, "launches": 4},
+             "scalar": {"bytes": 0.0, "ms": 1.0, "launches": 8}}
+    t = b.throughput_figures(1000, [3, 5], stats, ms_total=20.0, steps=2, ranks=2)
+    # 10 ms per step; 8 iterations of 1000 rows on each of 2 ranks
+    assert t["observation_iterations_per_s"] == 1000 * 8 * 2 / 0.01
+    assert t["lsmr_iterations_per_step"] == 16
+    assert t["alg_bytes_per_step"] == 4e9
+    assert abs(t["alg_GBps"] - 4e9 / 0.01 / 1e9) < 1e-9
