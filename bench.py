@@ -376,6 +376,7 @@ def run_ours(args):
                     "d2h_bytes_per_step": N * ncols * 4, "ms_per_step": e2e_ms},
             "roofline": {"bound": "hbm", "kernel": tname, "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": achieved / peak,
+                         "frac_of_nominal_7700": achieved / 7700.0,
                          "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
                          "traffic": traffic, "alg_bytes_per_launch": alg,
                          "launch_time": "mean CUDA-event time of the working launches "
