@@ -307,6 +307,13 @@ int plan_update_weights(fe_plan* pl, const double* weights) {
   const int K = pl->K;
   cudaStream_t s = pl->stream;
   FE_CK(cudaSetDevice(pl->device));
+  // captured LSMR loops hold the kernel instantiations and the weight
+  // pointers of the old weights (unit weights select other kernels): drop
+  // them, the next solve captures again
+  FE_CK(cudaStreamSynchronize(s));
+  for (auto& g : pl->graphs)
+    if (g.second.exec) cudaGraphExecDestroy(g.second.exec);
+  pl->graphs.clear();
   pl->weighted = weights != nullptr;
   if (weights) {
     DevBuf w;

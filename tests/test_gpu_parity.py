@@ -434,3 +434,27 @@ def test_absorbed_primary_matches_oracle(fe, oracle, case):
         out.append(R)
     for R in out[1:]:
         assert max(rel_err(out[0][:, j], R[:, j]) for j in range(Y.shape[1])) < REL
+
+
+def test_update_weights_drops_captured_loops(fe, synth):
+    # a 32-column mixed solve captures its LSMR loop in a CUDA graph; switching
+    # between unit and other weights must not replay the old capture
+    pb = synth.make(2, scale=0.005, ncols=32)
+    fes = [fe.FixedEffect.from_refs(r, n) for r, n in zip(pb.refs, pb.nlev)]
+    w = np.random.default_rng(5).uniform(0.5, 1.5, pb.N)
+    Y = np.asfortranarray(pb.Y.astype(np.float64))
+    feM = fe.AbstractFixedEffectSolver(fes, None, "CUDA", np.float32, precision="mixed")
+    R0, _, c0 = feM.solve_residuals(Y.copy(order="F"), tol=1e-8)
+    fe.update_weights(feM, w)
+    Rw, _, cw = feM.solve_residuals(Y.copy(order="F"), tol=1e-8)
+    fe.update_weights(feM, None)
+    R1, _, c1 = feM.solve_residuals(Y.copy(order="F"), tol=1e-8)
+    feM.close()
+    feW = fe.AbstractFixedEffectSolver(fes, w, "CUDA", np.float32, precision="mixed")
+    Rref, _, cref = feW.solve_residuals(Y.copy(order="F"), tol=1e-8)
+    feW.close()
+    assert c0.all() and cw.all() and c1.all() and cref.all()
+    assert max(rel_err(Rw[:, j], Rref[:, j]) for j in range(32)) < 1e-6
+    assert max(rel_err(R1[:, j], R0[:, j]) for j in range(32)) < 1e-6
+    # the weights matter: the unit-weight residuals differ from the weighted ones
+    assert max(rel_err(R0[:, j], Rref[:, j]) for j in range(32)) > 1e-3
