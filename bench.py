@@ -237,6 +237,8 @@ def run_ours(args):
     stream = torch.cuda.current_stream()
     L = fe._lib.load()
     fe._lib.check(L.fe_plan_set_stream(feM._h, stream.cuda_stream))
+    if args.no_absorb:  # the full-LSMR loop over all fixed effects
+        feM.set_option(fe._lib.FE_OPT_ABSORB, 0)
 
     N, ncols = pb.N, pb.Y.shape[1]
     # inputs resident in HBM: a pristine column-major copy, refreshed into the
@@ -283,6 +285,8 @@ def run_ours(args):
     Yh0 = np.ascontiguousarray(pb.Y.T)
     Yh = Yh_pin.numpy().T  # column-major view of pinned memory
     feM_h = fe.AbstractFixedEffectSolver(fes, pb.weights, "CUDA", np.float32, precision="mixed")
+    if args.no_absorb:
+        feM_h.set_option(fe._lib.FE_OPT_ABSORB, 0)
     Yh_pin.numpy()[...] = Yh0
     feM_h.solve_residuals(Yh, tol=1e-8, maxiter=10000)  # warm-up
     if dist:
@@ -580,6 +584,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--sweep-variants", action="store_true",
                     help="time every expand/segsum kernel variant and print a table")
+    ap.add_argument("--no-absorb", action="store_true",
+                    help="mixed solves run the full LSMR over all fixed effects (FE_OPT_ABSORB 0)")
     ap.add_argument("--plan-build", action="store_true",
                     help="time plan construction and key grouping, device vs host")
     ap.add_argument("--host-columns", type=int, default=0,
