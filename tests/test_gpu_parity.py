@@ -174,7 +174,7 @@ def test_batch_problems_vs_oracle(fe, oracle, synth):
             # about tol*||y||, so the bar is relative plus an absolute floor.
             y64 = p.Y[:, 0].astype(np.float64)
             err = np.linalg.norm(r - ro)
-            assert err <= 1e-5 * np.linalg.norm(ro) + 1e-6 * np.linalg.norm(y64)
+            assert err <= REL * np.linalg.norm(ro) + REL * np.linalg.norm(y64)
 
 
 def test_device_tensor_path(fe, synth, oracle):
