@@ -59,9 +59,16 @@ def build(force: bool = False, jobs: int | None = None, verbose: bool = False) -
     cc = nvcc()
     objs = []
     cmds = []
+    # an object is rebuilt when its source, any header or this script is
+    # newer than it (every source includes the shared headers)
+    hdr = max([f.stat().st_mtime for f in list(CSRC.glob("*.h")) + list(CSRC.glob("*.cuh"))
+               + list(INCLUDE.glob("*.h")) + [Path(__file__)]])
     for src in sources():
         obj = BUILD / (src.stem + ".o")
         objs.append(obj)
+        if (not force and obj.exists() and obj.stat().st_mtime >= src.stat().st_mtime
+                and obj.stat().st_mtime >= hdr):
+            continue
         cmds.append([cc, *ARCH, *COMMON, *PER_FILE.get(src.name, []), "-c", str(src), "-o", str(obj)])
 
     def run(cmd):

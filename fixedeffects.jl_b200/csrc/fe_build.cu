@@ -645,6 +645,7 @@ int plan_build_device(fe_plan* pl, const int64_t* const* refs, const int64_t* n_
 // ---------------------------------------------------------------------------
 extern "C" int fe_group_keys(const int64_t* const* keys, int32_t n_keys, int64_t n, int32_t device,
                              int64_t* refs_out, int64_t* n_levels_out) {
+  fe::DeviceRestore restore_device;
   using namespace fe;
   if (!keys || n_keys < 1 || n < 0 || !refs_out || !n_levels_out) {
     set_error("group_keys: need at least one key vector, n >= 0 and output pointers");

@@ -245,6 +245,7 @@ const char* fe_last_error(void) { return fe::last_error(); }
 int fe_plan_create(fe_plan** out, int64_t n_obs, int32_t n_fe, const int64_t* const* refs,
                    const int64_t* n_levels, const double* const* interaction,
                    const double* weights, int32_t device) {
+  fe::DeviceRestore restore_device;
   if (n_obs < 0) {
     set_error("n_obs must be >= 0");
     return FE_ERR_INVALID;
@@ -256,16 +257,19 @@ int fe_plan_create_batch(fe_plan** out, int32_t n_problems, const int64_t* n_obs
                          const int64_t* const* refs, const int64_t* n_levels,
                          const double* const* interaction, const double* weights,
                          int32_t device) {
+  fe::DeviceRestore restore_device;
   return create_common(out, n_problems, n_obs, n_fe, refs, n_levels, interaction, weights, device);
 }
 
 int fe_plan_update_weights(fe_plan* plan, const double* weights) {
+  fe::DeviceRestore restore_device;
   int st = check_plan(plan);
   if (st) return st;
   return fe::plan_update_weights(plan, weights);
 }
 
 int fe_plan_set_stream(fe_plan* plan, void* stream) {
+  fe::DeviceRestore restore_device;
   int st = check_plan(plan);
   if (st) return st;
   if (cudaStreamSynchronize(plan->stream) != cudaSuccess) {
@@ -288,6 +292,7 @@ int fe_plan_set_stream(fe_plan* plan, void* stream) {
 }
 
 int fe_plan_set_option(fe_plan* plan, int32_t option, double value) {
+  fe::DeviceRestore restore_device;
   int st = check_plan(plan);
   if (st) return st;
   switch (option) {
@@ -372,6 +377,7 @@ int fe_plan_set_option(fe_plan* plan, int32_t option, double value) {
 }
 
 int fe_plan_destroy(fe_plan* plan) {
+  fe::DeviceRestore restore_device;
   if (!plan) return FE_OK;
   return fe::plan_destroy(plan);
 }
@@ -379,6 +385,7 @@ int fe_plan_destroy(fe_plan* plan) {
 int fe_solve_residuals(fe_plan* plan, void* Y, int32_t dtype, int64_t ncols, int64_t ld,
                        int32_t precision, double tol, int64_t maxiter, int64_t* iterations,
                        uint8_t* converged) {
+  fe::DeviceRestore restore_device;
   int st = check_plan(plan);
   if (st) return st;
   if (ncols < 0 || (ncols > 0 && !Y && plan->N > 0)) {
@@ -396,6 +403,7 @@ int fe_solve_residuals(fe_plan* plan, void* Y, int32_t dtype, int64_t ncols, int
 int fe_solve_residuals_columns(fe_plan* plan, void* const* columns, int32_t dtype, int64_t ncols,
                                int32_t precision, double tol, int64_t maxiter,
                                int64_t* iterations, uint8_t* converged) {
+  fe::DeviceRestore restore_device;
   int st = check_plan(plan);
   if (st) return st;
   if (ncols < 0 || (ncols > 0 && !columns)) {
@@ -409,6 +417,7 @@ int fe_solve_residuals_columns(fe_plan* plan, void* const* columns, int32_t dtyp
 int fe_solve_residuals_device(fe_plan* plan, void* Y_dev, int32_t dtype, int64_t ncols,
                               int64_t ld, int32_t precision, double tol, int64_t maxiter,
                               int64_t* iterations, uint8_t* converged) {
+  fe::DeviceRestore restore_device;
   return solve_common(plan, Y_dev, nullptr, dtype, ncols, ld, precision, tol, maxiter, iterations,
                       converged);
 }
@@ -416,6 +425,7 @@ int fe_solve_residuals_device(fe_plan* plan, void* Y_dev, int32_t dtype, int64_t
 int fe_solve_coefficients(fe_plan* plan, const void* y, int32_t dtype, int32_t precision,
                           double tol, int64_t maxiter, double* const* coefs,
                           int64_t* iterations, uint8_t* converged) {
+  fe::DeviceRestore restore_device;
   int st = check_plan(plan);
   if (st) return st;
   if (dtype != FE_DTYPE_F64 && dtype != FE_DTYPE_F32) {
@@ -480,6 +490,7 @@ int fe_solve_coefficients(fe_plan* plan, const void* y, int32_t dtype, int32_t p
 }
 
 int fe_plan_problem_results(fe_plan* plan, int64_t* iterations, uint8_t* converged) {
+  fe::DeviceRestore restore_device;
   int st = check_plan(plan);
   if (st) return st;
   if (iterations)
@@ -490,6 +501,7 @@ int fe_plan_problem_results(fe_plan* plan, int64_t* iterations, uint8_t* converg
 
 int fe_plan_last_solve_info(fe_plan* plan, int64_t ncols, double* test2, int32_t* rounds,
                             int64_t* lsmr_iters) {
+  fe::DeviceRestore restore_device;
   int st = check_plan(plan);
   if (st) return st;
   const int64_t n = std::min<int64_t>(ncols, (int64_t)plan->last_test2.size());
@@ -503,6 +515,7 @@ int fe_plan_last_solve_info(fe_plan* plan, int64_t ncols, double* test2, int32_t
 
 int fe_plan_get_integer_plan(fe_plan* plan, int32_t* perm0, int64_t* const* offsets,
                              int32_t* const* segperm) {
+  fe::DeviceRestore restore_device;
   int st = check_plan(plan);
   if (st) return st;
   cudaSetDevice(plan->device);
@@ -530,6 +543,7 @@ int fe_plan_get_integer_plan(fe_plan* plan, int32_t* perm0, int64_t* const* offs
 }
 
 int fe_plan_get_scales(fe_plan* plan, double* const* scales) {
+  fe::DeviceRestore restore_device;
   int st = check_plan(plan);
   if (st) return st;
   if (!scales) {
@@ -549,6 +563,7 @@ int fe_plan_get_scales(fe_plan* plan, double* const* scales) {
 }
 
 int fe_plan_primary(fe_plan* plan, int32_t* primary) {
+  fe::DeviceRestore restore_device;
   int st = check_plan(plan);
   if (st) return st;
   if (primary) *primary = plan->primary;
@@ -557,6 +572,7 @@ int fe_plan_primary(fe_plan* plan, int32_t* primary) {
 
 int fe_plan_kernel_stat(fe_plan* plan, int32_t index, char* name, int64_t name_len,
                         int64_t* launches, double* total_ms, double* alg_bytes) {
+  fe::DeviceRestore restore_device;
   int st = check_plan(plan);
   if (st) return st;
   fe::prof_flush(plan);
@@ -579,6 +595,7 @@ int fe_plan_kernel_stat(fe_plan* plan, int32_t index, char* name, int64_t name_l
 
 int fe_plan_kernel_times(fe_plan* plan, int32_t index, float* ms, int64_t max_launches,
                          int64_t* launches) {
+  fe::DeviceRestore restore_device;
   int st = check_plan(plan);
   if (st) return st;
   fe::prof_flush(plan);
@@ -596,6 +613,7 @@ int fe_plan_kernel_times(fe_plan* plan, int32_t index, float* ms, int64_t max_la
 }
 
 int fe_plan_reset_stats(fe_plan* plan) {
+  fe::DeviceRestore restore_device;
   int st = check_plan(plan);
   if (st) return st;
   fe::prof_flush(plan);

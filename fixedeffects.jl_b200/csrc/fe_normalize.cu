@@ -151,6 +151,7 @@ using namespace fe;
 
 extern "C" int fe_normalize_coefficients(fe_plan* plan, double* const* coefs,
                                          int32_t coefs_on_device) {
+  fe::DeviceRestore restore_device;
   if (!plan || !coefs) {
     set_error_cstr("fe_normalize_coefficients: plan or coefs is NULL");
     return FE_ERR_INVALID;
@@ -270,6 +271,7 @@ extern "C" int fe_normalize_coefficients(fe_plan* plan, double* const* coefs,
 extern "C" int fe_full_coefficients(fe_plan* plan, const double* const* coefs,
                                     int32_t coefs_on_device, double* const* out,
                                     int32_t out_on_device) {
+  fe::DeviceRestore restore_device;
   if (!plan || !coefs || !out) {
     set_error_cstr("fe_full_coefficients: plan, coefs or out is NULL");
     return FE_ERR_INVALID;

@@ -7,6 +7,8 @@
 // (src/SolverCPU.jl:55-95).
 #include <cuda_runtime.h>
 
+#include <cstdlib>
+
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -34,6 +36,19 @@ const char* last_error() { return g_err; }
 DevBuf::~DevBuf() {
   if (p) cudaFree(p);
 }
+// Host-side fault injection for the allocation-failure path: with
+// FE_B200_FAIL_ALLOC_BYTES=b in the environment, every device allocation of at
+// least b bytes fails as an out-of-memory cudaMalloc would (FE_ERR_ALLOC and
+// a message), without touching the GPU.  Read on every allocation, so a test
+// can set and clear it between calls.
+static bool injected_alloc_failure(size_t n) {
+  const char* v = getenv("FE_B200_FAIL_ALLOC_BYTES");
+  if (!v || !*v) return false;
+  char* end = nullptr;
+  const unsigned long long b = strtoull(v, &end, 10);
+  return end != v && (unsigned long long)n >= b;
+}
+
 int DevBuf::ensure(size_t n) {
   if (n <= bytes && p) return 0;
   if (p) {
@@ -42,6 +57,11 @@ int DevBuf::ensure(size_t n) {
     bytes = 0;
   }
   if (n == 0) n = 16;
+  if (injected_alloc_failure(n)) {
+    set_error(std::string("cudaMalloc of ") + std::to_string(n) +
+              " bytes failed: injected by FE_B200_FAIL_ALLOC_BYTES");
+    return 3;  // FE_ERR_ALLOC
+  }
   cudaError_t e = cudaMalloc(&p, n);
   if (e != cudaSuccess) {
     p = nullptr;
@@ -708,6 +728,7 @@ int plan_destroy(fe_plan* pl) {
     cudaEventDestroy(pr.second.second);
   }
   if (pl->host_pinned) cudaFreeHost(pl->host_pinned);
+  if (pl->noalloc_order) cudaEventDestroy(pl->noalloc_order);
   for (auto& g : pl->graphs)
     if (g.second.exec) cudaGraphExecDestroy(g.second.exec);
   cudaStream_t s = pl->stream;

@@ -31,6 +31,30 @@ const char* last_error();
     }                                                                                   \
   } while (0)
 
+// The caller's current device, saved when an entry point starts and put back
+// on every return path.  A host binding such as CUDA.jl tracks its own
+// current device per task; the library switches to the plan's device for its
+// work and must not leave that switch behind.  With no usable device nothing
+// is saved and nothing is restored.
+struct DeviceRestore {
+  int saved = -1;
+  DeviceRestore() {
+    if (cudaGetDevice(&saved) != cudaSuccess) {
+      (void)cudaGetLastError();
+      saved = -1;
+    }
+  }
+  ~DeviceRestore() {
+    if (saved < 0) return;
+    int cur = -1;
+    if (cudaGetDevice(&cur) != cudaSuccess || cur != saved) {
+      if (cudaSetDevice(saved) != cudaSuccess) (void)cudaGetLastError();
+    }
+  }
+  DeviceRestore(const DeviceRestore&) = delete;
+  DeviceRestore& operator=(const DeviceRestore&) = delete;
+};
+
 // A device allocation owned by the plan.
 struct DevBuf {
   void* p = nullptr;
@@ -159,6 +183,8 @@ struct fe_plan {
   fe::Workspace ws;
   fe::Profile prof;
   void* host_pinned = nullptr;  // small pinned staging for counters
+  // fe_plan_scales_noalloc on a caller stream: orders it after the plan's stream
+  cudaEvent_t noalloc_order = nullptr;
 
   // results of the last solve (per column)
   std::vector<double> last_test2;

@@ -131,6 +131,13 @@ __device__ static void lsmr_init(Inst& s, int init_mode) {
   s.upd_mode = init_mode;  // h <- v, hbar <- 0 (and x <- 0) at the next reduce
   s.do_v = 1;
   s.active = (s.normAr != 0.0 && s.maxiter > 0 && !s.skip_lsmr) ? 1 : 0;
+  // a NaN or infinite right-hand side: the reference runs maxiter iterations
+  // on NaN norms (no test can pass) and reports istop = 7, not converged;
+  // here the instance stops at once with the same verdict
+  if (!isfinite(s.normAr)) {
+    s.active = 0;
+    s.istop = 7;
+  }
   s.ex_av = s.s_v;
   s.ex_au = -s.alpha * s.u_scale;
   if (!s.active) deactivate(s);
@@ -254,6 +261,15 @@ __global__ void __launch_bounds__(kScalarThreads) k_scalar(ScalarArgs a) {
         if (s.iter > 0) s.normA2_prev += s.normA * s.normA;
       }
       const double nAt = sqrt(s.normA2_prev);
+      if (!isfinite(nr) || !isfinite(ng)) {
+        // a NaN or infinite right-hand side: stop, not converged (the
+        // reference's verdict after maxiter iterations on NaN norms)
+        s.last_test2 = nr * ng;
+        s.converged = 0;
+        s.outer_active = 0;
+        deactivate(s);
+        break;
+      }
       bool conv = false;
       s.last_test2 = (nAt > 0 && nr > 0) ? ng / (nAt * nr) : (ng == 0.0 ? 0.0 : 1.0);
       if (s.skip_lsmr || ng == 0.0 || nr == 0.0) {

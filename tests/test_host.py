@@ -191,9 +191,49 @@ def test_bench_throughput_figures():
     spec.loader.exec_module(b)
     stats = {"expand": {"bytes": 4e9, "ms": 10.0, "launches": 4},
              "scalar": {"bytes": 0.0, "ms": 1.0, "launches": 8}}
-    t = b.throughput_figures(1000, [3, 5], stats, ms_total=20.0, steps=2, ranks=2)
+    t = b.throughput_figures(1000 * 8, [3, 5], stats, prof_steps=1, step_s=0.01, ranks=2)
     # 10 ms per step; 8 iterations of 1000 rows on each of 2 ranks
     assert t["observation_iterations_per_s"] == 1000 * 8 * 2 / 0.01
     assert t["lsmr_iterations_per_step"] == 16
-    assert t["alg_bytes_per_step"] == 4e9
-    assert abs(t["alg_GBps"] - 4e9 / 0.01 / 1e9) < 1e-9
+    assert t["alg_bytes_per_step"] == 8e9
+    assert abs(t["alg_GBps"] - 8e9 / 0.01 / 1e9) < 1e-9
+
+
+def _entry_point_bodies():
+    """(name, body) of every extern "C" entry point in the library sources."""
+    csrc = Path(__file__).resolve().parent.parent / "fixedeffects.jl_b200" / "csrc"
+    out = []
+    for f in sorted(csrc.glob("*.cu")):
+        src = f.read_text()
+        # functions inside an extern "C" { ... } block, or declared extern "C" one by one
+        for m in re.finditer(r'(?:^|\n)(?:extern "C" )?(?:int|const char\*) (fe_[a-z0-9_]+)\([^;{]*\)\s*\{',
+                             src):
+            start = m.end()
+            depth, i = 1, start
+            while depth and i < len(src):
+                depth += {"{": 1, "}": -1}.get(src[i], 0)
+                i += 1
+            out.append((m.group(1), f.name, src[start:i]))
+    return out
+
+
+def test_every_entry_point_restores_the_callers_device():
+    """Entry points that may switch devices save and restore the caller's
+    current device (a Julia caller tracks its own device per task)."""
+    bodies = _entry_point_bodies()
+    names = {n for n, _, _ in bodies}
+    assert set(_declared_symbols()) <= names | {"fe_version", "fe_last_error"}
+    for name, fname, body in bodies:
+        if name in ("fe_version", "fe_last_error"):
+            continue
+        assert "DeviceRestore" in body.split("\n", 2)[1], (name, fname)
+
+
+def test_noalloc_entry_point_calls_no_allocator():
+    """fe_plan_scales_noalloc's translation unit never allocates device memory
+    (no cudaMalloc / cudaFree / plan buffer growth)."""
+    src = (Path(__file__).resolve().parent.parent / "fixedeffects.jl_b200" / "csrc"
+           / "fe_noalloc.cu").read_text()
+    code = re.sub(r"//[^\n]*", "", src)
+    for word in ("cudaMalloc", "cudaFree", "cudaMallocAsync", ".ensure(", "new ", "malloc("):
+        assert word not in code, word
