@@ -1,9 +1,10 @@
 // fe_noalloc.cu -- fe_plan_scales_noalloc: the Jacobi preconditioner of one
 // fixed effect recomputed without any device allocation.
 //
-// Who needs it: code that must not call cudaMalloc at that moment.  Examples
-// are a caller whose device memory is owned by its own pool or by another
-// runtime (Julia's CUDA.jl allocator, for instance), and a host callback.
+// Who needs it: a caller that must not call cudaMalloc at that moment.  The
+// typical one owns the device heap itself: Julia's CUDA.jl hands out device
+// memory from its own pool, and a cudaMalloc behind its back can fail once
+// the pool holds the free memory, or breaks the memory budget the caller set.
 // fe_plan_update_weights allocates its level-sum and piece-partial scratch on
 // every call; this entry point keeps that scratch in one file-scope device
 // array instead.
@@ -14,8 +15,6 @@
 // start at zero; calls that overlap on the GPU (different streams, or
 // different host threads) race on it and must be serialized by the caller.
 #include <cuda_runtime.h>
-
-#include <mutex>
 
 #include "../../include/fe_b200.h"
 #include "fe_kernels.cuh"
@@ -29,30 +28,21 @@ static_assert(kNoAllocScratchBytes % 256 == 0, "scratch size");
 
 __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
-// Device address of g_noalloc_scratch per device.  In host code the symbol
-// is only a host-side stand-in; the device address comes from
-// cudaGetSymbolAddress, taken once per device with that device current.
-constexpr int kMaxDevices = 64;
-void* g_scratch_addr[kMaxDevices] = {};
-std::mutex g_scratch_mu;
-
-int scratch_address(int device, void** out) {
-  if (device < 0 || device >= kMaxDevices) {
-    set_error_cstr("fe_plan_scales_noalloc: device ordinal out of range");
-    return FE_ERR_INVALID;
+// Device address of g_noalloc_scratch on the current device.  In host code
+// the symbol is only a host-side stand-in; the device address comes from
+// cudaGetSymbolAddress with the plan's device current.  It is looked up on
+// every call (no allocation, a few microseconds), so a device reset, after
+// which the module and the array may be loaded at another address, leaves
+// no stale pointer behind.
+int scratch_address(void** out) {
+  void* p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  if (e != cudaSuccess || !p) {
+    (void)cudaGetLastError();
+    set_error_cstr("fe_plan_scales_noalloc: cudaGetSymbolAddress of the scratch array failed");
+    return FE_ERR_CUDA;
   }
-  std::lock_guard<std::mutex> lock(g_scratch_mu);
-  if (!g_scratch_addr[device]) {
-    void* p = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess || !p) {
-      (void)cudaGetLastError();
-      set_error_cstr("fe_plan_scales_noalloc: cudaGetSymbolAddress of the scratch array failed");
-      return FE_ERR_CUDA;
-    }
-    g_scratch_addr[device] = p;
-  }
-  *out = g_scratch_addr[device];
+  *out = p;
   return FE_OK;
 }
 
@@ -125,6 +115,7 @@ __global__ void k_scale_from_sums(const double* __restrict__ sums, int64_t n,
 
 extern "C" int fe_plan_scales_noalloc(fe_plan* plan, int32_t fe_index, double* scale_out_dev,
                                       void* stream) {
+  fe::DeviceRestore restore_device;
   using namespace fe;
   if (!plan) {
     set_error_cstr("fe_plan_scales_noalloc: plan is NULL");
@@ -156,7 +147,8 @@ extern "C" int fe_plan_scales_noalloc(fe_plan* plan, int32_t fe_index, double* s
   if (sums_bytes + piece_bytes + block_bytes + cnt_bytes + bcnt_bytes > kNoAllocScratchBytes) {
     set_error_cstr(
         "fe_plan_scales_noalloc: the fixed effect needs more scratch than FE_NOALLOC_SCRATCH_BYTES "
-        "(8 MiB: about 1e6 levels); use fe_plan_update_weights/fe_plan_get_scales");
+        "(8 MiB: its level sums, about 1e6 levels at most, plus the piece partials of the long "
+        "levels of every fixed effect of the plan); use fe_plan_update_weights/fe_plan_get_scales");
     return FE_ERR_INVALID;
   }
   if (cudaSetDevice(plan->device) != cudaSuccess) {
@@ -165,7 +157,7 @@ extern "C" int fe_plan_scales_noalloc(fe_plan* plan, int32_t fe_index, double* s
     return FE_ERR_CUDA;
   }
   void* base = nullptr;
-  int st = scratch_address(plan->device, &base);
+  int st = scratch_address(&base);
   if (st) return st;
   unsigned char* b = static_cast<unsigned char*>(base);
   double* sums = reinterpret_cast<double*>(b);
@@ -174,6 +166,21 @@ extern "C" int fe_plan_scales_noalloc(fe_plan* plan, int32_t fe_index, double* s
   int32_t* cnt = reinterpret_cast<int32_t*>(b + sums_bytes + piece_bytes + block_bytes);
   int32_t* bcnt = reinterpret_cast<int32_t*>(b + sums_bytes + piece_bytes + block_bytes + cnt_bytes);
   cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : plan->stream;
+  // a caller stream runs after the work already queued on the plan's stream
+  // (fe_plan_update_weights rewrites the weight arrays read here): an event
+  // recorded there and waited on here, created on the plan's first call
+  if (s != plan->stream) {
+    cudaError_t eo = cudaSuccess;
+    if (!plan->noalloc_order)
+      eo = cudaEventCreateWithFlags(&plan->noalloc_order, cudaEventDisableTiming);
+    if (eo == cudaSuccess) eo = cudaEventRecord(plan->noalloc_order, plan->stream);
+    if (eo == cudaSuccess) eo = cudaStreamWaitEvent(s, plan->noalloc_order, 0);
+    if (eo != cudaSuccess) {
+      (void)cudaGetLastError();
+      set_error_cstr("fe_plan_scales_noalloc: ordering after the plan's stream failed");
+      return FE_ERR_CUDA;
+    }
+  }
   // levels without positions are never written by the sum kernel and the
   // split counters must start at zero: clear both (the array keeps the
   // previous call's contents)

@@ -255,20 +255,26 @@ int fe_plan_reset_stats(fe_plan* plan);
  * Recomputes the Jacobi scales of fixed effect `fe_index` of an existing plan
  * (the values fe_plan_get_scales returns, src/SolverCPU.jl:78-89) into
  * `scale_out_dev`, n_levels[fe_index] doubles of DEVICE memory, enqueued on
- * `stream` (NULL: the plan's stream), without allocating any memory.  It is
- * for callers that cannot call cudaMalloc at that point: a caller whose device
- * memory belongs to its own pool or runtime (e.g. Julia's CUDA.jl allocator,
- * which owns the device heap it hands out), or code on a path where a
- * cudaMalloc would stall or is not allowed, such as a host callback.
+ * `stream` (NULL: the plan's stream), without allocating any device memory.
+ * It is for callers that cannot call cudaMalloc at that point, because the
+ * device heap is not theirs to grow: a caller whose device memory belongs to
+ * its own pool or runtime (Julia's CUDA.jl allocator hands out memory from a
+ * pool it owns, so a cudaMalloc behind its back can fail once the pool holds
+ * the free memory), or one that runs under a fixed device-memory budget.
  *
  * Its scratch is one file-scope device array of FE_NOALLOC_SCRATCH_BYTES
  * (8 MiB) that every GPU which loads the library holds until the process
- * exits; fixed effects whose level sums do not fit (about 1e6 levels) are
- * rejected with FE_ERR_INVALID and a message.  The first call on a device
- * looks up the array's device address (cudaGetSymbolAddress); make that first
- * call before any stream capture.  All calls share the array and it keeps
- * the last call's contents (each call clears what must start at zero): calls
- * that overlap on the GPU race and must be serialized by the caller.
+ * exits.  It holds the fixed effect's level sums (about 1e6 levels at most)
+ * and the piece partials of the plan's long levels; a fixed effect that does
+ * not fit is rejected with FE_ERR_INVALID and a message.  The array's device
+ * address is looked up (cudaGetSymbolAddress) with the plan's device current
+ * on every call; the first call on a device may also load the library's
+ * device code, so make that first call before any stream capture.  All calls
+ * share the array and it keeps the last call's contents (each call clears
+ * what must start at zero): calls that overlap on the GPU race and must be
+ * serialized by the caller.  A caller stream is ordered after the work
+ * already queued on the plan's stream (an event recorded there); the caller
+ * orders any later use of the output itself.
  */
 #define FE_NOALLOC_SCRATCH_BYTES (8u << 20)
 int fe_plan_scales_noalloc(fe_plan* plan, int32_t fe_index, double* scale_out_dev, void* stream);

@@ -1,7 +1,8 @@
 """fe_plan_scales_noalloc: the allocation-free recomputation of one fixed
-effect's Jacobi scales, for callers that cannot call cudaMalloc (a caller
-whose device memory belongs to its own pool, a host callback).  Its
-output must equal what fe_plan_get_scales returns for the same plan.
+effect's Jacobi scales, for callers that cannot call cudaMalloc because the
+device heap is not theirs to grow (a caller whose device memory belongs to its
+own pool, such as Julia's CUDA.jl allocator).  Its output must equal what
+fe_plan_get_scales returns for the same plan.
 
 This file is collected last on purpose: it exercises a shared, fixed-size
 device scratch array that keeps the previous call's contents."""
