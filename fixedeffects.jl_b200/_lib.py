@@ -24,6 +24,13 @@ FE_PREC_FP32 = 2
 FE_DTYPE_F64 = 0
 FE_DTYPE_F32 = 1
 
+FE_XCHG_F64 = 0
+FE_XCHG_F32 = 1
+
+# fe_exchange_fn: int (*)(void* ctx, void* buf, int64_t count, int32_t dtype, void* stream)
+EXCHANGE_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64,
+                               ctypes.c_int32, ctypes.c_void_p)
+
 FE_OPT_TILE = 1
 FE_OPT_CHECK_EVERY = 2
 FE_OPT_MAX_ROUNDS = 3
@@ -39,6 +46,7 @@ FE_OPT_ROWSUM_VARIANT = 12
 FE_OPT_ABSORB = 14
 FE_OPT_FUSED_DEMEAN = 15
 FE_OPT_ABSORB_SCALE = 16
+FE_OPT_EXDM_PIPE = 17
 
 # every symbol declared in include/fe_b200.h
 EXPORTS = (
@@ -49,7 +57,7 @@ EXPORTS = (
     "fe_plan_get_integer_plan", "fe_plan_get_scales", "fe_plan_primary",
     "fe_plan_kernel_stat", "fe_plan_reset_stats", "fe_plan_scales_noalloc",
     "fe_normalize_coefficients", "fe_full_coefficients", "fe_group_keys",
-    "fe_solve_residuals_columns", "fe_plan_kernel_times",
+    "fe_solve_residuals_columns", "fe_plan_kernel_times", "fe_plan_create_sharded",
 )
 
 _i64p = ctypes.POINTER(ctypes.c_int64)
@@ -123,6 +131,9 @@ def load(path: Path | str | None = None):
         "fe_solve_residuals_columns": (ctypes.c_int, [_vp, _vpp, ctypes.c_int32, ctypes.c_int64,
                                                       ctypes.c_int32, ctypes.c_double,
                                                       ctypes.c_int64, _i64p, _u8p]),
+        "fe_plan_create_sharded": (ctypes.c_int, [ctypes.POINTER(_vp), ctypes.c_int64,
+                                                  ctypes.c_int32, _vpp, _i64p, _vpp, _f64p,
+                                                  ctypes.c_int32, EXCHANGE_FN, _vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

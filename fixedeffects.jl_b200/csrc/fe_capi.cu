@@ -25,7 +25,8 @@ int check_plan(fe_plan* p) {
 
 int create_common(fe_plan** out, int32_t nprob, const int64_t* n_obs, int32_t K,
                   const int64_t* const* refs, const int64_t* n_levels,
-                  const double* const* interaction, const double* weights, int32_t device) {
+                  const double* const* interaction, const double* weights, int32_t device,
+                  fe_exchange_fn xchg = nullptr, void* xchg_ctx = nullptr) {
   if (!out) {
     set_error("out is NULL");
     return FE_ERR_INVALID;
@@ -46,6 +47,8 @@ int create_common(fe_plan** out, int32_t nprob, const int64_t* n_obs, int32_t K,
     set_error("host allocation failed");
     return FE_ERR_ALLOC;
   }
+  pl->xchg = xchg;
+  pl->xchg_ctx = xchg_ctx;
   int st = fe::plan_build(pl, nprob, n_obs, K, refs, n_levels, interaction, weights, device);
   if (st) {
     fe::plan_destroy(pl);
@@ -253,6 +256,24 @@ int fe_plan_create(fe_plan** out, int64_t n_obs, int32_t n_fe, const int64_t* co
   return create_common(out, 1, &n_obs, n_fe, refs, n_levels, interaction, weights, device);
 }
 
+int fe_plan_create_sharded(fe_plan** out, int64_t n_obs, int32_t n_fe, const int64_t* const* refs,
+                           const int64_t* n_levels, const double* const* interaction,
+                           const double* weights, int32_t device, fe_exchange_fn exchange,
+                           void* ctx) {
+  fe::DeviceRestore restore_device;
+  if (!exchange) {
+    set_error("a sharded plan needs an exchange function");
+    return FE_ERR_INVALID;
+  }
+  if (n_obs < 1) {
+    // every rank takes part in every exchange, so none may be empty
+    set_error("a sharded plan needs at least one observation on every rank");
+    return FE_ERR_INVALID;
+  }
+  return create_common(out, 1, &n_obs, n_fe, refs, n_levels, interaction, weights, device,
+                       exchange, ctx);
+}
+
 int fe_plan_create_batch(fe_plan** out, int32_t n_problems, const int64_t* n_obs, int32_t n_fe,
                          const int64_t* const* refs, const int64_t* n_levels,
                          const double* const* interaction, const double* weights,
@@ -350,6 +371,15 @@ int fe_plan_set_option(fe_plan* plan, int32_t option, double value) {
     case FE_OPT_ABSORB_SCALE:
       plan->opt_abs_scale = value != 0 ? 1 : 0;
       return FE_OK;
+    case FE_OPT_EXDM_PIPE: {
+      const int v = (int)value;
+      if (v < -1 || v > 2) {
+        set_error("pipelined absorbed kernel option must be -1 (default), 0 (off), 1 or 2");
+        return FE_ERR_INVALID;
+      }
+      plan->opt_exdm_pipe = v;
+      return FE_OK;
+    }
     case FE_OPT_ROWSUM_VARIANT: {
       const int v = (int)value;
       if (v < -1 || v > 1) {

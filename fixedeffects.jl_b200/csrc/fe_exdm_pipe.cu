@@ -1,0 +1,50 @@
+// fe_exdm_pipe.cu -- instantiations and launch of the pipelined fused
+// expand + demean kernel of the absorbed loop (fe_exdm_pipe.cuh).
+#include <cuda_runtime.h>
+
+#include "fe_exdm_pipe.cuh"
+#include "fe_plan.h"
+
+namespace fe {
+
+namespace {
+
+template <int NL, int NS, bool W, int STG, bool PG>
+int launch_one(const ExdmLaunch& a) {
+  auto kern = k_exdm_pipe<NL, NS, W, STG, PG>;
+  static size_t attr_smem = 0;  // per instantiation: the opt-in size set so far
+  if (a.smem > attr_smem) {
+    FE_CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)a.smem));
+    attr_smem = a.smem;
+  }
+  kern<<<(unsigned)a.grid, kThreads, a.smem, a.stream>>>(a.d, a.items, a.n_items, a.tab, a.rows,
+                                                        a.inst, a.rs, a.sr, a.lf, a.part, a.S);
+  FE_CK(cudaGetLastError());
+  return 0;
+}
+
+template <int NL, int NS, bool W>
+int launch_cfg(const ExdmLaunch& a, int cfg) {
+  return cfg == 2 ? launch_one<NL, NS, W, 2, false>(a) : launch_one<NL, NS, W, 2, true>(a);
+}
+
+}  // namespace
+
+int launch_exdm_pipe(const ExdmLaunch& a, int nl, int ns, bool w, int cfg) {
+  switch ((nl * 3 + ns) * 2 + (w ? 1 : 0)) {
+    case 0: return launch_cfg<0, 0, false>(a, cfg);
+    case 1: return launch_cfg<0, 0, true>(a, cfg);
+    case 2: return launch_cfg<0, 1, false>(a, cfg);
+    case 3: return launch_cfg<0, 1, true>(a, cfg);
+    case 4: return launch_cfg<0, 2, false>(a, cfg);
+    case 5: return launch_cfg<0, 2, true>(a, cfg);
+    case 6: return launch_cfg<1, 0, false>(a, cfg);
+    case 7: return launch_cfg<1, 0, true>(a, cfg);
+    case 8: return launch_cfg<1, 1, false>(a, cfg);
+    case 9: return launch_cfg<1, 1, true>(a, cfg);
+    case 10: return launch_cfg<1, 2, false>(a, cfg);
+    default: return launch_cfg<1, 2, true>(a, cfg);
+  }
+}
+
+}  // namespace fe

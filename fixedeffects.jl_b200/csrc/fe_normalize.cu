@@ -156,6 +156,12 @@ extern "C" int fe_normalize_coefficients(fe_plan* plan, double* const* coefs,
     set_error_cstr("fe_normalize_coefficients: plan or coefs is NULL");
     return FE_ERR_INVALID;
   }
+  if (plan->xchg) {
+    // the connected components span every rank's observations
+    set_error_cstr("fe_normalize_coefficients: not available for an observation-sharded plan "
+                   "(the components need every rank's observations)");
+    return FE_ERR_INVALID;
+  }
   const int K = plan->K;
   for (int k = 0; k < K; ++k)
     if (!coefs[k] && plan->nlev[k] > 0) {

@@ -36,6 +36,16 @@ const char* last_error() { return g_err; }
 DevBuf::~DevBuf() {
   if (p) cudaFree(p);
 }
+
+int exchange(fe_plan* pl, void* buf, int64_t count, int elem_bytes, cudaStream_t s) {
+  if (!pl->xchg || count <= 0) return 0;
+  const int rc = pl->xchg(pl->xchg_ctx, buf, count, elem_bytes == 8 ? 0 : 1, (void*)s);
+  if (rc != 0) {
+    set_error("the exchange over ranks failed (callback status " + std::to_string(rc) + ")");
+    return 2;  // FE_ERR_CUDA
+  }
+  return 0;
+}
 // Host-side fault injection for the allocation-failure path: with
 // FE_B200_FAIL_ALLOC_BYTES=b in the environment, every device allocation of at
 // least b bytes fails as an out-of-memory cudaMalloc would (FE_ERR_ALLOC and
@@ -180,10 +190,13 @@ __global__ void k_abs_pieces(AbsPiece* __restrict__ pc, int64_t n, const int32_t
   }
   pc[i] = a;
 }
+// partial: write the sum of squared projections `tot` of each level (the
+// share of this rank's primary levels; the ranks' shares are summed by the
+// exchange of a sharded plan and k_abs_final finishes), else the scale.
 __global__ void k_abs_join(const AbsPiece* __restrict__ pc, const int64_t* __restrict__ first,
                            int64_t nl, const double* __restrict__ scp,
                            const double* __restrict__ sck, double* __restrict__ out_d,
-                           float* __restrict__ out_f) {
+                           float* __restrict__ out_f, int partial) {
   const int64_t l = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (l >= nl) return;
   const double sk = sck[l];
@@ -208,8 +221,26 @@ __global__ void k_abs_join(const AbsPiece* __restrict__ pc, const int64_t* __res
       }
     }
     if (wc >= 0) tot += abs_run(sc, wc, scp);
+    if (partial) {
+      res = tot;
+    } else {
+      const double a2 = 1.0 / (sk * sk);
+      res = 1.0 / sqrt(fmax(a2 - tot, 1e-4 * a2));
+    }
+  }
+  out_d[l] = res;
+  if (!partial) out_f[l] = (float)res;
+}
+// the scales 1 / ||M a_l|| from the exchanged sums `tot` (in out_d)
+__global__ void k_abs_final(int64_t nl, const double* __restrict__ sck, double* __restrict__ out_d,
+                            float* __restrict__ out_f) {
+  const int64_t l = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (l >= nl) return;
+  const double sk = sck[l];
+  double res = 0.0;
+  if (sk > 0.0) {
     const double a2 = 1.0 / (sk * sk);
-    res = 1.0 / sqrt(fmax(a2 - tot, 1e-4 * a2));
+    res = 1.0 / sqrt(fmax(a2 - out_d[l], 1e-4 * a2));
   }
   out_d[l] = res;
   out_f[l] = (float)res;
@@ -221,6 +252,7 @@ __global__ void k_abs_join(const AbsPiece* __restrict__ pc, const int64_t* __res
 int plan_build(fe_plan* pl, int32_t nprob, const int64_t* n_obs, int32_t K,
                const int64_t* const* refs, const int64_t* n_levels,
                const double* const* interaction, const double* weights, int32_t device) {
+  NvtxRange nv("fe: plan build");
   if (nprob < 1 || !n_obs) {
     set_error("plan: need at least one problem");
     return 1;
@@ -323,6 +355,7 @@ int plan_build(fe_plan* pl, int32_t nprob, const int64_t* n_obs, int32_t K,
 
 // update_weights!: src/SolverCPU.jl:67-76, ext/CUDAExt.jl:112-121.
 int plan_update_weights(fe_plan* pl, const double* weights) {
+  NvtxRange nv("fe: weights and preconditioner");
   const int64_t N = pl->N;
   const int K = pl->K;
   cudaStream_t s = pl->stream;
@@ -409,6 +442,9 @@ int plan_update_weights(fe_plan* pl, const double* weights) {
         dd, its->d_rd.as<ReduceItem>(), (int64_t)its->rd.size(), LoadScaleSq{}, sums.as<double>(), sa);
     FE_CK(cudaGetLastError());
   }
+  // sharded plan: the sums of w * interaction^2 over every rank's rows
+  st = exchange(pl, sums.p, pl->P, 8, s);
+  if (st) return st;
   if (!its->pu.empty()) {
     PEpiScale epi;
     for (int k = 0; k < kMaxFE; ++k) {
@@ -459,10 +495,20 @@ int plan_update_weights(fe_plan* pl, const double* weights) {
         FE_CK(cudaGetLastError());
       }
       if (nl > 0) {
+        const int partial = pl->xchg ? 1 : 0;
         k_abs_join<<<grid1(nl, 128), 128, 0, s>>>(
             pcs.as<AbsPiece>(), first.as<int64_t>(), nl, d.scale_d[kp], d.scale_d[k],
-            pl->d_abs_scale_d[k].as<double>(), pl->d_abs_scale_f[k].as<float>());
+            pl->d_abs_scale_d[k].as<double>(), pl->d_abs_scale_f[k].as<float>(), partial);
         FE_CK(cudaGetLastError());
+        if (partial) {
+          // sharded plan: sum the ranks' shares, then finish the scales
+          st = exchange(pl, pl->d_abs_scale_d[k].p, nl, 8, s);
+          if (st) return st;
+          k_abs_final<<<grid1(nl, 128), 128, 0, s>>>(nl, d.scale_d[k],
+                                                      pl->d_abs_scale_d[k].as<double>(),
+                                                      pl->d_abs_scale_f[k].as<float>());
+          FE_CK(cudaGetLastError());
+        }
       }
       FE_CK(cudaStreamSynchronize(s));  // the host piece lists are reused
     }

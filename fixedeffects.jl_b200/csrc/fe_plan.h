@@ -11,7 +11,11 @@
 #include <string>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "fe_internal.h"
+
+struct fe_plan;
 
 namespace fe {
 
@@ -53,6 +57,23 @@ struct DeviceRestore {
   }
   DeviceRestore(const DeviceRestore&) = delete;
   DeviceRestore& operator=(const DeviceRestore&) = delete;
+};
+
+// fe_exchange_fn of include/fe_b200.h: in-place sum over ranks of `count`
+// elements (0: FP64, 1: FP32) at device address `buf`, ordered on `stream`.
+using ExchangeFn = int (*)(void* ctx, void* buf, int64_t count, int32_t dtype, void* stream);
+// calls the plan's exchange (a no-op for plans that are not sharded)
+int exchange(fe_plan* pl, void* buf, int64_t count, int elem_bytes, cudaStream_t s);
+
+// An NVTX range around a host phase of the library (plan build, a solve,
+// a column tile, a refinement round, an LSMR loop), visible on the timeline
+// of a profiler (Nsight Systems); without a profiler attached the calls
+// return at once.
+struct NvtxRange {
+  explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange&) = delete;
+  NvtxRange& operator=(const NvtxRange&) = delete;
 };
 
 // A device allocation owned by the plan.
@@ -105,6 +126,8 @@ struct Workspace {
   DevBuf small_part;  // the row-sum CTA partials of the small FEs
   DevBuf coef;
   DevBuf ystage;  // device copy of host Y for host-buffer solves
+  DevBuf xbuf;    // sharded plans: per-column norms exchanged over the ranks
+  DevBuf off01;   // sharded plans: the slot range {0, 1} of xbuf
 };
 
 // A captured run of LSMR iterations (the inner loop of one tile shape).
@@ -174,6 +197,7 @@ struct fe_plan {
   int32_t opt_absorb = 1;       // mixed residual solves project the primary FE out
   int32_t opt_exdm = 1;         // absorbed loop: fused expand + demean kernel
   int32_t opt_abs_scale = 1;    // absorbed loop: columns scaled by 1 / ||M a_l||
+  int32_t opt_exdm_pipe = -1;   // absorbed loop: pipelined fused kernel (-1 default, 0 off, 1 on)
   std::map<std::pair<int, int>, fe::LoopGraph> graphs;  // by (C, precision)
   // tuned variants per (tile width C, element size): {expand, segsum}
   std::map<std::pair<int, int>, std::pair<int, int>> tuned;
@@ -185,6 +209,9 @@ struct fe_plan {
   void* host_pinned = nullptr;  // small pinned staging for counters
   // fe_plan_scales_noalloc on a caller stream: orders it after the plan's stream
   cudaEvent_t noalloc_order = nullptr;
+  // observation-sharded plans: the sum-over-ranks exchange (fe_exchange_fn)
+  fe::ExchangeFn xchg = nullptr;
+  void* xchg_ctx = nullptr;
 
   // results of the last solve (per column)
   std::vector<double> last_test2;

@@ -126,6 +126,7 @@ int tile_width(const fe_plan* pl, int64_t remaining) {
 }
 
 int solve(fe_plan* pl, const SolveReq& rq) {
+  NvtxRange nv(rq.residuals ? "fe: solve_residuals" : "fe: solve_coefficients");
   FE_CK(cudaSetDevice(pl->device));
   const int64_t ncols = rq.ncols;
   pl->last_test2.assign((size_t)ncols, 0.0);

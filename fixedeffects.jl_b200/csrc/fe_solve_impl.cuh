@@ -25,6 +25,7 @@
 #include <vector>
 
 #pragma once
+#include "fe_exdm_pipe.cuh"
 #include "fe_kernels.cuh"
 #include "fe_plan.h"
 #include "fe_solve.h"
@@ -167,7 +168,76 @@ struct Ctx {
   double* small_part;  // the row-sum pass's CTA partials of the small FEs
   bool rowsum;         // primary and small FEs reduced by the row-sum pass
   bool absorb = false; // primary FE projected out (demean pass; mixed residual solves)
+  // observation-sharded plans: per-column norms summed over the ranks, read
+  // by the scalar phases as one slot per column
+  double* xbuf = nullptr;
+  const int64_t* off01 = nullptr;
 };
+
+// ---------------------------------------------------------------------------
+// observation-sharded plans: the exchange steps (no-ops otherwise)
+// ---------------------------------------------------------------------------
+// per-column totals of the [C][S] norm slots, summed in slot order (one CTA
+// per column, a fixed reduction tree)
+static __global__ void __launch_bounds__(256) k_slot_totals(const double* __restrict__ part, int64_t S,
+                                                     double* __restrict__ out) {
+  __shared__ double red[256];
+  const int j = blockIdx.x;
+  double t = 0.0;
+  for (int64_t q = threadIdx.x; q < S; q += 256) t += part[(int64_t)j * S + q];
+  red[threadIdx.x] = t;
+  __syncthreads();
+  for (int h = 128; h > 0; h >>= 1) {
+    if ((int)threadIdx.x < h) red[threadIdx.x] += red[threadIdx.x + h];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[j] = red[0];
+}
+
+// the norms of this rank's rows -> summed over the ranks (xbuf)
+static int xchg_slots(Ctx& c, const double* part) {
+  if (!c.pl->xchg) return 0;
+  k_slot_totals<<<c.C, 256, 0, c.s>>>(part, c.its->Se, c.xbuf);
+  FE_CK(cudaGetLastError());
+  return exchange(c.pl, c.xbuf, c.C, 8, c.s);
+}
+
+// slab rows exchanged: every FE's, or the non-primary FEs' in the absorbed
+// mode (the primary levels are this rank's own)
+static void slab_ranges(const Ctx& c, std::vector<std::pair<int64_t, int64_t>>& out) {
+  const fe_plan* pl = c.pl;
+  out.clear();
+  if (!c.absorb) {
+    out.push_back({0, pl->P});
+    return;
+  }
+  const int64_t pb = pl->lev_base[pl->primary], pe = pb + pl->nlev[pl->primary] + 1;
+  if (pb > 0) out.push_back({0, pb});
+  if (pe < pl->P) out.push_back({pe, pl->P});
+}
+// zeroed before the reductions (rows without local positions stay 0 instead
+// of keeping the last exchanged sums) ...
+static int zero_slab(Ctx& c, void* S, int elem) {
+  if (!c.pl->xchg) return 0;
+  std::vector<std::pair<int64_t, int64_t>> r;
+  slab_ranges(c, r);
+  for (const auto& q : r)
+    FE_CK(cudaMemsetAsync(static_cast<char*>(S) + (size_t)q.first * c.C * elem, 0,
+                          (size_t)(q.second - q.first) * c.C * elem, c.s));
+  return 0;
+}
+// ... and summed over the ranks after them
+static int xchg_slab(Ctx& c, void* S, int elem) {
+  if (!c.pl->xchg) return 0;
+  std::vector<std::pair<int64_t, int64_t>> r;
+  slab_ranges(c, r);
+  for (const auto& q : r) {
+    const int st = exchange(c.pl, static_cast<char*>(S) + (size_t)q.first * c.C * elem,
+                            (q.second - q.first) * c.C, elem, c.s);
+    if (st) return st;
+  }
+  return 0;
+}
 
 // Kernel variants (unroll depth = row slots per lane group per step, and
 // whether the next step's indices are prefetched).  Variant 0 is the default;
@@ -486,9 +556,103 @@ static int exdm_u(Ctx& c, Tab tab, T* rows) {
   }
 }
 
+// The pipelined fused kernel (k_exdm_pipe): FP32 rows of 32-column tiles, at
+// most one gathered (large) non-primary FE, and staging that fits the
+// shared-memory limit.  Sets *launched when it ran; otherwise the caller runs
+// k_expand_demean.  FE_OPT_EXDM_PIPE: -1 the default configuration (the
+// first of kExdmPrefer that fits), 1 or 2 one configuration, 0 off.
+static int try_exdm_pipe(Ctx& c, const float* tab, float* rows, int* launched) {
+  static const int kExdmPrefer[] = {1, 2};
+  *launched = 0;
+  const fe_plan* pl = c.pl;
+  if (pl->opt_exdm_pipe == 0) return 0;
+  static int smem_max = -1;  // opt-in shared memory per block of the device
+  if (smem_max < 0) {
+    int v = 0;
+    FE_CK(cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, pl->device));
+    smem_max = v;
+  }
+  ExdmFEs lf{};
+  int nl = 0, ns = 0;
+  bool w = false;
+  for (int k = 0; k < pl->K; ++k) {
+    const bool small = ((c.its->small_mask >> k) & 1u) != 0;
+    if (pl->weighted || pl->interacted[k]) w = true;
+    if (k == pl->primary) continue;
+    if (small) {
+      ++ns;
+      continue;
+    }
+    if (nl == 2) return 0;
+    lf.large[nl] = k;
+    lf.large_base[nl] = pl->lev_base[k];
+    ++nl;
+  }
+  if (nl > 1) return 0;
+  const int nsr = ns ? c.its->small_rows : 0;
+  // + the static norm scratch (kWarps x 32 doubles)
+  auto fits = [&](int cfg) {
+    const ExdmCfg k = exdm_cfg(cfg);
+    return exdm_pipe_smem(nl, nsr, k.stages, k.per_group) + kWarps * 32 * sizeof(double) <=
+           (size_t)smem_max;
+  };
+  int cfg = -1;
+  if (pl->opt_exdm_pipe > 0) {
+    if (fits(pl->opt_exdm_pipe)) cfg = pl->opt_exdm_pipe;
+  } else {
+    for (int k : kExdmPrefer)
+      if (fits(k)) {
+        cfg = k;
+        break;
+      }
+  }
+  if (cfg < 0) return 0;
+  const ExdmCfg kc = exdm_cfg(cfg);
+  ExdmLaunch a{};
+  a.d = c.d;
+  a.items = c.its->d_dm.as<ExpandItem>();
+  a.n_items = (int64_t)c.its->dm.size();
+  a.tab = tab;
+  a.rows = rows;
+  a.inst = c.inst;
+  a.rs.sum = c.S;
+  a.rs.small_part = c.small_part;
+  a.rs.small_rows = c.its->small_rows;
+  for (int k = 0; k < c.d.K; ++k)
+    if ((c.its->small_mask >> k) & 1u) {
+      a.rs.small_fe[a.rs.n_small] = k;
+      a.rs.small_off[a.rs.n_small] = c.its->small_off[k];
+      ++a.rs.n_small;
+    }
+  for (int r = 0; r < c.its->small_rows; ++r) a.sr.slab_row[r] = c.its->small_slab_row[(size_t)r];
+  a.lf = lf;
+  a.part = c.part_e;
+  a.S = c.its->Se;
+  // one CTA per SM (the staging fills the shared memory); the norm slots are
+  // the expand's, so the grid must not exceed their count
+  a.grid = std::max<int64_t>(1, std::min<int64_t>(c.its->Se, c.its->sms));
+  a.smem = exdm_pipe_smem(nl, nsr, kc.stages, kc.per_group);
+  a.stream = c.s;
+  int st = launch_exdm_pipe(a, nl, ns, w, cfg);
+  if (st) return st;
+  if (c.its->small_rows > 0) {
+    k_small_combine<float, 32><<<(unsigned)c.its->small_rows, kThreads, 0, c.s>>>(
+        c.small_part, (int)a.grid, c.its->small_rows, a.sr, static_cast<float*>(c.S),
+        c.d.active_pre);
+    FE_CK(cudaGetLastError());
+  }
+  *launched = 1;
+  return 0;
+}
+
 template <typename T, int C, class Tab>
 static int launch_expand_demean(Ctx& c, Tab tab, T* rows, const char* name, double bytes) {
   ProfScope ps(c.pl, name, bytes);
+  if constexpr (C == 32 && std::is_same<T, float>::value) {
+    int launched = 0;
+    const int st = try_exdm_pipe(c, tab.tab, rows, &launched);
+    if (st || launched) return st;
+  }
   // unroll depth 4 (measured fastest on the worker/firm/year workload), or
   // that of a forced expand variant
   const int var = c.pl->opt_ex_variant >= 0 ? c.pl->opt_ex_variant : 3;
@@ -605,6 +769,12 @@ static int launch_scalar_phase(Ctx& c, int phase, int init_mode) {
       break;
     default:
       break;
+  }
+  if (c.pl->xchg && a.part0) {
+    // sharded plan: the exchanged per-column totals, one slot per column
+    a.part0 = c.xbuf;
+    a.off0 = c.off01;
+    a.S0 = 1;
   }
   launch_scalar(a, c.n_inst, c.s);
   FE_CK(cudaGetLastError());
@@ -746,6 +916,15 @@ static int prepare(fe_plan* pl, int C, int sT, bool mixed, Ctx& c) {
   if ((st = w.small_part.ensure((size_t)its->sms * 8 * std::max(its->small_rows, 1) * nC * 8)))
     return st;
   if ((st = w.counters.ensure(64))) return st;
+  if (pl->xchg) {
+    if ((st = w.xbuf.ensure(nC * 8))) return st;
+    if (!w.off01.p) {
+      const int64_t off[2] = {0, 1};
+      if ((st = w.off01.ensure(sizeof(off)))) return st;
+      FE_CK(cudaMemcpyAsync(w.off01.p, off, sizeof(off), cudaMemcpyHostToDevice, pl->stream));
+      FE_CK(cudaStreamSynchronize(pl->stream));
+    }
+  }
   if (!pl->host_pinned) FE_CK(cudaMallocHost(&pl->host_pinned, 64));
   c.pl = pl;
   c.its = its;
@@ -767,6 +946,8 @@ static int prepare(fe_plan* pl, int C, int sT, bool mixed, Ctx& c) {
   c.S = w.S.p;
   c.small_part = w.small_part.as<double>();
   c.rowsum = use_rowsum(pl, C);
+  c.xbuf = pl->xchg ? w.xbuf.as<double>() : nullptr;
+  c.off01 = pl->xchg ? w.off01.as<int64_t>() : nullptr;
   // coefficient-side slabs start at zero (levels without observations and
   // the null levels are never written afterwards)
   FE_CK(cudaMemsetAsync(w.V.p, 0, P * nC * (size_t)sT, c.s));
@@ -781,6 +962,7 @@ static int prepare(fe_plan* pl, int C, int sT, bool mixed, Ctx& c) {
 }
 
 static int load_tile(fe_plan* pl, Ctx& c, const SolveReq& rq, int64_t col0, int ncols) {
+  NvtxRange nv("fe: load tile");
   const int64_t N = pl->N;
   if (N == 0) return 0;
   const double* sw = pl->weighted ? pl->d_sw_orig.as<double>() : nullptr;
@@ -798,6 +980,7 @@ static int load_tile(fe_plan* pl, Ctx& c, const SolveReq& rq, int64_t col0, int 
 }
 
 static int unload_tile(fe_plan* pl, Ctx& c, const SolveReq& rq, int64_t col0, int ncols) {
+  NvtxRange nv("fe: unload tile");
   const int64_t N = pl->N;
   if (N == 0) return 0;
   const double* sw = pl->weighted ? pl->d_sw_orig.as<double>() : nullptr;
@@ -853,10 +1036,12 @@ static void init_insts(fe_plan* pl, const SolveReq& rq, int C, int ncols, std::v
 template <class Body>
 static int run_loop(fe_plan* pl, Ctx& c, int prec, int64_t cap, int32_t nact0, Body body,
                     int64_t* done_iters) {
+  NvtxRange nv("fe: LSMR loop");
   int32_t nact = nact0;
   const int m = std::max(1, pl->opt_check_every);
   int64_t it = 0;
-  const bool graph = pl->opt_graph != 0 && !pl->prof.on;
+  // sharded plans exchange between launches: no graph replay
+  const bool graph = pl->opt_graph != 0 && !pl->prof.on && !pl->xchg;
   LoopGraph* lg = nullptr;
   if (graph) {
     size_t key = (size_t)c.C * 1000003u ^ (size_t)m;
@@ -872,6 +1057,7 @@ static int run_loop(fe_plan* pl, Ctx& c, int prec, int64_t cap, int32_t nact0, B
     key = key * 3 + (c.absorb ? 1u : 0u);
     key = key * 3 + (size_t)pl->opt_exdm;
     key = key * 3 + (size_t)pl->opt_abs_scale;
+    key = key * 3 + (size_t)(pl->opt_exdm_pipe + 1);
     lg = &pl->graphs[{c.C, prec}];
     if (!lg->exec || lg->key != key) {
       if (lg->exec) {
@@ -925,6 +1111,7 @@ void tune_cache_store(fe_plan* pl, int C, int sT, int ex, int seg);
 // contents are irrelevant to the timing and are left as scratch values)
 template <typename T, int C>
 static int autotune(fe_plan* pl, Ctx& c, T* rows, T* levels, bool resid_form = false) {
+  NvtxRange nv("fe: autotune");
   // tuning key: element size, + 100 for the mixed mode's FP64 refinement
   // kernels (a different expand epilogue than the plain FP64 loop)
   const int kind = (int)sizeof(T) + (resid_form ? 100 : 0);
@@ -1060,6 +1247,7 @@ static int download_coefs(fe_plan* pl, Ctx& c, const TX* X, const SolveReq& rq) 
 template <typename T, int C>
 static int solve_plain_tile(fe_plan* pl, const SolveReq& rq, int64_t col0, int ncols,
                             std::vector<Inst>& out) {
+  NvtxRange nv("fe: tile (plain LSMR)");
   Ctx c;
   int st = prepare(pl, C, (int)sizeof(T), false, c);
   if (st) return st;
@@ -1078,9 +1266,11 @@ static int solve_plain_tile(fe_plan* pl, const SolveReq& rq, int64_t col0, int n
   T* ST = static_cast<T*>(c.S);
   // warm start x = A'b (src/AbstractFixedEffectSolver.jl:56); solve_coefficients! starts at 0
   if (rq.residuals) {
+    if ((st = zero_slab(c, S64, 8))) return st;
     if ((st = launch_segsum<double, C>(c, LoadIn<double, double, vec_of<double, C>()>{B64}, S64, "segsum_warm", 0.0,
                                         c.rowsum, "rowsum_warm", 0.0)))
       return st;
+    if ((st = xchg_slab(c, S64, 8))) return st;
     if ((st = launch_pupdate<C>(c, S64, PEpiStoreX<T, vec_of<double, C>()>{X, true}, nullptr, nullptr, "pupdate_warm", 0.0)))
       return st;
   }
@@ -1090,6 +1280,7 @@ static int solve_plain_tile(fe_plan* pl, const SolveReq& rq, int64_t col0, int n
                                 EpiBminusAx<T, T, vec_of<T, C>()>{B64, U, nullptr, c.inst, 0}, c.part_e,
                                 "expand_init", by.expand)))
     return st;
+  if ((st = xchg_slots(c, c.part_e))) return st;
   if ((st = launch_scalar_phase(c, PH_INIT_BETA, 0))) return st;
   PEpiLsmr<T, vec_of<T, C>()> pe{};
   pe.V = V;
@@ -1097,9 +1288,11 @@ static int solve_plain_tile(fe_plan* pl, const SolveReq& rq, int64_t col0, int n
   pe.Hb = w.Hb.as<T>();
   pe.X = X;
   pe.inst = c.inst;
+  if ((st = zero_slab(c, ST, (int)sizeof(T)))) return st;
   if ((st = launch_segsum<T, C>(c, LoadIn<T, T, vec_of<T, C>()>{U}, ST, "segsum", by.segsum, fuse,
                                 "rowsum", by.rowsum)))
     return st;
+  if ((st = xchg_slab(c, ST, (int)sizeof(T)))) return st;
   if ((st = launch_pupdate<C>(c, ST, pe, c.part_a, c.part_b, "pupdate", by.pupdate))) return st;
   if ((st = launch_scalar_phase(c, PH_INIT_ALPHA, 1))) return st;
   int32_t nact = 0;
@@ -1112,10 +1305,13 @@ static int solve_plain_tile(fe_plan* pl, const SolveReq& rq, int64_t col0, int n
     int e;
     if ((e = launch_expand<T, C>(c, TabOne<T, T, vec_of<T, C>()>{V}, ee, c.part_e, "expand", by.expand)))
       return e;
+    if ((e = xchg_slots(c, c.part_e))) return e;
     if ((e = launch_scalar_phase(c, PH_BETA, 0))) return e;
+    if ((e = zero_slab(c, ST, (int)sizeof(T)))) return e;
     if ((e = launch_segsum<T, C>(c, LoadIn<T, T, vec_of<T, C>()>{U}, ST, "segsum", by.segsum, fuse,
                                  "rowsum", by.rowsum)))
       return e;
+    if ((e = xchg_slab(c, ST, (int)sizeof(T)))) return e;
     if ((e = launch_pupdate<C>(c, ST, pe, c.part_a, c.part_b, "pupdate", by.pupdate))) return e;
     return launch_scalar_phase(c, PH_ALPHA, 0);
   };
@@ -1146,6 +1342,7 @@ static int solve_plain_tile(fe_plan* pl, const SolveReq& rq, int64_t col0, int n
 template <int C>
 static int solve_mixed_tile(fe_plan* pl, const SolveReq& rq, int64_t col0, int ncols,
                             std::vector<Inst>& out) {
+  NvtxRange nv("fe: tile (mixed precision)");
   Ctx c;
   int st = prepare(pl, C, 4, true, c);
   if (st) return st;
@@ -1182,9 +1379,11 @@ static int solve_mixed_tile(fe_plan* pl, const SolveReq& rq, int64_t col0, int n
         c.d.scale_f[k] = pl->d_abs_scale_f[k].as<float>();
       }
   if (rq.residuals && pl->opt_mixed_warm && !absorb) {
+    if ((st = zero_slab(c, S64, 8))) return st;
     if ((st = launch_segsum<double, C>(c, LoadIn<double, double, vec_of<double, C>()>{B64}, S64, "segsum_warm", 0.0,
                                         c.rowsum, "rowsum_warm", 0.0)))
       return st;
+    if ((st = xchg_slab(c, S64, 8))) return st;
     if ((st = launch_pupdate<C>(c, S64, PEpiStoreX<double, vec_of<double, C>()>{X64, true}, nullptr, nullptr,
                                 "pupdate_warm", 0.0)))
       return st;
@@ -1212,11 +1411,13 @@ static int solve_mixed_tile(fe_plan* pl, const SolveReq& rq, int64_t col0, int n
   int64_t total_it = 0;
   const bool fuse = c.rowsum;
   for (int round = 0; round <= pl->opt_max_rounds + 1; ++round) {
+    NvtxRange nvr("fe: FP64 refinement round");
     FE_CK(cudaMemsetAsync(c.counters, 0, 3 * sizeof(int32_t), c.s));
     // r = b - A (x64 + dx32) in FP64, with the FP32 copy as the next inner u
     // (absorbed: r = M (b - A_r x), projected and copied by the demean pass)
     // absorbed: round 0 starts from x = 0, so r0 = M b comes straight from b
     const bool from_b = absorb && round == 0;
+    if ((st = zero_slab(c, S64, 8))) return st;
     if (!from_b &&
         (st = launch_expand<double, C>(
              c, TabSum64<vec_of<double, C>()>{X64, X},
@@ -1235,6 +1436,8 @@ static int solve_mixed_tile(fe_plan* pl, const SolveReq& rq, int64_t col0, int n
                                               "segsum64", by.segsum64, fuse, "rowsum64", by.rowsum64))) {
       return st;
     }
+    if ((st = xchg_slots(c, c.part_e))) return st;
+    if ((st = xchg_slab(c, S64, 8))) return st;
     if ((st = launch_pupdate<C>(c, S64, pg, c.part_a, c.part_b, "grad64",
                                 absorb ? by.grad64_np : by.grad64)))
       return st;
@@ -1247,6 +1450,7 @@ static int solve_mixed_tile(fe_plan* pl, const SolveReq& rq, int64_t col0, int n
       if (absorb) {
         // u = M (av A_r v + au u): the expand without the primary FE, then the
         // projection (which also gives ||u|| and the small FEs' sums)
+        if ((e = zero_slab(c, S32, 4))) return e;
         if (pl->opt_exdm) {
           if ((e = launch_expand_demean<float, C>(c, TabOne<float, float, vec_of<float, C>()>{VS}, U,
                                                   "expand_demean", by.expand_demean)))
@@ -1257,20 +1461,25 @@ static int solve_mixed_tile(fe_plan* pl, const SolveReq& rq, int64_t col0, int n
             return e;
           if ((e = launch_demean<float, C>(c, U, nullptr, S32, "demean", by.demean))) return e;
         }
+        if ((e = xchg_slots(c, c.part_e))) return e;
         if ((e = launch_scalar_phase(c, PH_BETA, 0))) return e;
         if ((e = launch_segsum<float, C>(c, LoadIn<float, float, vec_of<float, C>()>{U}, S32, "segsum",
                                          by.segsum, true, "", 0.0, true)))
           return e;
+        if ((e = xchg_slab(c, S32, 4))) return e;
         if ((e = launch_pupdate<C>(c, S32, pe, c.part_a, c.part_b, "pupdate", by.pupdate_np))) return e;
         return launch_scalar_phase(c, PH_ALPHA, 0);
       }
       if ((e = launch_expand<float, C>(c, TabOne<float, float, vec_of<float, C>()>{V}, ee, c.part_e,
                                        "expand", by.expand)))
         return e;
+      if ((e = xchg_slots(c, c.part_e))) return e;
       if ((e = launch_scalar_phase(c, PH_BETA, 0))) return e;
+      if ((e = zero_slab(c, S32, 4))) return e;
       if ((e = launch_segsum<float, C>(c, LoadIn<float, float, vec_of<float, C>()>{U}, S32, "segsum",
                                        by.segsum, fuse, "rowsum", by.rowsum)))
         return e;
+      if ((e = xchg_slab(c, S32, 4))) return e;
       if ((e = launch_pupdate<C>(c, S32, pe, c.part_a, c.part_b, "pupdate", by.pupdate))) return e;
       return launch_scalar_phase(c, PH_ALPHA, 0);
     };

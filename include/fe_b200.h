@@ -84,6 +84,14 @@ extern "C" {
 #define FE_OPT_ABSORB_SCALE 16 /* 1 (default): the absorbed LSMR scales the other FEs'
                                   columns by 1 / ||M a_l|| (their norms after the
                                   projection); 0: by the Jacobi scale 1 / ||a_l|| */
+#define FE_OPT_EXDM_PIPE 17  /* absorbed loop kernel: the pipelined fused kernel (the
+                                next item's rows and gathered coefficient rows staged
+                                by asynchronous copies) where the plan fits it (at most
+                                one gathered non-primary FE, staging within the
+                                shared-memory limit): -1 (default) the first
+                                configuration that fits, 1 small-FE sums in one table
+                                per lane group, 2 one table per warp; 0: the
+                                unpipelined kernel */
 
 typedef struct fe_plan fe_plan;
 
@@ -133,6 +141,45 @@ int fe_plan_create_batch(fe_plan** out, int32_t n_problems, const int64_t* n_obs
                          const int64_t* const* refs, const int64_t* n_levels,
                          const double* const* interaction, const double* weights,
                          int32_t device);
+
+/*
+ * Observation sharding of one problem over several GPUs (one process per GPU).
+ *
+ * fe_exchange_fn: replaces the `count` elements at `buf` (device memory of
+ * the plan's device; dtype FE_XCHG_F64 or FE_XCHG_F32) with their elementwise
+ * sum over all ranks, ordered on `stream` (a cudaStream_t; completing the sum
+ * before returning also satisfies the ordering).  Returns 0 on success; a
+ * non-zero return fails the library call with FE_ERR_CUDA.  Every rank's
+ * plan calls it the same number of times in the same order with the same
+ * counts, as long as every rank makes the same library calls with the same
+ * column counts, tolerances and options.
+ *
+ * fe_plan_create_sharded builds the plan of one rank's share of the
+ * observations of a single problem.  refs hold GLOBAL 1-based level ids and
+ * n_levels the GLOBAL level counts (the same on every rank); the share must
+ * hold whole levels of the primary FE (the FE with the most levels, the
+ * first of them on ties), so no primary level has observations on two
+ * ranks, and at least one observation.  The preconditioner (Jacobi scales
+ * src/SolverCPU.jl:78-89, and the absorbed-mode column norms) is computed
+ * from sums exchanged over the ranks.  Every solve then runs LSMR over the
+ * global problem: each iteration exchanges the per-column norms of the local
+ * rows and the per-level sums A'u of the local rows (the step between the
+ * two matrix-vector products of src/utils/lsmr.jl:104-109); the
+ * coefficient-side vectors are replicated and stay bitwise identical on
+ * every rank, because the exchanged sums are.  Residuals are returned for
+ * the rank's own observations; fe_solve_coefficients returns the same global
+ * coefficients on every rank (fe_normalize_coefficients, whose connected
+ * components span all ranks' observations, refuses a sharded plan).  Graph replay is off for sharded plans (the
+ * exchange runs between kernel launches).  No counterpart in the reference,
+ * which solves on one device (ext/CUDAExt.jl:99-165).
+ */
+typedef int (*fe_exchange_fn)(void* ctx, void* buf, int64_t count, int32_t dtype, void* stream);
+#define FE_XCHG_F64 0
+#define FE_XCHG_F32 1
+int fe_plan_create_sharded(fe_plan** out, int64_t n_obs, int32_t n_fe, const int64_t* const* refs,
+                           const int64_t* n_levels, const double* const* interaction,
+                           const double* weights, int32_t device, fe_exchange_fn exchange,
+                           void* ctx);
 
 /* update_weights!(feM, w): src/SolverCPU.jl:67-76, ext/CUDAExt.jl:112-121. */
 int fe_plan_update_weights(fe_plan* plan, const double* weights);

@@ -416,14 +416,17 @@ def test_absorbed_primary_matches_oracle(fe, oracle, case):
     R_o, _, _ = oracle.solve_residuals_cols(Y, refs, None, inter, w, tol=1e-8)
     fes = [fe.FixedEffect(r, interaction=a) for r, a in zip(refs, inter)]
     out = []
-    # (absorb, fused expand + demean, columns scaled by 1/||M a_l||): default,
-    # separate kernels, Jacobi scales of A_r, full LSMR
-    for absorb, fused, ascale in ((1, 1, 1), (1, 0, 1), (1, 1, 0), (0, 1, 1)):
+    # (absorb, fused expand + demean, columns scaled by 1/||M a_l||, pipelined
+    # fused kernel): default, the unpipelined fused kernel, separate kernels,
+    # Jacobi scales of A_r, full LSMR
+    for absorb, fused, ascale, pipe in ((1, 1, 1, -1), (1, 1, 1, 0), (1, 1, 1, 1), (1, 1, 1, 2),
+                                        (1, 0, 1, -1), (1, 1, 0, -1), (0, 1, 1, -1)):
         feM = fe.AbstractFixedEffectSolver(fes, w, "CUDA", np.float64, precision="mixed")
         feM.set_option(fe._lib.FE_OPT_TILE, 32)
         feM.set_option(fe._lib.FE_OPT_ABSORB, absorb)
         feM.set_option(fe._lib.FE_OPT_FUSED_DEMEAN, fused)
         feM.set_option(fe._lib.FE_OPT_ABSORB_SCALE, ascale)
+        feM.set_option(fe._lib.FE_OPT_EXDM_PIPE, pipe)
         R, its, cvs = feM.solve_residuals(Y.copy(), tol=1e-8)
         R2, its2, _ = feM.solve_residuals(Y.copy(), tol=1e-8)
         feM.close()
