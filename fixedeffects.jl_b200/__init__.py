@@ -622,8 +622,44 @@ class BatchSolver:
         out = [Y[self.offsets[p]:self.offsets[p + 1]].copy() for p in range(self.nprob)]
         return out, pit, pcv.astype(bool)
 
+    def solve_residuals_device(self, y, tol: float | None = None, maxiter: int = 100_000):
+        """Solves the problems' columns concatenated in one contiguous CUDA
+        torch tensor (problem p at rows offsets[p]:offsets[p+1]), in place on
+        the current torch stream; returns (y, iterations, converged) per
+        problem."""
+        import torch
+        if tol is None:
+            tol = math.sqrt(np.finfo(self.T).eps)
+        if y.dtype not in (torch.float64, torch.float32) or y.dim() != 1 or not y.is_contiguous():
+            raise ValueError("device y must be a contiguous float32/float64 vector")
+        if y.shape[0] != self.N:
+            raise ValueError("FixedEffects must have the same length as y")
+        L = _lib.load()
+        _lib.check(L.fe_plan_set_stream(self._h, torch.cuda.current_stream(y.device).cuda_stream))
+        its = np.zeros(1, dtype=np.int64)
+        cvs = np.zeros(1, dtype=np.uint8)
+        dt = FE_DTYPE_F64 if y.dtype == torch.float64 else FE_DTYPE_F32
+        _lib.check(L.fe_solve_residuals_device(self._h, y.data_ptr(), dt, 1, self.N,
+                                               self.precision, float(tol), int(maxiter),
+                                               its.ctypes.data_as(_lib._i64p),
+                                               cvs.ctypes.data_as(_lib._u8p)))
+        pit = np.zeros(self.nprob, dtype=np.int64)
+        pcv = np.zeros(self.nprob, dtype=np.uint8)
+        _lib.check(L.fe_plan_problem_results(self._h, pit.ctypes.data_as(_lib._i64p),
+                                             pcv.ctypes.data_as(_lib._u8p)))
+        return y, pit, pcv.astype(bool)
+
     def set_option(self, option: int, value: float) -> None:
         _lib.check(_lib.load().fe_plan_set_option(self._h, option, float(value)))
+
+    def last_solve_info(self, ncols: int = 1):
+        return FixedEffectSolverB200.last_solve_info(self, ncols)
+
+    def kernel_stats(self):
+        return FixedEffectSolverB200.kernel_stats(self)
+
+    def reset_stats(self):
+        _lib.check(_lib.load().fe_plan_reset_stats(self._h))
 
     def integer_plan(self):
         """(perm0, offsets[k], segperm[k]) over the concatenated problems;
