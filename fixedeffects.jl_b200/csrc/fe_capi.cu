@@ -10,6 +10,7 @@
 #include "../../include/fe_b200.h"
 #include "fe_plan.h"
 #include "fe_solve.h"
+#include "fe_staging.h"
 
 using fe::set_error;
 
@@ -63,19 +64,28 @@ int create_common(fe_plan** out, int32_t nprob, const int64_t* n_obs, int32_t K,
 // upload is queued at once on an upload stream with one event per tile, the
 // tile's solve waits for its event, and its download runs on a download
 // stream once the solve is done, so transfers in both directions overlap the
-// solves of the other tiles.  Pageable columns are copied tile by tile on the
-// plan's stream.
+// solves of the other tiles.  Pageable columns go through the plan's pinned
+// staging ring (fe_staging.cu), with the same overlap; small pageable solves
+// are copied tile by tile on the plan's stream.
 struct HostXfer {
   fe_plan* pl = nullptr;
   void* const* cols = nullptr;
   size_t bytes = 0;  // per column
   bool pinned = false;
+  fe::PageableStager* stager = nullptr;  // pageable columns through the pinned ring
   cudaStream_t up = nullptr, down = nullptr;
   std::vector<cudaEvent_t> ev;  // per tile: upload done, then solve done
   std::vector<int64_t> tile0;   // first column of each tile
   size_t tile = 0;
   char* stage() const { return static_cast<char*>(pl->ws.ystage.p); }
+  // waits for the staged downloads; the first staging error, or 0
+  int end_staging() {
+    fe::PageableStager* x = stager;
+    stager = nullptr;
+    return fe::stager_end(x);
+  }
   ~HostXfer() {
+    end_staging();
     if (up) cudaStreamSynchronize(up);
     if (down) cudaStreamSynchronize(down);
     for (cudaEvent_t e : ev) cudaEventDestroy(e);
@@ -92,6 +102,7 @@ int xfer_error(const char* what, cudaError_t e) {
 
 int xfer_before(void* ctx, int64_t col0, int nc) {
   HostXfer& x = *static_cast<HostXfer*>(ctx);
+  if (x.stager) return fe::stager_before_tile(x.stager, x.tile);
   cudaError_t e = cudaSuccess;
   if (x.pinned) {
     e = cudaStreamWaitEvent(x.pl->stream, x.ev[2 * x.tile], 0);
@@ -105,6 +116,7 @@ int xfer_before(void* ctx, int64_t col0, int nc) {
 
 int xfer_after(void* ctx, int64_t col0, int nc) {
   HostXfer& x = *static_cast<HostXfer*>(ctx);
+  if (x.stager) return fe::stager_after_tile(x.stager, x.tile++);
   cudaError_t e = cudaSuccess;
   cudaStream_t s = x.pl->stream;
   if (x.pinned) {
@@ -190,11 +202,14 @@ int solve_common(fe_plan* plan, void* Y, void* const* cols, int32_t dtype, int64
     x.bytes = (size_t)N * es;
     x.pinned = true;
     for (int64_t j = 0; j < ncols && x.pinned; ++j) x.pinned = is_pinned(cols[j]);
-    if (x.pinned) {
-      for (int64_t c0 = 0; c0 < ncols; c0 += std::min<int64_t>(fe::tile_width(plan, ncols - c0),
-                                                                ncols - c0))
-        x.tile0.push_back(c0);
-      x.tile0.push_back(ncols);
+    for (int64_t c0 = 0; c0 < ncols; c0 += std::min<int64_t>(fe::tile_width(plan, ncols - c0),
+                                                              ncols - c0))
+      x.tile0.push_back(c0);
+    x.tile0.push_back(ncols);
+    if (!x.pinned && (size_t)N * (size_t)ncols * es >= fe::kStageMinBytes) {
+      st = fe::stager_begin(plan, cols, x.bytes, x.tile0, x.stage(), &x.stager);
+      if (st) return st;
+    } else if (x.pinned) {
       cudaError_t e = cudaStreamCreateWithFlags(&x.up, cudaStreamNonBlocking);
       if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&x.down, cudaStreamNonBlocking);
       // the uploads must not overtake work already queued on the plan's
@@ -228,6 +243,7 @@ int solve_common(fe_plan* plan, void* Y, void* const* cols, int32_t dtype, int64
   }
   st = fe::solve(plan, rq);
   if (st) return st;
+  if ((st = x.end_staging())) return st;
   cudaError_t e = cudaStreamSynchronize(plan->stream);
   if (e == cudaSuccess && x.down) e = cudaStreamSynchronize(x.down);
   if (e != cudaSuccess) {

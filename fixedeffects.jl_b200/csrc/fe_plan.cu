@@ -775,6 +775,8 @@ int plan_destroy(fe_plan* pl) {
   }
   if (pl->host_pinned) cudaFreeHost(pl->host_pinned);
   if (pl->noalloc_order) cudaEventDestroy(pl->noalloc_order);
+  if (pl->ring_up) cudaFreeHost(pl->ring_up);
+  if (pl->ring_down) cudaFreeHost(pl->ring_down);
   for (auto& g : pl->graphs)
     if (g.second.exec) cudaGraphExecDestroy(g.second.exec);
   cudaStream_t s = pl->stream;

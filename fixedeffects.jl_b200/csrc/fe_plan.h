@@ -209,6 +209,10 @@ struct fe_plan {
   void* host_pinned = nullptr;  // small pinned staging for counters
   // fe_plan_scales_noalloc on a caller stream: orders it after the plan's stream
   cudaEvent_t noalloc_order = nullptr;
+  // pinned staging rings of pageable host-buffer solves (fe_staging.cu)
+  void* ring_up = nullptr;
+  void* ring_down = nullptr;
+  size_t ring_slot_bytes = 0;
   // observation-sharded plans: the sum-over-ranks exchange (fe_exchange_fn)
   fe::ExchangeFn xchg = nullptr;
   void* xchg_ctx = nullptr;

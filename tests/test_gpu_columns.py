@@ -65,3 +65,26 @@ def test_columns_mixed_types_and_readonly(fe, synth):
     with pytest.raises(ValueError):
         feM.solve_residuals([Y[:-1, 0]], tol=1e-8)
     feM.close()
+
+
+def test_pageable_staging_ring_multi_chunk(fe):
+    """Pageable columns longer than one pinned ring slot (16 MB), over two
+    tiles (32 + 1 columns): the staged uploads and downloads give the
+    device-resident solve's residuals bit for bit."""
+    import torch
+    rng = np.random.default_rng(12)
+    N = 2_200_000  # 17.6 MB per FP64 column: two ring chunks
+    r1 = rng.integers(1, 200_001, N)
+    r2 = rng.integers(1, 31, N)
+    fes = [fe.FixedEffect(r1), fe.FixedEffect(r2)]
+    Y = np.asfortranarray(rng.standard_normal((N, 33)))
+    feM = fe.AbstractFixedEffectSolver(fes, None, "CUDA", np.float32)
+    D = torch.from_numpy(np.ascontiguousarray(Y.T)).cuda().t()
+    Dr, its_d, _ = feM.solve_residuals(D, tol=1e-8)
+    Rd = Dr.cpu().numpy()
+    P = Y.copy(order="F")  # pageable
+    R, its, cvs = feM.solve_residuals(P, tol=1e-8)
+    feM.close()
+    assert cvs.all()
+    assert np.array_equal(R, Rd)
+    assert np.array_equal(its, its_d)
