@@ -876,8 +876,10 @@ static Bytes alg_bytes(const fe_plan* pl, const ItemSet* its, int C, int sT) {
     b.demean = keys + 2.0 * N * C * sT + Pp * sT;
     b.demean64 = keys64 + 2.0 * N * C * 8.0 + N * C * 4.0 + Pp * 8.0;
     b.pupdate_np = 9.0 * Pnp * C * sT;
-    // fused: the expand's bytes plus the primary and small-FE keys and scales
-    b.expand_demean = b.expand_abs + keys + Pp * sT;
+    // fused: the expand's bytes (which already hold every non-primary FE's
+    // refs and weights, the small FEs' included) plus the primary FE's keys,
+    // weights and scales
+    b.expand_demean = b.expand_abs + N * (4.0 + (cwp ? sT : 0)) + Pp * sT;
     b.grad64_np = Pnp * C * (8.0 + 4.0 + 8.0 + 4.0 + 8.0);
   }
   b.pupdate = 9.0 * P * C * sT;
