@@ -387,6 +387,15 @@ int fe_plan_set_option(fe_plan* plan, int32_t option, double value) {
     case FE_OPT_ABSORB_SCALE:
       plan->opt_abs_scale = value != 0 ? 1 : 0;
       return FE_OK;
+    case FE_OPT_FIRM_ATOMIC: {
+      const int v = (int)value;
+      if (v < -1 || v > 1) {
+        set_error("gathered-FE reduction option must be -1 (tuned), 0 or 1");
+        return FE_ERR_INVALID;
+      }
+      plan->opt_firm_atomic = v;
+      return FE_OK;
+    }
     case FE_OPT_EXDM_PIPE: {
       const int v = (int)value;
       if (v < -1 || v > 2) {

@@ -9,9 +9,9 @@ namespace fe {
 
 namespace {
 
-template <int NL, int NS, bool W, int STG, bool PG>
+template <int NL, int NS, bool W, int STG, bool PG, bool ATOM = false>
 int launch_one(const ExdmLaunch& a) {
-  auto kern = k_exdm_pipe<NL, NS, W, STG, PG>;
+  auto kern = k_exdm_pipe<NL, NS, W, STG, PG, ATOM>;
   static size_t attr_smem = 0;  // per instantiation: the opt-in size set so far
   if (a.smem > attr_smem) {
     FE_CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)a.smem));
@@ -24,26 +24,29 @@ int launch_one(const ExdmLaunch& a) {
 }
 
 template <int NL, int NS, bool W>
-int launch_cfg(const ExdmLaunch& a, int cfg) {
+int launch_cfg(const ExdmLaunch& a, int cfg, bool atomic) {
+  if constexpr (NL == 1) {
+    if (atomic) return launch_one<NL, NS, W, 2, true, true>(a);
+  }
   return cfg == 2 ? launch_one<NL, NS, W, 2, false>(a) : launch_one<NL, NS, W, 2, true>(a);
 }
 
 }  // namespace
 
-int launch_exdm_pipe(const ExdmLaunch& a, int nl, int ns, bool w, int cfg) {
+int launch_exdm_pipe(const ExdmLaunch& a, int nl, int ns, bool w, int cfg, bool atomic) {
   switch ((nl * 3 + ns) * 2 + (w ? 1 : 0)) {
-    case 0: return launch_cfg<0, 0, false>(a, cfg);
-    case 1: return launch_cfg<0, 0, true>(a, cfg);
-    case 2: return launch_cfg<0, 1, false>(a, cfg);
-    case 3: return launch_cfg<0, 1, true>(a, cfg);
-    case 4: return launch_cfg<0, 2, false>(a, cfg);
-    case 5: return launch_cfg<0, 2, true>(a, cfg);
-    case 6: return launch_cfg<1, 0, false>(a, cfg);
-    case 7: return launch_cfg<1, 0, true>(a, cfg);
-    case 8: return launch_cfg<1, 1, false>(a, cfg);
-    case 9: return launch_cfg<1, 1, true>(a, cfg);
-    case 10: return launch_cfg<1, 2, false>(a, cfg);
-    default: return launch_cfg<1, 2, true>(a, cfg);
+    case 0: return launch_cfg<0, 0, false>(a, cfg, atomic);
+    case 1: return launch_cfg<0, 0, true>(a, cfg, atomic);
+    case 2: return launch_cfg<0, 1, false>(a, cfg, atomic);
+    case 3: return launch_cfg<0, 1, true>(a, cfg, atomic);
+    case 4: return launch_cfg<0, 2, false>(a, cfg, atomic);
+    case 5: return launch_cfg<0, 2, true>(a, cfg, atomic);
+    case 6: return launch_cfg<1, 0, false>(a, cfg, atomic);
+    case 7: return launch_cfg<1, 0, true>(a, cfg, atomic);
+    case 8: return launch_cfg<1, 1, false>(a, cfg, atomic);
+    case 9: return launch_cfg<1, 1, true>(a, cfg, atomic);
+    case 10: return launch_cfg<1, 2, false>(a, cfg, atomic);
+    default: return launch_cfg<1, 2, true>(a, cfg, atomic);
   }
 }
 

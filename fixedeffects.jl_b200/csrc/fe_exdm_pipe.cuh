@@ -76,7 +76,19 @@ __device__ __forceinline__ float4 f4_fma(float a, const float4 x, float4 y) {
 // (fast, 4x the shared memory); else one table per warp, added one column
 // per lane after the rows are projected (rows of a group of 4 with equal
 // keys merged first, as in the row-sum pass).
-template <int NL, int NS, bool W, int STG, bool PG>
+// Vector reduction of 4 floats into global memory (one 16-byte red).
+__device__ __forceinline__ void red_add_v4(float* p, float a, float b, float c, float d) {
+  asm volatile("red.relaxed.gpu.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(p), "f"(a), "f"(b),
+               "f"(c), "f"(d)
+               : "memory");
+}
+
+// ATOM (NL == 1 only): the gathered FE's level sums A'u are added here, row
+// by row, with vector reductions into the [P][32] FP32 slab rs.sum (zeroed
+// before the launch) instead of by the level-order segmented sum that
+// follows; the order of the additions is not fixed, so the sums are not
+// bitwise reproducible.
+template <int NL, int NS, bool W, int STG, bool PG, bool ATOM = false>
 __global__ void __launch_bounds__(kThreads, 1)
 k_exdm_pipe(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_items,
             const float* __restrict__ tab, float* __restrict__ rows,
@@ -295,6 +307,8 @@ k_exdm_pipe(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_items
     for (int t = 0; t < NT8; ++t) {
       const int r = t * G + g;
       const float fr = __shfl_sync(FE_FULL, f, r);
+      const int fref = ATOM ? __shfl_sync(FE_FULL, m.rl[0], r) : 0;
+      const float fcl = (ATOM && W) ? __shfl_sync(FE_FULL, m.cl[0], r) : 1.f;
       float cs[NS > 0 ? NS : 1];
       int ks[NS > 0 ? NS : 1];
 #pragma unroll
@@ -311,6 +325,10 @@ k_exdm_pipe(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_items
         u.z -= fr * z.z;
         u.w -= fr * z.w;
         *reinterpret_cast<float4*>(rows + (m.ib + r) * C + jl * 4) = u;
+        if (ATOM) {
+          float* sl = static_cast<float*>(rs.sum) + (lf.large_base[0] + fref) * C + jl * 4;
+          red_add_v4(sl, fcl * u.x, fcl * u.y, fcl * u.z, fcl * u.w);
+        }
         nv.x += u.x * u.x;
         nv.y += u.y * u.y;
         nv.z += u.z * u.z;
@@ -404,6 +422,12 @@ k_exdm_pipe(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_items
         u.z -= fr * z.z;
         u.w -= fr * z.w;
         *up = u;
+        if (ATOM) {
+          const int ref = __ldg(refL[0] + p);
+          const float c = (W && cwL[0]) ? __ldg(cwL[0] + p) : 1.f;
+          red_add_v4(static_cast<float*>(rs.sum) + (lf.large_base[0] + ref) * C + jl * 4, c * u.x,
+                     c * u.y, c * u.z, c * u.w);
+        }
         nv.x += u.x * u.x;
         nv.y += u.y * u.y;
         nv.z += u.z * u.z;
@@ -527,7 +551,8 @@ inline ExdmCfg exdm_cfg(int cfg) {
 }
 
 // Launches k_exdm_pipe<nl, ns, w, stages, per_group> of configuration
-// `cfg`; returns a CUDA status (0 = launched).
-int launch_exdm_pipe(const ExdmLaunch& a, int nl, int ns, bool w, int cfg);
+// `cfg` (atomic: the gathered FE's level sums by vector reductions, cfg 1
+// and nl == 1 only); returns a CUDA status (0 = launched).
+int launch_exdm_pipe(const ExdmLaunch& a, int nl, int ns, bool w, int cfg, bool atomic = false);
 
 }  // namespace fe

@@ -197,7 +197,9 @@ struct fe_plan {
   int32_t opt_absorb = 1;       // mixed residual solves project the primary FE out
   int32_t opt_exdm = 1;         // absorbed loop: fused expand + demean kernel
   int32_t opt_abs_scale = 1;    // absorbed loop: columns scaled by 1 / ||M a_l||
-  int32_t opt_exdm_pipe = -1;   // absorbed loop: pipelined fused kernel (-1 default, 0 off, 1 on)
+  int32_t opt_exdm_pipe = -1;   // absorbed loop: pipelined fused kernel (-1 default, 0 off, 1.. cfg)
+  int32_t opt_firm_atomic = 0;  // absorbed loop: gathered FE's sums by reductions (-1 tuned, 0, 1)
+  float last_firm_tune_ms[2] = {0.f, 0.f};  // the tuner's times: segmented sum, reductions
   std::map<std::pair<int, int>, fe::LoopGraph> graphs;  // by (C, precision)
   // tuned variants per (tile width C, element size): {expand, segsum}
   std::map<std::pair<int, int>, std::pair<int, int>> tuned;

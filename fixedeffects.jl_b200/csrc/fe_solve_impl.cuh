@@ -168,6 +168,9 @@ struct Ctx {
   double* small_part;  // the row-sum pass's CTA partials of the small FEs
   bool rowsum;         // primary and small FEs reduced by the row-sum pass
   bool absorb = false; // primary FE projected out (demean pass; mixed residual solves)
+  // absorbed loop: the gathered FE's level sums by vector reductions inside
+  // the pipelined kernel (no level-order segmented sum)
+  bool firm_atomic = false;
   // observation-sharded plans: per-column norms summed over the ranks, read
   // by the scalar phases as one slot per column
   double* xbuf = nullptr;
@@ -561,9 +564,17 @@ static int exdm_u(Ctx& c, Tab tab, T* rows) {
 // shared-memory limit.  Sets *launched when it ran; otherwise the caller runs
 // k_expand_demean.  FE_OPT_EXDM_PIPE: -1 the default configuration (the
 // first of kExdmPrefer that fits), 1 or 2 one configuration, 0 off.
-static int try_exdm_pipe(Ctx& c, const float* tab, float* rows, int* launched) {
+// The configuration of the pipelined kernel the plan's tile takes: ok = 0
+// when it does not fit (the caller then runs k_expand_demean).
+struct ExdmChoice {
+  bool ok = false;
+  int nl = 0, ns = 0, nsr = 0, cfg = -1;
+  bool w = false;
+  ExdmFEs lf{};
+};
+static int exdm_choose(const Ctx& c, ExdmChoice* ch) {
   static const int kExdmPrefer[] = {1, 2};
-  *launched = 0;
+  *ch = ExdmChoice{};
   const fe_plan* pl = c.pl;
   if (pl->opt_exdm_pipe == 0) return 0;
   static int smem_max = -1;  // opt-in shared memory per block of the device
@@ -572,41 +583,68 @@ static int try_exdm_pipe(Ctx& c, const float* tab, float* rows, int* launched) {
     FE_CK(cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, pl->device));
     smem_max = v;
   }
-  ExdmFEs lf{};
-  int nl = 0, ns = 0;
-  bool w = false;
   for (int k = 0; k < pl->K; ++k) {
     const bool small = ((c.its->small_mask >> k) & 1u) != 0;
-    if (pl->weighted || pl->interacted[k]) w = true;
+    if (pl->weighted || pl->interacted[k]) ch->w = true;
     if (k == pl->primary) continue;
     if (small) {
-      ++ns;
+      ++ch->ns;
       continue;
     }
-    if (nl == 2) return 0;
-    lf.large[nl] = k;
-    lf.large_base[nl] = pl->lev_base[k];
-    ++nl;
+    if (ch->nl == 2) return 0;
+    ch->lf.large[ch->nl] = k;
+    ch->lf.large_base[ch->nl] = pl->lev_base[k];
+    ++ch->nl;
   }
-  if (nl > 1) return 0;
-  const int nsr = ns ? c.its->small_rows : 0;
+  if (ch->nl > 1) return 0;
+  ch->nsr = ch->ns ? c.its->small_rows : 0;
   // + the static norm scratch (kWarps x 32 doubles)
   auto fits = [&](int cfg) {
     const ExdmCfg k = exdm_cfg(cfg);
-    return exdm_pipe_smem(nl, nsr, k.stages, k.per_group) + kWarps * 32 * sizeof(double) <=
-           (size_t)smem_max;
+    return exdm_pipe_smem(ch->nl, ch->nsr, k.stages, k.per_group) +
+               kWarps * 32 * sizeof(double) <= (size_t)smem_max;
   };
-  int cfg = -1;
   if (pl->opt_exdm_pipe > 0) {
-    if (fits(pl->opt_exdm_pipe)) cfg = pl->opt_exdm_pipe;
+    if (fits(pl->opt_exdm_pipe)) ch->cfg = pl->opt_exdm_pipe;
   } else {
     for (int k : kExdmPrefer)
       if (fits(k)) {
-        cfg = k;
+        ch->cfg = k;
         break;
       }
   }
-  if (cfg < 0) return 0;
+  ch->ok = ch->cfg > 0;
+  return 0;
+}
+
+// Whether the tile's gathered FE can take its level sums by vector
+// reductions inside the pipelined kernel: configuration 1, one gathered FE,
+// and no level of it with more than kAtomicMaxLevel positions.  The
+// reductions of one level arrive in no fixed order, each rounded into one
+// FP32 sum; over the ~1e5-1e6 rows of a Zipf head level that error stalled
+// the FP32 inner LSMR (measured: non-convergence at maxiter), and the
+// contention on the level's row made the fused kernel 5x slower.
+constexpr int64_t kAtomicMaxLevel = 1024;
+static bool exdm_atomic_eligible(const fe_plan* pl, const ExdmChoice& ch) {
+  if (!(ch.ok && ch.cfg == 1 && ch.nl == 1)) return false;
+  const int k = ch.lf.large[0];
+  const std::vector<int64_t>& off = pl->seg_off[k];
+  int64_t mx = 0;
+  for (size_t l = 0; l + 1 < off.size(); ++l) mx = std::max(mx, off[l + 1] - off[l]);
+  return mx <= kAtomicMaxLevel;
+}
+
+// The pipelined fused kernel; *launched = 1 when it ran (with the gathered
+// FE's level sums by reductions when c.firm_atomic), else the caller runs
+// k_expand_demean.
+static int try_exdm_pipe(Ctx& c, const float* tab, float* rows, int* launched) {
+  *launched = 0;
+  ExdmChoice ch;
+  int st0 = exdm_choose(c, &ch);
+  if (st0 || !ch.ok) return st0;
+  const int nl = ch.nl, ns = ch.ns, nsr = ch.nsr, cfg = ch.cfg;
+  const bool w = ch.w;
+  const ExdmFEs lf = ch.lf;
   const ExdmCfg kc = exdm_cfg(cfg);
   ExdmLaunch a{};
   a.d = c.d;
@@ -633,7 +671,7 @@ static int try_exdm_pipe(Ctx& c, const float* tab, float* rows, int* launched) {
   a.grid = std::max<int64_t>(1, std::min<int64_t>(c.its->Se, c.its->sms));
   a.smem = exdm_pipe_smem(nl, nsr, kc.stages, kc.per_group);
   a.stream = c.s;
-  int st = launch_exdm_pipe(a, nl, ns, w, cfg);
+  int st = launch_exdm_pipe(a, nl, ns, w, cfg, c.firm_atomic && exdm_atomic_eligible(c.pl, ch));
   if (st) return st;
   if (c.its->small_rows > 0) {
     k_small_combine<float, 32><<<(unsigned)c.its->small_rows, kThreads, 0, c.s>>>(
@@ -1060,6 +1098,7 @@ static int run_loop(fe_plan* pl, Ctx& c, int prec, int64_t cap, int32_t nact0, B
     key = key * 3 + (size_t)pl->opt_exdm;
     key = key * 3 + (size_t)pl->opt_abs_scale;
     key = key * 3 + (size_t)(pl->opt_exdm_pipe + 1);
+    key = key * 3 + (c.firm_atomic ? 1u : 0u);
     lg = &pl->graphs[{c.C, prec}];
     if (!lg->exec || lg->key != key) {
       if (lg->exec) {
@@ -1224,6 +1263,96 @@ static int autotune(fe_plan* pl, Ctx& c, T* rows, T* levels, bool resid_form = f
 }
 
 // ---------------------------------------------------------------------------
+// absorbed loop: the gathered FE's level sums by vector reductions inside the
+// pipelined kernel, or by the deterministic level-order segmented sum.  With
+// FE_OPT_FIRM_ATOMIC = -1 both are timed once per plan shape on the plan's
+// own index data (best of two after a warm-up) and the faster is kept, in
+// the plan and in the tuning cache (kind 300).
+// ---------------------------------------------------------------------------
+template <int C>
+static int tune_firm_atomic(fe_plan* pl, Ctx& c, bool* out) {
+  *out = false;
+  if constexpr (C != 32) {
+    (void)pl;
+    (void)c;
+    return 0;
+  } else {
+  ExdmChoice ch;
+  int st = exdm_choose(c, &ch);
+  if (st) return st;
+  if (!c.absorb || !pl->opt_exdm || !exdm_atomic_eligible(pl, ch) || pl->opt_firm_atomic == 0)
+    return 0;
+  if (pl->opt_firm_atomic == 1) {
+    *out = true;
+    return 0;
+  }
+  const std::pair<int, int> key(c.C, 300);
+  auto f = pl->tuned.find(key);
+  if (f != pl->tuned.end()) {
+    *out = f->second.first == 1;
+    return 0;
+  }
+  int a = 0, b = 0;
+  if (tune_cache_load(pl, c.C, 300, &a, &b)) {
+    pl->tuned[key] = {a, 0};
+    *out = a == 1;
+    return 0;
+  }
+  if (!pl->opt_autotune) return 0;
+  NvtxRange nv("fe: autotune (gathered-FE reduction)");
+  Workspace& w = pl->ws;
+  std::vector<Inst> h((size_t)pl->nprob * c.C);
+  for (Inst& s0 : h) {
+    memset(&s0, 0, sizeof(s0));
+    s0.active = 1;
+    s0.ex_av = 1.0;
+    s0.ex_au = 0.5;
+  }
+  FE_CK(cudaMemcpyAsync(c.inst, h.data(), h.size() * sizeof(Inst), cudaMemcpyHostToDevice, c.s));
+  const int k = ch.lf.large[0];
+  float* S32 = static_cast<float*>(c.S);
+  const size_t frow = (size_t)pl->lev_base[k] * c.C, fbytes = (size_t)(pl->nlev[k] + 1) * c.C * 4;
+  cudaEvent_t e0, e1;
+  FE_CK(cudaEventCreate(&e0));
+  FE_CK(cudaEventCreate(&e1));
+  const bool prof = pl->prof.on;
+  pl->prof.on = false;
+  float best[2] = {1e30f, 1e30f};
+  for (int v = 0; v < 2 && !st; ++v) {
+    c.firm_atomic = v == 1;
+    for (int rep = 0; rep < 3 && !st; ++rep) {
+      cudaEventRecord(e0, c.s);
+      if (v == 1 && cudaMemsetAsync(S32 + frow, 0, fbytes, c.s) != cudaSuccess) st = 2;
+      if (!st)
+        st = launch_expand_demean<float, 32>(c, TabOne<float, float, vec_of<float, 32>()>{w.VS.as<float>()},
+                                             w.U.as<float>(), "tune", 0.0);
+      if (!st && v == 0)
+        st = launch_segsum<float, 32>(c, LoadIn<float, float, vec_of<float, 32>()>{w.U.as<float>()}, S32,
+                                      "tune", 0.0, true, "", 0.0, true);
+      cudaEventRecord(e1, c.s);
+      cudaEventSynchronize(e1);
+      float t = 0.f;
+      cudaEventElapsedTime(&t, e0, e1);
+      if (rep > 0) best[v] = std::min(best[v], t);
+    }
+  }
+  c.firm_atomic = false;
+  pl->prof.on = prof;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (st) return st;
+  FE_CK(cudaMemsetAsync(c.S, 0, (size_t)pl->P * c.C * 8, c.s));
+  const int choice = best[1] < best[0] ? 1 : 0;
+  pl->tuned[key] = {choice, 0};
+  tune_cache_store(pl, c.C, 300, choice, 0);
+  pl->last_firm_tune_ms[0] = best[0];
+  pl->last_firm_tune_ms[1] = best[1];
+  *out = choice == 1;
+  return 0;
+  }
+}
+
+// ---------------------------------------------------------------------------
 // coefficient download (solve_coefficients!)
 // ---------------------------------------------------------------------------
 template <typename TX>
@@ -1354,18 +1483,6 @@ static int solve_mixed_tile(fe_plan* pl, const SolveReq& rq, int64_t col0, int n
     return st;
   Workspace& w = pl->ws;
   const Bytes by = alg_bytes(pl, c.its, C, 4);
-  std::vector<Inst> h;
-  init_insts(pl, rq, C, ncols, h);
-  FE_CK(cudaMemcpyAsync(c.inst, h.data(), h.size() * sizeof(Inst), cudaMemcpyHostToDevice, c.s));
-  if ((st = load_tile(pl, c, rq, col0, ncols))) return st;
-  float* U = w.U.as<float>();
-  float* V = w.V.as<float>();
-  float* X = w.X.as<float>();
-  double* X64 = w.X64.as<double>();
-  double* B64 = w.B64.as<double>();
-  double* R64 = w.R64.as<double>();
-  double* S64 = static_cast<double*>(c.S);
-  float* S32 = static_cast<float*>(c.S);
   // absorbed-primary mode (residual solves): LSMR over the other FEs, from
   // x0 = 0 (the reference's warm start A'b belongs to the full problem)
   const bool absorb = rq.residuals && use_absorb(pl, c.its, C);
@@ -1380,6 +1497,20 @@ static int solve_mixed_tile(fe_plan* pl, const SolveReq& rq, int64_t col0, int n
         c.d.scale_d[k] = pl->d_abs_scale_d[k].as<double>();
         c.d.scale_f[k] = pl->d_abs_scale_f[k].as<float>();
       }
+  // the gathered FE's reduction (timed on scratch before the tile is loaded)
+  if (absorb && (st = tune_firm_atomic<C>(pl, c, &c.firm_atomic))) return st;
+  std::vector<Inst> h;
+  init_insts(pl, rq, C, ncols, h);
+  FE_CK(cudaMemcpyAsync(c.inst, h.data(), h.size() * sizeof(Inst), cudaMemcpyHostToDevice, c.s));
+  if ((st = load_tile(pl, c, rq, col0, ncols))) return st;
+  float* U = w.U.as<float>();
+  float* V = w.V.as<float>();
+  float* X = w.X.as<float>();
+  double* X64 = w.X64.as<double>();
+  double* B64 = w.B64.as<double>();
+  double* R64 = w.R64.as<double>();
+  double* S64 = static_cast<double*>(c.S);
+  float* S32 = static_cast<float*>(c.S);
   if (rq.residuals && pl->opt_mixed_warm && !absorb) {
     if ((st = zero_slab(c, S64, 8))) return st;
     if ((st = launch_segsum<double, C>(c, LoadIn<double, double, vec_of<double, C>()>{B64}, S64, "segsum_warm", 0.0,
@@ -1453,6 +1584,13 @@ static int solve_mixed_tile(fe_plan* pl, const SolveReq& rq, int64_t col0, int n
         // u = M (av A_r v + au u): the expand without the primary FE, then the
         // projection (which also gives ||u|| and the small FEs' sums)
         if ((e = zero_slab(c, S32, 4))) return e;
+        if (c.firm_atomic) {
+          // the gathered FE's level sums are added by the fused kernel
+          for (int k = 0; k < pl->K; ++k)
+            if (k != pl->primary && !((c.its->small_mask >> k) & 1u))
+              FE_CK(cudaMemsetAsync(S32 + (size_t)pl->lev_base[k] * C, 0,
+                                    (size_t)(pl->nlev[k] + 1) * C * 4, c.s));
+        }
         if (pl->opt_exdm) {
           if ((e = launch_expand_demean<float, C>(c, TabOne<float, float, vec_of<float, C>()>{VS}, U,
                                                   "expand_demean", by.expand_demean)))
@@ -1465,7 +1603,8 @@ static int solve_mixed_tile(fe_plan* pl, const SolveReq& rq, int64_t col0, int n
         }
         if ((e = xchg_slots(c, c.part_e))) return e;
         if ((e = launch_scalar_phase(c, PH_BETA, 0))) return e;
-        if ((e = launch_segsum<float, C>(c, LoadIn<float, float, vec_of<float, C>()>{U}, S32, "segsum",
+        if (!c.firm_atomic &&
+            (e = launch_segsum<float, C>(c, LoadIn<float, float, vec_of<float, C>()>{U}, S32, "segsum",
                                          by.segsum, true, "", 0.0, true)))
           return e;
         if ((e = xchg_slab(c, S32, 4))) return e;
