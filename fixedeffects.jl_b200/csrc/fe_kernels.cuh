@@ -178,8 +178,11 @@ __device__ __forceinline__ void cta_norm_to_slot(const double (&nrm)[VEC], doubl
 // ---------------------------------------------------------------------------
 // Coefficient tables gathered by the expand.
 // ---------------------------------------------------------------------------
+// kPrescaled: the table rows already hold scale_l * x_l, so the gather
+// multiplies by the observation's weight only.
 template <typename T, typename TA, int VEC>
 struct TabOne {
+  static constexpr bool kPrescaled = false;
   const T* __restrict__ tab;
   __device__ __forceinline__ VA<TA, VEC> load(int64_t off) const {
     const VA<T, VEC> a = vldg<T, VEC>(tab + off);
@@ -189,20 +192,33 @@ struct TabOne {
     return r;
   }
 };
-// x64 + x32: the FP64 accumulated solution plus the FP32 correction of the
-// inner solve that just finished (the mixed-precision residual).
+// (x64 + dx32) .* scale, written once per refinement round by k_prescale64
+// (the FP64 residual's table: one FP64 row per gathered level, no scale load).
 template <int VEC>
-struct TabSum64 {
-  const double* __restrict__ hi;
-  const float* __restrict__ lo;
+struct TabPre64 {
+  static constexpr bool kPrescaled = true;
+  const double* __restrict__ tab;
   __device__ __forceinline__ VA<double, VEC> load(int64_t off) const {
-    VA<double, VEC> a = vldg<double, VEC>(hi + off);
-    const VA<float, VEC> b = vldg<float, VEC>(lo + off);
-#pragma unroll
-    for (int v = 0; v < VEC; ++v) a.v[v] += (double)b.v[v];
-    return a;
+    return vldg<double, VEC>(tab + off);
   }
 };
+
+// out[l][j] = (x64[l][j] + x32[l][j]) * scale[l] for the n levels of one FE
+// (pointers already offset to the FE's first level); two columns per thread.
+static __global__ void __launch_bounds__(256) k_prescale64(const double* __restrict__ x64,
+                                                           const float* __restrict__ x32,
+                                                           const double* __restrict__ scale,
+                                                           double* __restrict__ out, int64_t n, int C) {
+  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;  // pair index
+  const int half = (C + 1) / 2;
+  if (e >= n * half) return;
+  const int64_t l = e / half;
+  const int j = (int)(e - l * half) * 2;
+  const double sc = scale[l];
+  const int64_t o = l * C + j;
+  out[o] = (x64[o] + (double)x32[o]) * sc;
+  if (j + 1 < C) out[o + 1] = (x64[o + 1] + (double)x32[o + 1]) * sc;
+}
 
 // ---------------------------------------------------------------------------
 // Expand epilogues.  begin() loads the per-column coefficients of the lane's
@@ -542,8 +558,13 @@ k_expand(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_items, T
               const TA c = wk ? __shfl_sync(FE_FULL, cc[k][q >> 5], (q & 31) + g) : TA(1);
               const int64_t i = base + u * G + g;
               if (i < it.ie && epi.act) {
-                const TA scl = __ldg(sc + ref);
-                const TA cs = wk ? c * scl : scl;
+                TA cs;
+                if constexpr (Tab::kPrescaled) {
+                  cs = wk ? c : TA(1);
+                } else {
+                  const TA scl = __ldg(sc + ref);
+                  cs = wk ? c * scl : scl;
+                }
                 const VA<TA, VEC> t = tab.load((lb + ref) * C + jl * VEC);
 #pragma unroll
                 for (int v = 0; v < VEC; ++v) s[u].v[v] += cs * t.v[v];

@@ -121,6 +121,7 @@ struct Workspace {
   int C = 0;
   DevBuf B64, R64, U, V, H, Hb, X, X64, S;
   DevBuf VS;  // scale * v, the fused absorbed loop's coefficient table (FP32)
+  DevBuf XS64;  // (x64 + dx32) * scale, the FP64 residual's coefficient table
   DevBuf part_e, part_a, part_b, piece_part, ex_piece_part, block_part, ex_block_part, inst,
       counters;
   DevBuf small_part;  // the row-sum CTA partials of the small FEs

@@ -39,56 +39,88 @@ namespace fe {
 // (src/AbstractFixedEffectSolver.jl:50-55).  A CTA stages kLoadRows
 // observations x C columns in shared memory: the reads are coalesced along
 // observations (column-major input), the writes are whole contiguous rows.
+// Every thread issues all its loads (kLoadPer, independent) before the first
+// shared-memory store, so 16 KB per CTA are in flight at C = 32.  C is a
+// compile-time power of two (index splits are shifts) and W says whether there
+// are weights (without, no multiply or divide by sqrt(w) = 1).
 constexpr int kLoadRows = 64;
-template <typename TY>
+template <int C> constexpr int load_per() { return kLoadRows * C >= 256 ? kLoadRows * C / 256 : 1; }
+template <typename TY, int C, bool W>
 __global__ void __launch_bounds__(256) k_load(const TY* __restrict__ Y, int64_t ld, int64_t col0,
-                                              int ncols, int C, const int32_t* __restrict__ dst,
+                                              int ncols, const int32_t* __restrict__ dst,
                                               const double* __restrict__ sw,
                                               double* __restrict__ B, int64_t N) {
-  __shared__ double tile[kLoadRows][33];
-  __shared__ int64_t rows[kLoadRows];
+  constexpr int PER = load_per<C>();
+  constexpr int JS = 256 / kLoadRows;  // column stride between a thread's loads
+  __shared__ double tile[kLoadRows][C + 1];
+  __shared__ int32_t rows[kLoadRows];
   const int64_t i0 = (int64_t)blockIdx.x * kLoadRows;
-  for (int e = threadIdx.x; e < kLoadRows * C; e += blockDim.x) {
-    const int j = e / kLoadRows, r = e - j * kLoadRows;
-    const int64_t i = i0 + r;
-    double v = 0.0;
-    if (i < N && j < ncols) v = (double)Y[i + (col0 + j) * ld] * (sw ? sw[i] : 1.0);
-    tile[r][j] = v;
+  // load phase: thread t reads row t % kLoadRows of columns t / kLoadRows + JS u
+  const int r = threadIdx.x % kLoadRows, j0 = threadIdx.x / kLoadRows;
+  const int64_t i = i0 + r;
+  const bool in = i < N;
+  double v[PER];
+#pragma unroll
+  for (int u = 0; u < PER; ++u) {
+    const int j = j0 + u * JS;
+    v[u] = (in && j < ncols) ? (double)Y[i + (col0 + j) * ld] : 0.0;
   }
-  for (int r = threadIdx.x; r < kLoadRows; r += blockDim.x)
-    rows[r] = (i0 + r < N) ? (int64_t)dst[i0 + r] : -1;
+  if (threadIdx.x < kLoadRows)
+    rows[threadIdx.x] = (i0 + threadIdx.x < N) ? dst[i0 + threadIdx.x] : -1;
+  const double s = (W && in) ? sw[i] : 1.0;
+#pragma unroll
+  for (int u = 0; u < PER; ++u) {
+    const int j = j0 + u * JS;
+    if (j < C) tile[r][j] = W ? v[u] * s : v[u];
+  }
   __syncthreads();
-  for (int e = threadIdx.x; e < kLoadRows * C; e += blockDim.x) {
-    const int r = e / C, j = e - r * C;
-    const int64_t q = rows[r];
-    if (q >= 0) B[q * C + j] = tile[r][j];
+#pragma unroll
+  for (int u = 0; u < PER; ++u) {
+    const int e = threadIdx.x + u * 256;
+    const int rr = e / C, j = e % C;
+    if (e < kLoadRows * C) {
+      const int32_t q = rows[rr];
+      if (q >= 0) B[(int64_t)q * C + j] = tile[rr][j];
+    }
   }
 }
 
 // y[i][col0 + j] = R[q][j] / sqrt(w_i)  (src/AbstractFixedEffectSolver.jl:62-66):
-// whole rows in, coalesced columns out.
-template <typename TY>
+// whole rows in (all of a thread's row loads issued before the first
+// shared-memory store), coalesced columns out.
+template <typename TY, int C, bool W>
 __global__ void __launch_bounds__(256) k_unload(const double* __restrict__ R, int64_t ld,
-                                                int64_t col0, int ncols, int C,
+                                                int64_t col0, int ncols,
                                                 const int32_t* __restrict__ dst,
                                                 const double* __restrict__ sw,
                                                 TY* __restrict__ Y, int64_t N) {
-  __shared__ double tile[kLoadRows][33];
-  __shared__ int64_t rows[kLoadRows];
+  constexpr int PER = load_per<C>();
+  constexpr int JS = 256 / kLoadRows;
+  __shared__ double tile[kLoadRows][C + 1];
   const int64_t i0 = (int64_t)blockIdx.x * kLoadRows;
-  for (int r = threadIdx.x; r < kLoadRows; r += blockDim.x)
-    rows[r] = (i0 + r < N) ? (int64_t)dst[i0 + r] : -1;
-  __syncthreads();
-  for (int e = threadIdx.x; e < kLoadRows * C; e += blockDim.x) {
-    const int r = e / C, j = e - r * C;
-    const int64_t q = rows[r];
-    tile[r][j] = q >= 0 ? R[q * C + j] : 0.0;
+  double v[PER];
+#pragma unroll
+  for (int u = 0; u < PER; ++u) {
+    const int e = threadIdx.x + u * 256;
+    const int rr = e / C, j = e % C;
+    const int64_t i = i0 + rr;
+    v[u] = (e < kLoadRows * C && i < N) ? R[(int64_t)dst[i] * C + j] : 0.0;
+  }
+#pragma unroll
+  for (int u = 0; u < PER; ++u) {
+    const int e = threadIdx.x + u * 256;
+    const int rr = e / C, j = e % C;
+    if (e < kLoadRows * C) tile[rr][j] = v[u];
   }
   __syncthreads();
-  for (int e = threadIdx.x; e < kLoadRows * ncols; e += blockDim.x) {
-    const int j = e / kLoadRows, r = e - j * kLoadRows;
-    const int64_t i = i0 + r;
-    if (i < N) Y[i + (col0 + j) * ld] = (TY)(tile[r][j] / (sw ? sw[i] : 1.0));
+  const int r = threadIdx.x % kLoadRows, j0 = threadIdx.x / kLoadRows;
+  const int64_t i = i0 + r;
+  if (i >= N) return;
+  const double s = W ? sw[i] : 1.0;
+#pragma unroll
+  for (int u = 0; u < PER; ++u) {
+    const int j = j0 + u * JS;
+    if (j < ncols) Y[i + (col0 + j) * ld] = (TY)(W ? tile[r][j] / s : tile[r][j]);
   }
 }
 
@@ -296,6 +328,24 @@ static int expand_kb(Ctx& c, Tab tab, Epi epi, double* part) {
     case 5: return expand_kbu<KB, 4, 2, TA, C>(c, tab, epi, part);
     default: return expand_kbu<KB, 2, 1, TA, C>(c, tab, epi, part);
   }
+}
+
+// The FP64 residual's coefficient table: (x64 + dx32) .* scale for every FE
+// the expand gathers (all but the primary when it is absorbed), once per
+// refinement round.
+static int launch_prescale64(Ctx& c, const double* x64, const float* x32, double* out,
+                             bool absorb, double bytes) {
+  ProfScope ps(c.pl, "prescale64", bytes);
+  const fe_plan* pl = c.pl;
+  for (int k = 0; k < pl->K; ++k) {
+    if (absorb && k == pl->primary) continue;
+    const int64_t n = pl->nlev[k] + 1;
+    const int64_t o = pl->lev_base[k] * c.C;
+    const int64_t pairs = n * ((c.C + 1) / 2);
+    k_prescale64<<<grid1(pairs), 256, 0, c.s>>>(x64 + o, x32 + o, c.d.scale_d[k], out + o, n, c.C);
+    FE_CK(cudaGetLastError());
+  }
+  return 0;
 }
 
 template <typename TA, int C, class Tab, class Epi>
@@ -849,6 +899,7 @@ struct Bytes {
   double expand, segsum, pupdate, resid64, segsum64, grad64, rowsum, rowsum64;
   // absorbed-primary mode
   double expand_abs, resid64_abs, demean, demean64, pupdate_np, grad64_np, expand_demean;
+  double prescale64, prescale64_abs;
 };
 static Bytes alg_bytes(const fe_plan* pl, const ItemSet* its, int C, int sT) {
   Bytes b{};
@@ -910,7 +961,8 @@ static Bytes alg_bytes(const fe_plan* pl, const ItemSet* its, int C, int sT) {
       }
     const double cwnp = cw - (cwp ? N * sT : 0.0), cwnp64 = cw64 - (cwp ? N * 8.0 : 0.0);
     b.expand_abs = N * 4.0 * (pl->K - 1) + cwnp + 2.0 * N * C * sT + Pnp * C * sT;
-    b.resid64_abs = N * 4.0 * (pl->K - 1) + cwnp64 + N * C * 16.0 + Pnp * C * 12.0;
+    b.resid64_abs = N * 4.0 * (pl->K - 1) + cwnp64 + N * C * 16.0 + Pnp * C * 8.0;
+    b.prescale64_abs = Pnp * (C * 20.0 + 8.0);
     b.demean = keys + 2.0 * N * C * sT + Pp * sT;
     b.demean64 = keys64 + 2.0 * N * C * 8.0 + N * C * 4.0 + Pp * 8.0;
     b.pupdate_np = 9.0 * Pnp * C * sT;
@@ -921,7 +973,8 @@ static Bytes alg_bytes(const fe_plan* pl, const ItemSet* its, int C, int sT) {
     b.grad64_np = Pnp * C * (8.0 + 4.0 + 8.0 + 4.0 + 8.0);
   }
   b.pupdate = 9.0 * P * C * sT;
-  b.resid64 = refs + cw64 + N * C * (8.0 + 8.0 + 4.0) + P * C * 12.0;
+  b.resid64 = refs + cw64 + N * C * (8.0 + 8.0 + 4.0) + P * C * 8.0;
+  b.prescale64 = P * (C * 20.0 + 8.0);
   b.segsum64 = posmeta + cwp64 + pos * C * 8.0 + (P - Pf) * C * 8.0;
   b.grad64 = P * C * (8.0 + 4.0 + 8.0 + 4.0 + 8.0);
   return b;
@@ -943,6 +996,7 @@ static int prepare(fe_plan* pl, int C, int sT, bool mixed, Ctx& c) {
   if ((st = w.Hb.ensure(P * nC * (size_t)sT))) return st;
   if ((st = w.X.ensure(P * nC * (size_t)sT))) return st;
   if (mixed && (st = w.X64.ensure(P * nC * 8))) return st;
+  if (mixed && (st = w.XS64.ensure(P * nC * 8))) return st;
   if ((st = w.part_e.ensure((size_t)std::max<int64_t>(its->Se, 1) * nC * 8))) return st;
   if ((st = w.part_a.ensure((size_t)std::max<int64_t>(its->Sp, 1) * nC * 8))) return st;
   if ((st = w.part_b.ensure((size_t)std::max<int64_t>(its->Sp, 1) * nC * 8))) return st;
@@ -1001,36 +1055,45 @@ static int prepare(fe_plan* pl, int C, int sT, bool mixed, Ctx& c) {
   return 0;
 }
 
+template <int C, typename TY, bool W>
+static void launch_load(const fe_plan* pl, Ctx& c, const SolveReq& rq, int64_t col0, int ncols) {
+  k_load<TY, C, W><<<grid1(pl->N, kLoadRows), 256, 0, c.s>>>(
+      (const TY*)rq.Y, rq.ld, col0, ncols, pl->d_obs_dst.as<int32_t>(),
+      W ? pl->d_sw_orig.as<double>() : nullptr, pl->ws.B64.as<double>(), pl->N);
+}
+template <int C, typename TY, bool W>
+static void launch_unload(const fe_plan* pl, Ctx& c, const SolveReq& rq, int64_t col0, int ncols) {
+  k_unload<TY, C, W><<<grid1(pl->N, kLoadRows), 256, 0, c.s>>>(
+      pl->ws.R64.as<double>(), rq.ld, col0, ncols, pl->d_obs_dst.as<int32_t>(),
+      W ? pl->d_sw_orig.as<double>() : nullptr, (TY*)rq.Y, pl->N);
+}
+
+template <int C>
 static int load_tile(fe_plan* pl, Ctx& c, const SolveReq& rq, int64_t col0, int ncols) {
   NvtxRange nv("fe: load tile");
-  const int64_t N = pl->N;
-  if (N == 0) return 0;
-  const double* sw = pl->weighted ? pl->d_sw_orig.as<double>() : nullptr;
-  ProfScope ps(pl, "load", (double)N * ncols * (rq.dtype == 0 ? 8 : 4) + (double)N * c.C * 8);
+  if (pl->N == 0) return 0;
+  ProfScope ps(pl, "load", (double)pl->N * ncols * (rq.dtype == 0 ? 8 : 4) + (double)pl->N * C * 8);
   if (rq.dtype == 0)
-    k_load<double><<<grid1(N, kLoadRows), 256, 0, c.s>>>((const double*)rq.Y, rq.ld, col0, ncols, c.C,
-                                                pl->d_obs_dst.as<int32_t>(), sw,
-                                                pl->ws.B64.as<double>(), N);
+    pl->weighted ? launch_load<C, double, true>(pl, c, rq, col0, ncols)
+                 : launch_load<C, double, false>(pl, c, rq, col0, ncols);
   else
-    k_load<float><<<grid1(N, kLoadRows), 256, 0, c.s>>>((const float*)rq.Y, rq.ld, col0, ncols, c.C,
-                                               pl->d_obs_dst.as<int32_t>(), sw,
-                                               pl->ws.B64.as<double>(), N);
+    pl->weighted ? launch_load<C, float, true>(pl, c, rq, col0, ncols)
+                 : launch_load<C, float, false>(pl, c, rq, col0, ncols);
   FE_CK(cudaGetLastError());
   return 0;
 }
 
+template <int C>
 static int unload_tile(fe_plan* pl, Ctx& c, const SolveReq& rq, int64_t col0, int ncols) {
   NvtxRange nv("fe: unload tile");
-  const int64_t N = pl->N;
-  if (N == 0) return 0;
-  const double* sw = pl->weighted ? pl->d_sw_orig.as<double>() : nullptr;
-  ProfScope ps(pl, "unload", (double)N * ncols * (rq.dtype == 0 ? 8 : 4) + (double)N * c.C * 8);
+  if (pl->N == 0) return 0;
+  ProfScope ps(pl, "unload", (double)pl->N * ncols * (rq.dtype == 0 ? 8 : 4) + (double)pl->N * C * 8);
   if (rq.dtype == 0)
-    k_unload<double><<<grid1(N, kLoadRows), 256, 0, c.s>>>(pl->ws.R64.as<double>(), rq.ld, col0, ncols, c.C,
-                                                  pl->d_obs_dst.as<int32_t>(), sw, (double*)rq.Y, N);
+    pl->weighted ? launch_unload<C, double, true>(pl, c, rq, col0, ncols)
+                 : launch_unload<C, double, false>(pl, c, rq, col0, ncols);
   else
-    k_unload<float><<<grid1(N, kLoadRows), 256, 0, c.s>>>(pl->ws.R64.as<double>(), rq.ld, col0, ncols, c.C,
-                                                 pl->d_obs_dst.as<int32_t>(), sw, (float*)rq.Y, N);
+    pl->weighted ? launch_unload<C, float, true>(pl, c, rq, col0, ncols)
+                 : launch_unload<C, float, false>(pl, c, rq, col0, ncols);
   FE_CK(cudaGetLastError());
   return 0;
 }
@@ -1204,10 +1267,10 @@ static int autotune(fe_plan* pl, Ctx& c, T* rows, T* levels, bool resid_form = f
     for (int rep = 0; rep < 3 && !st; ++rep) {
       cudaEventRecord(e0, c.s);
       if constexpr (std::is_same<T, double>::value) {
-        if (resid_form) {  // the refinement's r = b - A (x64 + x32), all columns
+        if (resid_form) {  // the refinement's r = b - A x (pre-scaled table), all columns
           Workspace& w = pl->ws;
           st = launch_expand<double, C>(
-              c, TabSum64<vec_of<double, C>()>{levels, w.X.as<float>()},
+              c, TabPre64<vec_of<double, C>()>{levels},
               EpiBminusAx<double, double, vec_of<double, C>()>{w.B64.as<double>(), rows,
                                                                 w.U.as<float>(), c.inst, 0},
               c.part_e, "tune", 0.0);
@@ -1388,7 +1451,7 @@ static int solve_plain_tile(fe_plan* pl, const SolveReq& rq, int64_t col0, int n
   std::vector<Inst> h;
   init_insts(pl, rq, C, ncols, h);
   FE_CK(cudaMemcpyAsync(c.inst, h.data(), h.size() * sizeof(Inst), cudaMemcpyHostToDevice, c.s));
-  if ((st = load_tile(pl, c, rq, col0, ncols))) return st;
+  if ((st = load_tile<C>(pl, c, rq, col0, ncols))) return st;
   T* U = w.U.as<T>();
   T* V = w.V.as<T>();
   T* X = w.X.as<T>();
@@ -1456,7 +1519,7 @@ static int solve_plain_tile(fe_plan* pl, const SolveReq& rq, int64_t col0, int n
                                   EpiBminusAx<double, T, vec_of<T, C>()>{B64, w.R64.as<double>(), nullptr, c.inst, 0},
                                   nullptr, "expand_final", by.expand)))
       return st;
-    if ((st = unload_tile(pl, c, rq, col0, ncols))) return st;
+    if ((st = unload_tile<C>(pl, c, rq, col0, ncols))) return st;
   }
   out.resize(h.size());
   FE_CK(cudaMemcpyAsync(out.data(), c.inst, h.size() * sizeof(Inst), cudaMemcpyDeviceToHost, c.s));
@@ -1502,7 +1565,7 @@ static int solve_mixed_tile(fe_plan* pl, const SolveReq& rq, int64_t col0, int n
   std::vector<Inst> h;
   init_insts(pl, rq, C, ncols, h);
   FE_CK(cudaMemcpyAsync(c.inst, h.data(), h.size() * sizeof(Inst), cudaMemcpyHostToDevice, c.s));
-  if ((st = load_tile(pl, c, rq, col0, ncols))) return st;
+  if ((st = load_tile<C>(pl, c, rq, col0, ncols))) return st;
   float* U = w.U.as<float>();
   float* V = w.V.as<float>();
   float* X = w.X.as<float>();
@@ -1551,9 +1614,12 @@ static int solve_mixed_tile(fe_plan* pl, const SolveReq& rq, int64_t col0, int n
     // absorbed: round 0 starts from x = 0, so r0 = M b comes straight from b
     const bool from_b = absorb && round == 0;
     if ((st = zero_slab(c, S64, 8))) return st;
+    if (!from_b && (st = launch_prescale64(c, X64, X, w.XS64.as<double>(), absorb,
+                                           absorb ? by.prescale64_abs : by.prescale64)))
+      return st;
     if (!from_b &&
         (st = launch_expand<double, C>(
-             c, TabSum64<vec_of<double, C>()>{X64, X},
+             c, TabPre64<vec_of<double, C>()>{w.XS64.as<double>()},
              EpiBminusAx<double, double, vec_of<double, C>()>{B64, R64, absorb ? nullptr : U, c.inst, 2},
              absorb ? nullptr : c.part_e, "resid64", absorb ? by.resid64_abs : by.resid64)))
       return st;
@@ -1634,7 +1700,7 @@ static int solve_mixed_tile(fe_plan* pl, const SolveReq& rq, int64_t col0, int n
     total_it += done;
   }
   if (rq.residuals) {
-    if ((st = unload_tile(pl, c, rq, col0, ncols))) return st;
+    if ((st = unload_tile<C>(pl, c, rq, col0, ncols))) return st;
   }
   out.resize(h.size());
   FE_CK(cudaMemcpyAsync(out.data(), c.inst, h.size() * sizeof(Inst), cudaMemcpyDeviceToHost, c.s));
