@@ -48,6 +48,7 @@ FE_OPT_FUSED_DEMEAN = 15
 FE_OPT_ABSORB_SCALE = 16
 FE_OPT_EXDM_PIPE = 17
 FE_OPT_FIRM_ATOMIC = 18
+FE_OPT_FUSED_RESID = 19
 
 # every symbol declared in include/fe_b200.h
 EXPORTS = (

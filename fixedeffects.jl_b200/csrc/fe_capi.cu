@@ -384,6 +384,9 @@ int fe_plan_set_option(fe_plan* plan, int32_t option, double value) {
     case FE_OPT_FUSED_DEMEAN:
       plan->opt_exdm = value != 0 ? 1 : 0;
       return FE_OK;
+    case FE_OPT_FUSED_RESID:
+      plan->opt_fused_resid = value != 0 ? 1 : 0;
+      return FE_OK;
     case FE_OPT_ABSORB_SCALE:
       plan->opt_abs_scale = value != 0 ? 1 : 0;
       return FE_OK;

@@ -523,10 +523,13 @@ static int launch_demean(Ctx& c, T* rows, float* rows32, T* out, const char* nam
 // The fused expand + demean of the absorbed-primary loop (k_expand_demean):
 // u = M (av A_r v + au u), in place on rows, ||u||^2 to the expand norm slots,
 // small-FE sums to the slab (through the CTA partials).
-template <typename T, int C, int U, int KB, bool W, int NS, class Tab>
-static int exdm_launch(Ctx& c, Tab tab, T* rows) {
+// RESID (FP64): rows = M (B - A_r x) with tab holding scale * x, an FP32 copy
+// into rows32; columns whose refinement has stopped (mask 2) keep their rows.
+template <typename T, int C, int U, int KB, bool W, int NS, class Tab, bool RESID = false>
+static int exdm_launch(Ctx& c, Tab tab, T* rows, const double* B = nullptr,
+                       float* rows32 = nullptr, int mask = 0) {
   if constexpr (C == 32) {
-    auto kern = k_expand_demean<T, C, U, KB, false, W, NS, Tab, true>;
+    auto kern = k_expand_demean<T, C, U, KB, RESID, W, NS, Tab, true>;
     const size_t smem =
         (size_t)kWarps * ((2 * kDemeanRows + c.its->small_rows) * C * sizeof(T) + 32 * sizeof(int));
     static bool attr_set = false;  // per instantiation
@@ -558,7 +561,7 @@ static int exdm_launch(Ctx& c, Tab tab, T* rows) {
         ++rs.n_small;
       }
     kern<<<(unsigned)grid, kThreads, smem, c.s>>>(c.d, c.its->d_dm.as<ExpandItem>(), n, tab, rows,
-                                                  nullptr, nullptr, c.inst, 0, rs, c.part_e,
+                                                  B, rows32, c.inst, mask, rs, c.part_e,
                                                   c.its->Se);
     FE_CK(cudaGetLastError());
     if (c.its->small_rows > 0) {
@@ -573,13 +576,17 @@ static int exdm_launch(Ctx& c, Tab tab, T* rows) {
     (void)c;
     (void)tab;
     (void)rows;
+    (void)B;
+    (void)rows32;
+    (void)mask;
     set_error_cstr("fused expand-demean requested for a tile narrower than 32 columns");
     return 1;
   }
 }
 
-template <typename T, int C, int U, class Tab>
-static int exdm_u(Ctx& c, Tab tab, T* rows) {
+template <typename T, int C, int U, class Tab, bool RESID = false>
+static int exdm_u(Ctx& c, Tab tab, T* rows, const double* B = nullptr, float* rows32 = nullptr,
+                  int mask = 0) {
   const fe_plan* pl = c.pl;
   bool w = false;
   int ns = 0;
@@ -589,24 +596,39 @@ static int exdm_u(Ctx& c, Tab tab, T* rows) {
     if ((small || k == pl->primary) && (pl->weighted || pl->interacted[k])) w = true;
   }
   const int sel = ns * 2 + (w ? 1 : 0);
+#define FE_EXDM_CASE(KB, W_, NS_) \
+  return exdm_launch<T, C, U, KB, W_, NS_, Tab, RESID>(c, tab, rows, B, rows32, mask)
   if (c.d.K <= 4) {
     switch (sel) {
-      case 0: return exdm_launch<T, C, U, 4, false, 0>(c, tab, rows);
-      case 1: return exdm_launch<T, C, U, 4, true, 0>(c, tab, rows);
-      case 2: return exdm_launch<T, C, U, 4, false, 1>(c, tab, rows);
-      case 3: return exdm_launch<T, C, U, 4, true, 1>(c, tab, rows);
-      case 4: return exdm_launch<T, C, U, 4, false, 2>(c, tab, rows);
-      default: return exdm_launch<T, C, U, 4, true, 2>(c, tab, rows);
+      case 0: FE_EXDM_CASE(4, false, 0);
+      case 1: FE_EXDM_CASE(4, true, 0);
+      case 2: FE_EXDM_CASE(4, false, 1);
+      case 3: FE_EXDM_CASE(4, true, 1);
+      case 4: FE_EXDM_CASE(4, false, 2);
+      default: FE_EXDM_CASE(4, true, 2);
     }
   }
   switch (sel) {
-    case 0: return exdm_launch<T, C, U, kMaxFE, false, 0>(c, tab, rows);
-    case 1: return exdm_launch<T, C, U, kMaxFE, true, 0>(c, tab, rows);
-    case 2: return exdm_launch<T, C, U, kMaxFE, false, 1>(c, tab, rows);
-    case 3: return exdm_launch<T, C, U, kMaxFE, true, 1>(c, tab, rows);
-    case 4: return exdm_launch<T, C, U, kMaxFE, false, 2>(c, tab, rows);
-    default: return exdm_launch<T, C, U, kMaxFE, true, 2>(c, tab, rows);
+    case 0: FE_EXDM_CASE(kMaxFE, false, 0);
+    case 1: FE_EXDM_CASE(kMaxFE, true, 0);
+    case 2: FE_EXDM_CASE(kMaxFE, false, 1);
+    case 3: FE_EXDM_CASE(kMaxFE, true, 1);
+    case 4: FE_EXDM_CASE(kMaxFE, false, 2);
+    default: FE_EXDM_CASE(kMaxFE, true, 2);
   }
+#undef FE_EXDM_CASE
+}
+
+// The refinement's residual of the absorbed mode in one pass (rounds after
+// the first): R64 = M (B64 - A_r x) with x the pre-scaled FP64 table, its FP32
+// copy U, ||R64||^2 and the small FEs' sums; columns whose refinement has
+// stopped keep their rows.
+template <int C>
+static int launch_resid_demean(Ctx& c, const double* xs64, double* R64, const double* B64,
+                               float* U, double bytes) {
+  ProfScope ps(c.pl, "resid_demean64", bytes);
+  return exdm_u<double, C, 4, TabPre64<vec_of<double, C>()>, true>(
+      c, TabPre64<vec_of<double, C>()>{xs64}, R64, B64, U, 2);
 }
 
 // The pipelined fused kernel (k_exdm_pipe): FP32 rows of 32-column tiles, at
@@ -899,7 +921,7 @@ struct Bytes {
   double expand, segsum, pupdate, resid64, segsum64, grad64, rowsum, rowsum64;
   // absorbed-primary mode
   double expand_abs, resid64_abs, demean, demean64, pupdate_np, grad64_np, expand_demean;
-  double prescale64, prescale64_abs;
+  double prescale64, prescale64_abs, resid_demean64;
 };
 static Bytes alg_bytes(const fe_plan* pl, const ItemSet* its, int C, int sT) {
   Bytes b{};
@@ -970,6 +992,9 @@ static Bytes alg_bytes(const fe_plan* pl, const ItemSet* its, int C, int sT) {
     // refs and weights, the small FEs' included) plus the primary FE's keys,
     // weights and scales
     b.expand_demean = b.expand_abs + N * (4.0 + (cwp ? sT : 0)) + Pp * sT;
+    // fused FP64 residual + projection: the residual's bytes, the FP32 copy,
+    // the primary FE's keys, weights and scales
+    b.resid_demean64 = b.resid64_abs + N * C * 4.0 + N * (4.0 + (cwp ? 8.0 : 0.0)) + Pp * 8.0;
     b.grad64_np = Pnp * C * (8.0 + 4.0 + 8.0 + 4.0 + 8.0);
   }
   b.pupdate = 9.0 * P * C * sT;
@@ -1613,11 +1638,14 @@ static int solve_mixed_tile(fe_plan* pl, const SolveReq& rq, int64_t col0, int n
     // (absorbed: r = M (b - A_r x), projected and copied by the demean pass)
     // absorbed: round 0 starts from x = 0, so r0 = M b comes straight from b
     const bool from_b = absorb && round == 0;
+    // absorbed rounds after the first, FE_OPT_FUSED_RESID: the residual and
+    // its projection in one pass
+    const bool fused_r = absorb && !from_b && pl->opt_fused_resid;
     if ((st = zero_slab(c, S64, 8))) return st;
     if (!from_b && (st = launch_prescale64(c, X64, X, w.XS64.as<double>(), absorb,
                                            absorb ? by.prescale64_abs : by.prescale64)))
       return st;
-    if (!from_b &&
+    if (!from_b && !fused_r &&
         (st = launch_expand<double, C>(
              c, TabPre64<vec_of<double, C>()>{w.XS64.as<double>()},
              EpiBminusAx<double, double, vec_of<double, C>()>{B64, R64, absorb ? nullptr : U, c.inst, 2},
@@ -1625,9 +1653,13 @@ static int solve_mixed_tile(fe_plan* pl, const SolveReq& rq, int64_t col0, int n
       return st;
     // g = A'r in FP64 (the next inner v), x64 += dx32, ||x64||
     if (absorb) {
-      if ((st = launch_demean<double, C>(c, R64, U, S64, "demean64", by.demean64,
-                                         from_b ? B64 : nullptr)))
+      if (fused_r) {
+        if ((st = launch_resid_demean<C>(c, w.XS64.as<double>(), R64, B64, U, by.resid_demean64)))
+          return st;
+      } else if ((st = launch_demean<double, C>(c, R64, U, S64, "demean64", by.demean64,
+                                                from_b ? B64 : nullptr))) {
         return st;
+      }
       if ((st = launch_segsum<double, C>(c, LoadIn<double, double, vec_of<double, C>()>{R64}, S64,
                                          "segsum64", by.segsum64, true, "", 0.0, true)))
         return st;

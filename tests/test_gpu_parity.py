@@ -421,11 +421,12 @@ def test_absorbed_primary_matches_oracle(fe, oracle, case):
     # Jacobi scales of A_r, full LSMR
     # and the gathered FE's level sums by vector reductions (atomic = 1; not
     # bitwise reproducible; its levels here hold at most ~100 positions) or by
-    # the deterministic segmented sum (0)
-    for absorb, fused, ascale, pipe, atomic in ((1, 1, 1, -1, 0), (1, 1, 1, -1, 1),
-                                                (1, 1, 1, 0, 0), (1, 1, 1, 1, 0), (1, 1, 1, 2, 0),
-                                                (1, 0, 1, -1, 0), (1, 1, 0, -1, 0),
-                                                (0, 1, 1, -1, 0)):
+    # the deterministic segmented sum (0); fres = 1: the refinement's FP64
+    # residual and its projection in one kernel
+    for absorb, fused, ascale, pipe, atomic, fres in (
+            (1, 1, 1, -1, 0, 0), (1, 1, 1, -1, 1, 0), (1, 1, 1, 0, 0, 0), (1, 1, 1, 1, 0, 0),
+            (1, 1, 1, 2, 0, 0), (1, 0, 1, -1, 0, 0), (1, 1, 0, -1, 0, 0), (0, 1, 1, -1, 0, 0),
+            (1, 1, 1, -1, 0, 1), (1, 0, 1, -1, 0, 1)):
         feM = fe.AbstractFixedEffectSolver(fes, w, "CUDA", np.float64, precision="mixed")
         feM.set_option(fe._lib.FE_OPT_TILE, 32)
         feM.set_option(fe._lib.FE_OPT_ABSORB, absorb)
@@ -433,6 +434,7 @@ def test_absorbed_primary_matches_oracle(fe, oracle, case):
         feM.set_option(fe._lib.FE_OPT_ABSORB_SCALE, ascale)
         feM.set_option(fe._lib.FE_OPT_EXDM_PIPE, pipe)
         feM.set_option(fe._lib.FE_OPT_FIRM_ATOMIC, atomic)
+        feM.set_option(fe._lib.FE_OPT_FUSED_RESID, fres)
         R, its, cvs = feM.solve_residuals(Y.copy(), tol=1e-8)
         R2, its2, _ = feM.solve_residuals(Y.copy(), tol=1e-8)
         feM.close()
