@@ -133,7 +133,9 @@ def throughput_figures(obs_iters: float, lsmr_iters, stats: dict, prof_steps: in
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+    """nvidia-smi clocks and throttle reasons sampled every 25 ms; entering
+    waits (up to 3 s) for the first sample, so the samples cover the timed
+    region that follows and not nvidia-smi's start-up."""
 
     def __init__(self, index: int):
         self.index = index
@@ -149,11 +151,24 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "25"],
                 stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
+            return self
+        t0 = time.time()
+        while time.time() - t0 < 3.0 and self.proc.poll() is None:
+            if os.path.getsize(self.path) > 0:
+                break
+            time.sleep(0.01)
+        self.skip = self._count()
         return self
+
+    def _count(self):
+        try:
+            return len(Path(self.path).read_text().strip().splitlines())
+        except Exception:
+            return 0
 
     def __exit__(self, *exc):
         if self.proc is not None:
@@ -169,6 +184,9 @@ class ClockSampler:
             rows = [r.split(",") for r in Path(self.path).read_text().strip().splitlines()]
         except Exception:
             return out
+        # the samples taken during the region (the one before it if none)
+        skip = getattr(self, "skip", 0)
+        rows = rows[skip:] if len(rows) > skip else rows[-1:]
         sm, smax, reasons = [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for r in rows:
@@ -547,21 +565,22 @@ def run_ours(args):
         feM_h.set_option(fe._lib.FE_OPT_ABSORB, 0)
     for name, val in plan_options(args):
         feM_h.set_option(getattr(fe._lib, name), val)
-    e2e = {}
+    e2e, e2e_calls = {}, {}
     for kind in ("pinned", "pageable"):
         buf, A = wl.host_buffers(torch, kind == "pinned")
         wl.refresh_host(A)
         wl.solve_host(feM_h, A)  # warm-up
         if dist:
             dist.barrier()
-        tot = 0.0
+        calls = []
         for _ in range(e2e_steps):
             wl.refresh_host(A)  # fresh inputs (outside the timed call)
             torch.cuda.synchronize()
             t = time.perf_counter()
             wl.solve_host(feM_h, A)
-            tot += (time.perf_counter() - t) * 1e3
-        tot /= e2e_steps
+            calls.append((time.perf_counter() - t) * 1e3)
+        e2e_calls[kind] = [round(x, 3) for x in calls]
+        tot = sum(calls) / e2e_steps
         if dist:
             t = torch.tensor([tot], device=dev, dtype=torch.float64)
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -650,7 +669,8 @@ def run_ours(args):
                     "ms_per_step": e2e["pinned"], "host_memory": "pinned",
                     "pageable": {"value": total / (e2e["pageable"] * 1e-3),
                                  "ms_per_step": e2e["pageable"],
-                                 "ratio_to_pinned_time": e2e["pageable"] / e2e["pinned"]}},
+                                 "ratio_to_pinned_time": e2e["pageable"] / e2e["pinned"]},
+                    "ms_per_call": e2e_calls},
             "roofline": {"bound": "hbm", "kernel": tname, "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": achieved / peak,
                          "frac_of_nominal_7700": achieved / 7700.0,

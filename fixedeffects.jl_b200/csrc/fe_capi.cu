@@ -384,9 +384,15 @@ int fe_plan_set_option(fe_plan* plan, int32_t option, double value) {
     case FE_OPT_FUSED_DEMEAN:
       plan->opt_exdm = value != 0 ? 1 : 0;
       return FE_OK;
-    case FE_OPT_FUSED_RESID:
-      plan->opt_fused_resid = value != 0 ? 1 : 0;
+    case FE_OPT_FUSED_RESID: {
+      const int v = (int)value;
+      if (v < -1 || v > 2) {
+        set_error("fused residual option must be -1 (default), 0, 1 or 2");
+        return FE_ERR_INVALID;
+      }
+      plan->opt_fused_resid = v;
       return FE_OK;
+    }
     case FE_OPT_ABSORB_SCALE:
       plan->opt_abs_scale = value != 0 ? 1 : 0;
       return FE_OK;

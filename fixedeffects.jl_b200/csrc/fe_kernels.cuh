@@ -974,12 +974,19 @@ k_rowsum_reg(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_item
 // read of an item's rows hits L1/L2.  Lane = column, STEP rows per step held
 // in registers.  The only cross-lane dependency is the z row of a level,
 // written by all lanes in pass 1 and read in pass 2 after a __syncwarp.
+//
+// NG > 0, the refinement's residual form: the rows are w = in - A_r x, with
+// `in` the right-hand side B and x given by the pre-scaled table xs
+// ([P][C], scale_l * x_l), the NG = K - 1 non-primary FEs gathered in FE
+// order (one coalesced row per FE and row, an L2 hit), the same sums as the
+// separate residual kernel; columns whose refinement has stopped
+// (inst[j].outer_active == 0) project their stored rows instead.
 // ---------------------------------------------------------------------------
-template <typename T, int C, bool W, int NS>
+template <typename T, int C, bool W, int NS, int NG = 0>
 __global__ void __launch_bounds__(kThreads, 2)
 k_demean(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_items, const T* in,
          T* rows, float* __restrict__ rows32, RowSumArgs rs, double* __restrict__ part,
-         int64_t S) {
+         int64_t S, const T* __restrict__ xs, const Inst* __restrict__ inst) {
   static_assert(C == 32, "one column per lane");
   constexpr int STEP = sizeof(T) == 4 ? 16 : 8;
   constexpr int RC = (int)kDemeanRows;  // rows of an item held in registers
@@ -1004,6 +1011,38 @@ k_demean(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_items, c
   const T* __restrict__ cw0 = NS > 0 ? cw_of<T>(d, rs.small_fe[0]) : nullptr;
   const T* __restrict__ cw1 = NS > 1 ? cw_of<T>(d, rs.small_fe[1]) : nullptr;
   const int off0 = rs.small_off[0], off1 = rs.small_off[1];
+  // residual form: the gathered FEs (every FE but the primary, in FE order),
+  // and whether this lane's column is still refined
+  const int32_t* __restrict__ gref[NG > 0 ? NG : 1];
+  const T* __restrict__ gcw[NG > 0 ? NG : 1];
+  const T* __restrict__ gtab[NG > 0 ? NG : 1];
+  bool ract = true;
+  if (NG > 0) {
+    int j = 0;
+    for (int k = 0; k < d.K && j < NG; ++k) {
+      if (k == kp) continue;
+      gref[j] = d.refs[k];
+      gcw[j] = cw_of<T>(d, k);
+      gtab[j] = xs + d.lev_base[k] * C + lane;
+      ++j;
+    }
+    ract = inst[lane].outer_active != 0;
+  }
+  // row p of w into registers: (B - A_r x) for refined columns, the stored row
+  // otherwise; ref/cw: the gathered FEs' refs and weights of row p
+  auto w_row = [&](int64_t p, const int (&ref)[NG > 0 ? NG : 1], const T (&cw)[NG > 0 ? NG : 1]) {
+    if (NG == 0) return in[p * C + lane];
+    T acc = T(0);
+    if (ract) {
+#pragma unroll
+      for (int j = 0; j < NG; ++j) {
+        const T t = gtab[j][(int64_t)ref[j] * C];
+        acc += gcw[j] ? cw[j] * t : t;
+      }
+      return in[p * C + lane] - acc;
+    }
+    return rows[p * C + lane];
+  };
   double nrm = 0.0;
   const int64_t wstride = (int64_t)gridDim.x * kWarps;
   for (int64_t wi = (int64_t)blockIdx.x * kWarps + wib; wi < n_items; wi += wstride) {
@@ -1033,9 +1072,45 @@ k_demean(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_items, c
         if (W && cw1) c1 = __ldg(cw1 + p);
       }
       T x[RC];
-      const T* src = in + it.ib * C + lane;
+      {
+        // the rows (residual form: the right-hand side, or the stored row of
+        // a stopped column)
+        const T* src = (NG > 0 && !ract ? rows : in) + it.ib * C + lane;
 #pragma unroll
-      for (int r = 0; r < RC; ++r) x[r] = r < n ? src[(int64_t)r * C] : T(0);
+        for (int r = 0; r < RC; ++r) x[r] = r < n ? src[(int64_t)r * C] : T(0);
+      }
+      if (NG > 0) {
+        // minus A_r x, four rows at a time: the gathers of a group are
+        // unconditional (padding rows read level 0), so they are in flight
+        // together; the sums are the residual kernel's, in FE order
+        int grl[NG > 0 ? NG : 1];
+        T gcl[NG > 0 ? NG : 1];
+#pragma unroll
+        for (int j = 0; j < NG; ++j) {
+          grl[j] = okl ? __ldg(gref[j] + p) : 0;
+          gcl[j] = (okl && gcw[j]) ? __ldg(gcw[j] + p) : T(1);
+        }
+#pragma unroll
+        for (int r0 = 0; r0 < RC; r0 += 4) {
+          if (r0 < n) {  // warp-uniform
+            T t[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+              t[q] = T(0);
+#pragma unroll
+              for (int j = 0; j < NG; ++j) {
+                const int ref = __shfl_sync(FE_FULL, grl[j], r0 + q);
+                const T cr = __shfl_sync(FE_FULL, gcl[j], r0 + q);
+                const T v = gtab[j][(int64_t)ref * C];
+                t[q] += gcw[j] ? cr * v : v;
+              }
+            }
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+              if (ract && r0 + q < n) x[r0 + q] -= t[q];
+          }
+        }
+      }
       const int kn = __shfl_down_sync(FE_FULL, kpr, 1);
       // level ends after row r: a key change, or the item's last row
       const uint32_t ends = __ballot_sync(FE_FULL, okl && (lane + 1 == n || kn != kpr));
@@ -1091,9 +1166,25 @@ k_demean(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_items, c
       const bool okl = lane < nvalid;
       const int kpr = okl ? __ldg(refp + base + lane) : kSentinel;
       const T cpv = (W && okl && cwp) ? __ldg(cwp + base + lane) : T(1);
+      int grl[NG > 0 ? NG : 1];
+      T gcl[NG > 0 ? NG : 1];
+#pragma unroll
+      for (int j = 0; j < NG; ++j) {
+        grl[j] = okl ? __ldg(gref[j] + base + lane) : 0;
+        gcl[j] = (okl && gcw[j]) ? __ldg(gcw[j] + base + lane) : T(1);
+      }
       T x[STEP];
 #pragma unroll
-      for (int r = 0; r < STEP; ++r) x[r] = r < nvalid ? in[(base + r) * C + lane] : T(0);
+      for (int r = 0; r < STEP; ++r) {
+        int rr[NG > 0 ? NG : 1];
+        T cr[NG > 0 ? NG : 1];
+#pragma unroll
+        for (int j = 0; j < NG; ++j) {
+          rr[j] = __shfl_sync(FE_FULL, grl[j], r);
+          cr[j] = __shfl_sync(FE_FULL, gcl[j], r);
+        }
+        x[r] = r < nvalid ? w_row(base + r, rr, cr) : T(0);
+      }
       const int kn = __shfl_down_sync(FE_FULL, kpr, 1);
       const uint32_t bmask = __ballot_sync(FE_FULL, lane + 1 < nvalid && kn != kpr);
       const int kfirst = __shfl_sync(FE_FULL, kpr, 0);
@@ -1129,6 +1220,13 @@ k_demean(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_items, c
         k1 = off1 + __ldg(ref1 + p);
         if (W && cw1) c1 = __ldg(cw1 + p);
       }
+      int grl[NG > 0 ? NG : 1];
+      T gcl[NG > 0 ? NG : 1];
+#pragma unroll
+      for (int j = 0; j < NG; ++j) {
+        grl[j] = okl ? __ldg(gref[j] + p) : 0;
+        gcl[j] = (okl && gcw[j]) ? __ldg(gcw[j] + p) : T(1);
+      }
       T x[STEP];
 #pragma unroll
       for (int r = 0; r < STEP; ++r) {
@@ -1136,7 +1234,14 @@ k_demean(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_items, c
           const int kr = __shfl_sync(FE_FULL, kpr, r);
           const T fr = __shfl_sync(FE_FULL, f, r);
           const int64_t o = (base + r) * C + lane;
-          const T u = in[o] - fr * Z[(int64_t)kr * C];
+          int rr[NG > 0 ? NG : 1];
+          T cr[NG > 0 ? NG : 1];
+#pragma unroll
+          for (int j = 0; j < NG; ++j) {
+            rr[j] = __shfl_sync(FE_FULL, grl[j], r);
+            cr[j] = __shfl_sync(FE_FULL, gcl[j], r);
+          }
+          const T u = w_row(base + r, rr, cr) - fr * Z[(int64_t)kr * C];
           rows[o] = u;
           if (rows32) rows32[o] = (float)u;
           nrm += (double)u * (double)u;

@@ -197,7 +197,7 @@ struct fe_plan {
   int32_t opt_rowsum_variant = -1; // row-sum pass: 0 shared-memory ring, 1 registers
   int32_t opt_absorb = 1;       // mixed residual solves project the primary FE out
   int32_t opt_exdm = 1;         // absorbed loop: fused expand + demean kernel
-  int32_t opt_fused_resid = 0;  // absorbed refinement: FP64 residual + projection in one kernel
+  int32_t opt_fused_resid = -1;  // absorbed refinement: FP64 residual + projection in one kernel
   int32_t opt_abs_scale = 1;    // absorbed loop: columns scaled by 1 / ||M a_l||
   int32_t opt_exdm_pipe = -1;   // absorbed loop: pipelined fused kernel (-1 default, 0 off, 1.. cfg)
   int32_t opt_firm_atomic = 0;  // absorbed loop: gathered FE's sums by reductions (-1 tuned, 0, 1)

@@ -441,10 +441,11 @@ static int launch_rowsum(Ctx& c, const TA* src, TA* out) {
 // its small-FE partials.  rows: [N][32] of T, projected in place; rows32: an
 // optional FP32 copy; out: the [P][C] sum slab (z rows of the primary FE,
 // small-FE sums); ||rows||^2 goes to the expand norm slots.
-template <typename T, int C, bool W, int NS>
-static int demean_launch(Ctx& c, const T* in, T* rows, float* rows32, T* out) {
+template <typename T, int C, bool W, int NS, int NG = 0>
+static int demean_launch(Ctx& c, const T* in, T* rows, float* rows32, T* out,
+                         const T* xs = nullptr) {
   if constexpr (C == 32) {
-    auto kern = k_demean<T, C, W, NS>;
+    auto kern = k_demean<T, C, W, NS, NG>;
     const size_t smem = (size_t)kWarps * (kDemeanRows + c.its->small_rows) * C * sizeof(T);
     static bool attr_set = false;  // per instantiation
     static size_t occ_smem = (size_t)-1;
@@ -475,7 +476,7 @@ static int demean_launch(Ctx& c, const T* in, T* rows, float* rows32, T* out) {
         ++rs.n_small;
       }
     kern<<<(unsigned)grid, kThreads, smem, c.s>>>(c.d, c.its->d_dm.as<ExpandItem>(), n, in, rows,
-                                                  rows32, rs, c.part_e, c.its->Se);
+                                                  rows32, rs, c.part_e, c.its->Se, xs, c.inst);
     FE_CK(cudaGetLastError());
     if (c.its->small_rows > 0) {
       SmallRows m{};
@@ -491,17 +492,19 @@ static int demean_launch(Ctx& c, const T* in, T* rows, float* rows32, T* out) {
     (void)rows;
     (void)rows32;
     (void)out;
+    (void)xs;
     set_error_cstr("demean pass requested for a tile narrower than 32 columns");
     return 1;
   }
 }
 
-// in: source rows (nullptr: rows, projected in place)
-template <typename T, int C>
-static int launch_demean(Ctx& c, T* rows, float* rows32, T* out, const char* name, double bytes,
-                         const T* in = nullptr) {
-  if (!in) in = rows;
-  ProfScope ps(c.pl, name, bytes);
+// in: source rows (nullptr: rows, projected in place).  xs (FP64 only): the
+// refinement's residual form, rows = M (in - A_r x) with xs the pre-scaled
+// table of x (resid_demean_fits: at most kDemeanResidFE gathered FEs).
+constexpr int kDemeanResidFE = 3;
+inline bool resid_demean_fits(const fe_plan* pl) { return pl->K - 1 <= kDemeanResidFE; }
+template <typename T, int C, int NG>
+static int demean_sel(Ctx& c, const T* in, T* rows, float* rows32, T* out, const T* xs) {
   const fe_plan* pl = c.pl;
   bool w = false;
   int ns = 0;
@@ -511,13 +514,32 @@ static int launch_demean(Ctx& c, T* rows, float* rows32, T* out, const char* nam
     if ((small || k == pl->primary) && (pl->weighted || pl->interacted[k])) w = true;
   }
   switch (ns * 2 + (w ? 1 : 0)) {
-    case 0: return demean_launch<T, C, false, 0>(c, in, rows, rows32, out);
-    case 1: return demean_launch<T, C, true, 0>(c, in, rows, rows32, out);
-    case 2: return demean_launch<T, C, false, 1>(c, in, rows, rows32, out);
-    case 3: return demean_launch<T, C, true, 1>(c, in, rows, rows32, out);
-    case 4: return demean_launch<T, C, false, 2>(c, in, rows, rows32, out);
-    default: return demean_launch<T, C, true, 2>(c, in, rows, rows32, out);
+    case 0: return demean_launch<T, C, false, 0, NG>(c, in, rows, rows32, out, xs);
+    case 1: return demean_launch<T, C, true, 0, NG>(c, in, rows, rows32, out, xs);
+    case 2: return demean_launch<T, C, false, 1, NG>(c, in, rows, rows32, out, xs);
+    case 3: return demean_launch<T, C, true, 1, NG>(c, in, rows, rows32, out, xs);
+    case 4: return demean_launch<T, C, false, 2, NG>(c, in, rows, rows32, out, xs);
+    default: return demean_launch<T, C, true, 2, NG>(c, in, rows, rows32, out, xs);
   }
+}
+template <typename T, int C>
+static int launch_demean(Ctx& c, T* rows, float* rows32, T* out, const char* name, double bytes,
+                         const T* in = nullptr, const T* xs = nullptr) {
+  if (!in) in = rows;
+  ProfScope ps(c.pl, name, bytes);
+  if constexpr (std::is_same<T, double>::value) {
+    if (xs) {
+      switch (c.pl->K - 1) {
+        case 1: return demean_sel<T, C, 1>(c, in, rows, rows32, out, xs);
+        case 2: return demean_sel<T, C, 2>(c, in, rows, rows32, out, xs);
+        case 3: return demean_sel<T, C, 3>(c, in, rows, rows32, out, xs);
+        default:
+          set_error_cstr("residual demean pass requested for more than 4 fixed effects");
+          return 1;
+      }
+    }
+  }
+  return demean_sel<T, C, 0>(c, in, rows, rows32, out, nullptr);
 }
 
 // The fused expand + demean of the absorbed-primary loop (k_expand_demean):
@@ -921,7 +943,7 @@ struct Bytes {
   double expand, segsum, pupdate, resid64, segsum64, grad64, rowsum, rowsum64;
   // absorbed-primary mode
   double expand_abs, resid64_abs, demean, demean64, pupdate_np, grad64_np, expand_demean;
-  double prescale64, prescale64_abs, resid_demean64;
+  double prescale64, prescale64_abs, resid_demean64, resid_dm64;
 };
 static Bytes alg_bytes(const fe_plan* pl, const ItemSet* its, int C, int sT) {
   Bytes b{};
@@ -995,6 +1017,9 @@ static Bytes alg_bytes(const fe_plan* pl, const ItemSet* its, int C, int sT) {
     // fused FP64 residual + projection: the residual's bytes, the FP32 copy,
     // the primary FE's keys, weights and scales
     b.resid_demean64 = b.resid64_abs + N * C * 4.0 + N * (4.0 + (cwp ? 8.0 : 0.0)) + Pp * 8.0;
+    // the demean kernel's residual form: the same bytes (the small FEs' keys
+    // are among the K - 1 gathered FEs' refs, counted once)
+    b.resid_dm64 = b.resid_demean64;
     b.grad64_np = Pnp * C * (8.0 + 4.0 + 8.0 + 4.0 + 8.0);
   }
   b.pupdate = 9.0 * P * C * sT;
@@ -1639,8 +1664,12 @@ static int solve_mixed_tile(fe_plan* pl, const SolveReq& rq, int64_t col0, int n
     // absorbed: round 0 starts from x = 0, so r0 = M b comes straight from b
     const bool from_b = absorb && round == 0;
     // absorbed rounds after the first, FE_OPT_FUSED_RESID: the residual and
-    // its projection in one pass
-    const bool fused_r = absorb && !from_b && pl->opt_fused_resid;
+    // its projection in one pass, by the demean kernel (2, and the default
+    // where it fits) or by the staged fused kernel (1)
+    const int fres = pl->opt_fused_resid < 0 ? (resid_demean_fits(pl) ? 2 : 0)
+                                             : (pl->opt_fused_resid == 2 && !resid_demean_fits(pl)
+                                                    ? 0 : pl->opt_fused_resid);
+    const bool fused_r = absorb && !from_b && fres != 0;
     if ((st = zero_slab(c, S64, 8))) return st;
     if (!from_b && (st = launch_prescale64(c, X64, X, w.XS64.as<double>(), absorb,
                                            absorb ? by.prescale64_abs : by.prescale64)))
@@ -1653,7 +1682,11 @@ static int solve_mixed_tile(fe_plan* pl, const SolveReq& rq, int64_t col0, int n
       return st;
     // g = A'r in FP64 (the next inner v), x64 += dx32, ||x64||
     if (absorb) {
-      if (fused_r) {
+      if (fused_r && fres == 2) {
+        if ((st = launch_demean<double, C>(c, R64, U, S64, "resid_demean64", by.resid_dm64, B64,
+                                           w.XS64.as<double>())))
+          return st;
+      } else if (fused_r) {
         if ((st = launch_resid_demean<C>(c, w.XS64.as<double>(), R64, B64, U, by.resid_demean64)))
           return st;
       } else if ((st = launch_demean<double, C>(c, R64, U, S64, "demean64", by.demean64,

@@ -105,12 +105,13 @@ extern "C" {
                                  per iteration on a uniform FE, slower per solve (the FP32
                                  sums in no fixed order cost iterations). */
 #define FE_OPT_FUSED_RESID 19 /* absorbed FE_PREC_MIXED residual solves, refinement rounds
-                                 after the first: 1 the FP64 residual b - A_r x and its
-                                 projection in one kernel (one pass over the rows instead
-                                 of two); 0 (default): the residual kernel, then the
-                                 projection.  Measured on 10M rows x 32 columns: 4.05 ms
-                                 per round fused against 1.32 + 1.34 ms separate (the
-                                 fused kernel holds one CTA per SM) */
+                                 after the first: the FP64 residual b - A_r x and its
+                                 projection in one pass over the rows.  -1 (default): 2
+                                 where the plan has at most 4 FEs, else 0; 2: the
+                                 projection kernel gathers the other FEs' pre-scaled
+                                 FP64 rows itself (the same sums as 0); 1: the staged
+                                 fused kernel (measured slower: it holds one CTA per
+                                 SM); 0: the residual kernel, then the projection */
 
 typedef struct fe_plan fe_plan;
 

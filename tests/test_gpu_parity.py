@@ -421,12 +421,14 @@ def test_absorbed_primary_matches_oracle(fe, oracle, case):
     # Jacobi scales of A_r, full LSMR
     # and the gathered FE's level sums by vector reductions (atomic = 1; not
     # bitwise reproducible; its levels here hold at most ~100 positions) or by
-    # the deterministic segmented sum (0); fres = 1: the refinement's FP64
-    # residual and its projection in one kernel
-    for absorb, fused, ascale, pipe, atomic, fres in (
-            (1, 1, 1, -1, 0, 0), (1, 1, 1, -1, 1, 0), (1, 1, 1, 0, 0, 0), (1, 1, 1, 1, 0, 0),
-            (1, 1, 1, 2, 0, 0), (1, 0, 1, -1, 0, 0), (1, 1, 0, -1, 0, 0), (0, 1, 1, -1, 0, 0),
-            (1, 1, 1, -1, 0, 1), (1, 0, 1, -1, 0, 1)):
+    # the deterministic segmented sum (0); fres: the refinement's FP64
+    # residual and its projection by the projection kernel (-1, the default,
+    # and 2; the same sums as 0, so bitwise equal results), as two kernels
+    # (0), or by the staged fused kernel (1)
+    cases = ((1, 1, 1, -1, 0, -1), (1, 1, 1, -1, 1, -1), (1, 1, 1, 0, 0, -1), (1, 1, 1, 1, 0, -1),
+             (1, 1, 1, 2, 0, -1), (1, 0, 1, -1, 0, -1), (1, 1, 0, -1, 0, -1), (0, 1, 1, -1, 0, -1),
+             (1, 1, 1, -1, 0, 0), (1, 1, 1, -1, 0, 2), (1, 1, 1, -1, 0, 1), (1, 0, 1, -1, 0, 1))
+    for absorb, fused, ascale, pipe, atomic, fres in cases:
         feM = fe.AbstractFixedEffectSolver(fes, w, "CUDA", np.float64, precision="mixed")
         feM.set_option(fe._lib.FE_OPT_TILE, 32)
         feM.set_option(fe._lib.FE_OPT_ABSORB, absorb)
@@ -446,6 +448,9 @@ def test_absorbed_primary_matches_oracle(fe, oracle, case):
         out.append(R)
     for R in out[1:]:
         assert max(rel_err(out[0][:, j], R[:, j]) for j in range(Y.shape[1])) < REL
+    # the projection kernel's residual form = the residual kernel + projection
+    i_def, i_sep, i_two = (cases.index((1, 1, 1, -1, 0, f)) for f in (-1, 0, 2))
+    assert np.array_equal(out[i_def], out[i_sep]) and np.array_equal(out[i_two], out[i_sep])
 
 
 def test_update_weights_drops_captured_loops(fe, synth):
