@@ -1080,7 +1080,7 @@ k_demean(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_items, c
         for (int r = 0; r < RC; ++r) x[r] = r < n ? src[(int64_t)r * C] : T(0);
       }
       if (NG > 0) {
-        // minus A_r x, four rows at a time: the gathers of a group are
+        // minus A_r x, GB rows at a time: the gathers of a group are
         // unconditional (padding rows read level 0), so they are in flight
         // together; the sums are the residual kernel's, in FE order
         int grl[NG > 0 ? NG : 1];
@@ -1090,12 +1090,13 @@ k_demean(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_items, c
           grl[j] = okl ? __ldg(gref[j] + p) : 0;
           gcl[j] = (okl && gcw[j]) ? __ldg(gcw[j] + p) : T(1);
         }
+        constexpr int GB = (NG <= 2 && !W) ? 8 : 4;  // rows gathered together (no spills)
 #pragma unroll
-        for (int r0 = 0; r0 < RC; r0 += 4) {
+        for (int r0 = 0; r0 < RC; r0 += GB) {
           if (r0 < n) {  // warp-uniform
-            T t[4];
+            T t[GB];
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
+            for (int q = 0; q < GB; ++q) {
               t[q] = T(0);
 #pragma unroll
               for (int j = 0; j < NG; ++j) {
@@ -1106,7 +1107,7 @@ k_demean(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_items, c
               }
             }
 #pragma unroll
-            for (int q = 0; q < 4; ++q)
+            for (int q = 0; q < GB; ++q)
               if (ract && r0 + q < n) x[r0 + q] -= t[q];
           }
         }
