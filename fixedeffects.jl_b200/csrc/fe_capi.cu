@@ -407,8 +407,8 @@ int fe_plan_set_option(fe_plan* plan, int32_t option, double value) {
     }
     case FE_OPT_EXDM_PIPE: {
       const int v = (int)value;
-      if (v < -1 || v > 2) {
-        set_error("pipelined absorbed kernel option must be -1 (default), 0 (off), 1 or 2");
+      if (v < -1 || v > 3) {
+        set_error("pipelined absorbed kernel option must be -1 (default), 0 (off), 1, 2 or 3");
         return FE_ERR_INVALID;
       }
       plan->opt_exdm_pipe = v;

@@ -9,16 +9,21 @@ namespace fe {
 
 namespace {
 
-template <int NL, int NS, bool W, int STG, bool PG, bool ATOM = false>
+template <int NL, int NS, bool W, int STG, bool PG, bool ATOM = false, int WARPS = kWarps>
 int launch_one(const ExdmLaunch& a) {
-  auto kern = k_exdm_pipe<NL, NS, W, STG, PG, ATOM>;
+  auto kern = k_exdm_pipe<NL, NS, W, STG, PG, ATOM, WARPS>;
   static size_t attr_smem = 0;  // per instantiation: the opt-in size set so far
   if (a.smem > attr_smem) {
     FE_CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)a.smem));
+    // the largest shared-memory carve-out, so that the CTAs the grid counts
+    // on (up to three of 4 warps) are resident together
+    FE_CK(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
+                               (int)cudaSharedmemCarveoutMaxShared));
     attr_smem = a.smem;
   }
-  kern<<<(unsigned)a.grid, kThreads, a.smem, a.stream>>>(a.d, a.items, a.n_items, a.tab, a.rows,
-                                                        a.inst, a.rs, a.sr, a.lf, a.part, a.S);
+  kern<<<(unsigned)a.grid, WARPS * 32, a.smem, a.stream>>>(a.d, a.items, a.n_items, a.tab,
+                                                          a.rows, a.inst, a.rs, a.sr, a.lf,
+                                                          a.part, a.S);
   FE_CK(cudaGetLastError());
   return 0;
 }
@@ -28,6 +33,7 @@ int launch_cfg(const ExdmLaunch& a, int cfg, bool atomic) {
   if constexpr (NL == 1) {
     if (atomic) return launch_one<NL, NS, W, 2, true, true>(a);
   }
+  if (cfg == 3) return launch_one<NL, NS, W, 2, false, false, 4>(a);
   return cfg == 2 ? launch_one<NL, NS, W, 2, false>(a) : launch_one<NL, NS, W, 2, true>(a);
 }
 

@@ -54,12 +54,14 @@ struct ExdmMeta {
 };
 
 // shared-memory bytes of one CTA of k_exdm_pipe with `stages` pipeline
-// stages and per-group (pg) or per-warp small-FE tables
-inline size_t exdm_pipe_smem(int NL, int small_rows, int stages, bool pg) {
+// stages, per-group (pg) or per-warp small-FE tables, `warps` warps, and the
+// small FEs' coefficient rows in shared memory (vsm) or read through L1
+inline size_t exdm_pipe_smem(int NL, int small_rows, int stages, bool pg, int warps = kWarps,
+                             bool vsm = true) {
   const size_t stage = (size_t)(1 + NL) * 32 * 32;
   const size_t per_warp = stages * stage + (NL == 0 ? 32 * 32 : 0) +
                           (pg ? 4 : 1) * (size_t)small_rows * 32 + 32;
-  return ((size_t)small_rows * 32 + kWarps * per_warp) * sizeof(float);
+  return ((vsm ? (size_t)small_rows * 32 : 0) + warps * per_warp) * sizeof(float);
 }
 
 __device__ __forceinline__ float4 f4_fma(float a, const float4 x, float4 y) {
@@ -88,8 +90,11 @@ __device__ __forceinline__ void red_add_v4(float* p, float a, float b, float c, 
 // before the launch) instead of by the level-order segmented sum that
 // follows; the order of the additions is not fixed, so the sums are not
 // bitwise reproducible.
-template <int NL, int NS, bool W, int STG, bool PG, bool ATOM = false>
-__global__ void __launch_bounds__(kThreads, 1)
+// WARPS < kWarps: small CTAs, three per SM; they read the small FEs'
+// coefficient rows through L1 instead of holding a shared copy (VG), so that
+// three CTAs' staging fits the shared memory of an SM.
+template <int NL, int NS, bool W, int STG, bool PG, bool ATOM = false, int WARPS = kWarps>
+__global__ void __launch_bounds__(WARPS * 32, WARPS < kWarps ? 3 : 1)
 k_exdm_pipe(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_items,
             const float* __restrict__ tab, float* __restrict__ rows,
             const Inst* __restrict__ inst, RowSumArgs rs, SmallRows sr, ExdmFEs lf,
@@ -97,9 +102,10 @@ k_exdm_pipe(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_items
   constexpr int C = 32, G = 4, RC = 32;
   constexpr int STAGE = (1 + NL) * RC * C;  // floats per stage
   constexpr int NT = PG ? 4 : 1;            // small-FE tables per warp
+  constexpr bool VG = WARPS < kWarps;       // small-FE rows through L1
+  constexpr int NTH = WARPS * 32;
   static_assert(STG == 2, "two copy stages: the item computed and the next");
   using Meta = ExdmMeta<NL, NS>;
-  __shared__ double sm[kWarps][32];
   extern __shared__ __align__(16) float xs_smem[];
   if (d.active_pre && *d.active_pre == 0) return;  // the whole CTA
   const int lane = threadIdx.x & 31;
@@ -107,15 +113,27 @@ k_exdm_pipe(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_items
   const int g = lane >> 3, jl = lane & 7;
   const int nsr = NS > 0 ? rs.small_rows : 0;
   const int wstride_f = STG * STAGE + (NL == 0 ? RC * C : 0) + NT * nsr * C + 32;
+  const int vsm_f = VG ? 0 : nsr * C;
   float* vsm = xs_smem;  // [nsr][32] the small FEs' pre-scaled coefficient rows
-  float* wbase = xs_smem + nsr * C + (size_t)wib * wstride_f;
+  float* wbase = xs_smem + vsm_f + (size_t)wib * wstride_f;
   float* zs_own = wbase + STG * STAGE;            // level sums when NL == 0
   float* tbl = zs_own + (NL == 0 ? RC * C : 0);   // [NT][nsr][32] small-FE sums
   int* lend = reinterpret_cast<int*>(tbl + NT * nsr * C);
-  for (int e = threadIdx.x; e < nsr * C; e += kThreads)
-    vsm[e] = tab[sr.slab_row[e / C] * C + (e % C)];
+  if (!VG)
+    for (int e = threadIdx.x; e < nsr * C; e += NTH)
+      vsm[e] = tab[sr.slab_row[e / C] * C + (e % C)];
   for (int e = lane; e < NT * nsr * C; e += 32) tbl[e] = 0.f;
   __syncthreads();
+  // small-FE coefficient row k (table row k = small_off[j] + ref of FE j):
+  // slab row lev_base[j's FE] + ref
+  int64_t vgoff[NS > 0 ? NS : 1];
+#pragma unroll
+  for (int j = 0; j < NS; ++j)
+    vgoff[j] = (int64_t)(d.lev_base[rs.small_fe[j]] - rs.small_off[j]) * C + jl * 4;
+  auto small_row = [&](int j, int k) -> float4 {
+    if (VG) return __ldg(reinterpret_cast<const float4*>(tab + vgoff[j] + (int64_t)k * C));
+    return *reinterpret_cast<const float4*>(vsm + k * C + jl * 4);
+  };
 
   const int kp = d.primary;
   const int32_t* __restrict__ refp = d.refs[kp];
@@ -250,8 +268,7 @@ k_exdm_pipe(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_items
         for (int j = 0; j < NL; ++j)
           a = f4_fma(cl[j], *reinterpret_cast<const float4*>(lg + j * RC * C + r * C + jl * 4), a);
 #pragma unroll
-        for (int j = 0; j < NS; ++j)
-          a = f4_fma(cs[j], *reinterpret_cast<const float4*>(vsm + ks[j] * C + jl * 4), a);
+        for (int j = 0; j < NS; ++j) a = f4_fma(cs[j], small_row(j, ks[j]), a);
         float4 w;
         w.x = av[0] * a.x + au[0] * o.x;
         w.y = av[1] * a.y + au[1] * o.y;
@@ -385,7 +402,7 @@ k_exdm_pipe(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_items
       for (int j = 0; j < NS; ++j) {
         const int k = offS[j] + __ldg(refS[j] + p);
         const float c = (W && cwS[j]) ? __ldg(cwS[j] + p) : 1.f;
-        a = f4_fma(c, *reinterpret_cast<const float4*>(vsm + k * C + jl * 4), a);
+        a = f4_fma(c, small_row(j, k), a);
       }
       float4 w;
       w.x = av[0] * a.x + au[0] * o.x;
@@ -465,8 +482,8 @@ k_exdm_pipe(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_items
     // is computed, the copies of item i+1 are in flight (stage s ^ 1), the
     // refs of item i+2 are being loaded into registers, and the descriptor of
     // item i+3; nothing loaded is used before the next step.
-    const int64_t wstride = (int64_t)gridDim.x * kWarps;
-    const int64_t w0 = (int64_t)blockIdx.x * kWarps + wib;
+    const int64_t wstride = (int64_t)gridDim.x * WARPS;
+    const int64_t w0 = (int64_t)blockIdx.x * WARPS + wib;
     ExpandItem d2 = load_desc(w0 + 2 * wstride);
     Meta m0 = load_meta(load_desc(w0));
     issue(m0, wbase);
@@ -488,7 +505,12 @@ k_exdm_pipe(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_items
     }
     cp_async_wait<0>();
   }
-  // ||u||^2 per column: groups, then warps in order -> the CTA's slot
+  // ||u||^2 per column: groups, then warps in order -> the CTA's slot.  The
+  // scratch of the warp sums reuses the start of the dynamic shared memory
+  // (staged rows and small-FE rows, dead once every warp is past its items),
+  // so that the CTA holds no static shared memory.
+  __syncthreads();
+  double(*sm)[32] = reinterpret_cast<double(*)[32]>(xs_smem);
 #pragma unroll
   for (int v = 0; v < 4; ++v) {
     double a = nrm[v];
@@ -500,7 +522,7 @@ k_exdm_pipe(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_items
   if (part != nullptr && threadIdx.x < C) {
     double t = 0.0;
 #pragma unroll
-    for (int w = 0; w < kWarps; ++w) t += sm[w][threadIdx.x];
+    for (int w = 0; w < WARPS; ++w) t += sm[w][threadIdx.x];
     part[(int64_t)threadIdx.x * S + blockIdx.x] = t;
     for (int64_t sl = (int64_t)blockIdx.x + gridDim.x; sl < S; sl += gridDim.x)
       part[(int64_t)threadIdx.x * S + sl] = 0.0;
@@ -509,10 +531,10 @@ k_exdm_pipe(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_items
     // small-FE sums: warp tables in warp order, groups in group order
     const int n = nsr * C;
     double* __restrict__ out = rs.small_part + (int64_t)blockIdx.x * n;
-    const float* t0 = xs_smem + nsr * C + STG * STAGE + (NL == 0 ? RC * C : 0);
-    for (int e = threadIdx.x; e < n; e += kThreads) {
+    const float* t0 = xs_smem + vsm_f + STG * STAGE + (NL == 0 ? RC * C : 0);
+    for (int e = threadIdx.x; e < n; e += NTH) {
       double t = 0.0;
-      for (int w = 0; w < kWarps; ++w)
+      for (int w = 0; w < WARPS; ++w)
 #pragma unroll
         for (int gg = 0; gg < NT; ++gg) t += (double)t0[(size_t)w * wstride_f + gg * n + e];
       out[e] = t;
@@ -541,13 +563,18 @@ struct ExdmLaunch {
 };
 
 // Kernel configurations (FE_OPT_EXDM_PIPE values): 1 per-group small-FE
-// tables (vector layout), 2 one table per warp (less shared memory).
+// tables (vector layout), 2 one table per warp (less shared memory), 3 one
+// table per warp in CTAs of 4 warps, three per SM, the small FEs' rows read
+// through L1.
 struct ExdmCfg {
   int stages;
   bool per_group;
+  int warps;
+  bool vsm;  // the small FEs' coefficient rows held in shared memory
 };
 inline ExdmCfg exdm_cfg(int cfg) {
-  return cfg == 2 ? ExdmCfg{2, false} : ExdmCfg{2, true};
+  if (cfg == 3) return ExdmCfg{2, false, 4, false};
+  return cfg == 2 ? ExdmCfg{2, false, kWarps, true} : ExdmCfg{2, true, kWarps, true};
 }
 
 // Launches k_exdm_pipe<nl, ns, w, stages, per_group> of configuration

@@ -692,11 +692,10 @@ static int exdm_choose(const Ctx& c, ExdmChoice* ch) {
   }
   if (ch->nl > 1) return 0;
   ch->nsr = ch->ns ? c.its->small_rows : 0;
-  // + the static norm scratch (kWarps x 32 doubles)
   auto fits = [&](int cfg) {
     const ExdmCfg k = exdm_cfg(cfg);
-    return exdm_pipe_smem(ch->nl, ch->nsr, k.stages, k.per_group) +
-               kWarps * 32 * sizeof(double) <= (size_t)smem_max;
+    return exdm_pipe_smem(ch->nl, ch->nsr, k.stages, k.per_group, k.warps, k.vsm) <=
+           (size_t)smem_max;
   };
   if (pl->opt_exdm_pipe > 0) {
     if (fits(pl->opt_exdm_pipe)) ch->cfg = pl->opt_exdm_pipe;
@@ -760,10 +759,21 @@ static int try_exdm_pipe(Ctx& c, const float* tab, float* rows, int* launched) {
   a.lf = lf;
   a.part = c.part_e;
   a.S = c.its->Se;
-  // one CTA per SM (the staging fills the shared memory); the norm slots are
-  // the expand's, so the grid must not exceed their count
-  a.grid = std::max<int64_t>(1, std::min<int64_t>(c.its->Se, c.its->sms));
-  a.smem = exdm_pipe_smem(nl, nsr, kc.stages, kc.per_group);
+  // as many CTAs as the shared memory of the SMs holds (one of 8 warps, or up
+  // to three of 4 warps); the norm slots are the expand's, so the grid must
+  // not exceed their count
+  a.smem = exdm_pipe_smem(nl, nsr, kc.stages, kc.per_group, kc.warps, kc.vsm);
+  static int smem_sm = -1, smem_res = 0;  // shared memory per SM, reserved per CTA
+  if (smem_sm < 0) {
+    int v = 0, r = 0;
+    FE_CK(cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerMultiprocessor, c.pl->device));
+    FE_CK(cudaDeviceGetAttribute(&r, cudaDevAttrReservedSharedMemoryPerBlock, c.pl->device));
+    smem_sm = v;
+    smem_res = r;
+  }
+  const size_t per_cta = a.smem + (size_t)smem_res;  // no static shared memory
+  const int per_sm = std::max(1, std::min(kc.warps < kWarps ? 3 : 1, (int)(smem_sm / per_cta)));
+  a.grid = std::max<int64_t>(1, std::min<int64_t>(c.its->Se, (int64_t)per_sm * c.its->sms));
   a.stream = c.s;
   int st = launch_exdm_pipe(a, nl, ns, w, cfg, c.firm_atomic && exdm_atomic_eligible(c.pl, ch));
   if (st) return st;
@@ -1210,7 +1220,7 @@ static int run_loop(fe_plan* pl, Ctx& c, int prec, int64_t cap, int32_t nact0, B
     key = key * 3 + (c.absorb ? 1u : 0u);
     key = key * 3 + (size_t)pl->opt_exdm;
     key = key * 3 + (size_t)pl->opt_abs_scale;
-    key = key * 3 + (size_t)(pl->opt_exdm_pipe + 1);
+    key = key * 7 + (size_t)(pl->opt_exdm_pipe + 1);
     key = key * 3 + (c.firm_atomic ? 1u : 0u);
     lg = &pl->graphs[{c.C, prec}];
     if (!lg->exec || lg->key != key) {

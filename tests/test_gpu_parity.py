@@ -426,7 +426,8 @@ def test_absorbed_primary_matches_oracle(fe, oracle, case):
     # and 2; the same sums as 0, so bitwise equal results), as two kernels
     # (0), or by the staged fused kernel (1)
     cases = ((1, 1, 1, -1, 0, -1), (1, 1, 1, -1, 1, -1), (1, 1, 1, 0, 0, -1), (1, 1, 1, 1, 0, -1),
-             (1, 1, 1, 2, 0, -1), (1, 0, 1, -1, 0, -1), (1, 1, 0, -1, 0, -1), (0, 1, 1, -1, 0, -1),
+             (1, 1, 1, 2, 0, -1), (1, 1, 1, 3, 0, -1), (1, 0, 1, -1, 0, -1), (1, 1, 0, -1, 0, -1),
+             (0, 1, 1, -1, 0, -1),
              (1, 1, 1, -1, 0, 0), (1, 1, 1, -1, 0, 2), (1, 1, 1, -1, 0, 1), (1, 0, 1, -1, 0, 1))
     for absorb, fused, ascale, pipe, atomic, fres in cases:
         feM = fe.AbstractFixedEffectSolver(fes, w, "CUDA", np.float64, precision="mixed")
