@@ -549,6 +549,10 @@ int plan_items(fe_plan* pl, int C, ItemSet** out) {
   int64_t total_rows = 0;
   for (int k = 0; k < pl->K; ++k) total_rows += pl->nlev[k];
   const int64_t Tp = item_size(total_rows);
+  // the non-primary FEs' levels alone (the absorbed loop's P side) are sized
+  // on their own count, so that their items fill the GPU in whole waves
+  const int64_t Tp_np =
+      item_size(total_rows - (pl->nprob == 1 ? pl->nlev[pl->primary] : 0));
 
   const int nprob = pl->nprob;
   const int K = pl->K;
@@ -634,21 +638,21 @@ int plan_items(fe_plan* pl, int C, ItemSet** out) {
     // Single-problem plans list the non-primary FEs first, padded on their
     // own, so that the absorbed-primary mode can run just that prefix.
     const size_t q0 = its->pu.size();
-    auto pu_fe = [&](int k) {
+    auto pu_fe = [&](int k, int64_t T) {
       const int64_t rb = pl->lev_base[k] + pl->prob_lev_off[(size_t)p * K + k];
       const int64_t re = pl->lev_base[k] + pl->prob_lev_off[(size_t)(p + 1) * K + k];
-      for (int64_t b = rb; b < re; b += Tp) its->pu.push_back({b, std::min(re, b + Tp), k, p});
+      for (int64_t b = rb; b < re; b += T) its->pu.push_back({b, std::min(re, b + T), k, p});
     };
     if (nprob == 1) {
       for (int k = 0; k < K; ++k)
-        if (k != kp) pu_fe(k);
+        if (k != kp) pu_fe(k, Tp_np);
       while ((its->pu.size() - q0) % kWarps) its->pu.push_back({0, 0, 0, p});
       if (its->pu.size() == q0)
         for (int w = 0; w < kWarps; ++w) its->pu.push_back({0, 0, 0, p});
       its->pu_np = (int64_t)its->pu.size();
-      pu_fe(kp);
+      pu_fe(kp, Tp);
     } else {
-      for (int k = 0; k < K; ++k) pu_fe(k);
+      for (int k = 0; k < K; ++k) pu_fe(k, Tp);
     }
     while ((its->pu.size() - q0) % kWarps) its->pu.push_back({0, 0, 0, p});
     if (its->pu.size() == q0)

@@ -454,6 +454,28 @@ def test_absorbed_primary_matches_oracle(fe, oracle, case):
     assert np.array_equal(out[i_def], out[i_sep]) and np.array_equal(out[i_two], out[i_sep])
 
 
+def test_absorbed_column_stopping_at_round0(fe):
+    # a zero column stops at refinement round 0 (||r0|| = 0): its residual is
+    # r0 = M b = 0.  The plan first solves a nonzero column in the same slot,
+    # so stale rows would show; the other columns are solved exactly as before.
+    rng = np.random.default_rng(23)
+    N = 40_000
+    refs = [rng.integers(1, 4001, N), rng.integers(1, 401, N), rng.integers(1, 21, N)]
+    fes = [fe.FixedEffect(r) for r in refs]
+    Y = np.asfortranarray(rng.standard_normal((N, 4)))
+    feM = fe.AbstractFixedEffectSolver(fes, None, "CUDA", np.float64, precision="mixed")
+    feM.set_option(fe._lib.FE_OPT_TILE, 32)
+    R1, its1, cv1 = feM.solve_residuals(Y.copy(order="F"), tol=1e-8)
+    Y2 = Y.copy(order="F")
+    Y2[:, 2] = 0.0
+    R2, its2, cv2 = feM.solve_residuals(Y2, tol=1e-8)
+    feM.close()
+    assert cv1.all() and cv2.all()
+    assert np.array_equal(R2[:, 2], np.zeros(N))
+    for j in (0, 1, 3):
+        assert np.array_equal(R2[:, j], R1[:, j]) and its2[j] == its1[j]
+
+
 def test_update_weights_drops_captured_loops(fe, synth):
     # a 32-column mixed solve captures its LSMR loop in a CUDA graph; switching
     # between unit and other weights must not replay the old capture
