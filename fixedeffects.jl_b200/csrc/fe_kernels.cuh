@@ -1821,28 +1821,33 @@ k_segsum(const FeDev d, const ReduceItem* __restrict__ items, int64_t n_items, L
 // data visible; keys and weights are copied by lane jl = 0 of each group and
 // shared through a __syncwarp.
 // ---------------------------------------------------------------------------
-// shared memory per warp of k_segsum_async
-template <typename TA, int C, int U, int S>
+// shared memory per warp of k_segsum_async.  VF > 0: VF elements per lane
+// instead of the default 16 bytes (FP64 32-column tiles take 4: 8 lanes per
+// row and 4 rows per warp instruction, as FP32 rows do).
+template <typename TA, int C, int U, int S, int VF = 0>
 struct AsyncSegLayout {
   using Sh = Shape<TA, C>;
-  static constexpr int STEP = Sh::G * U;
+  static constexpr int VEC = VF > 0 ? VF : Sh::VEC;
+  static constexpr int G = 32 / (C / VEC);
+  static constexpr int STEP = G * U;
   static constexpr int kRowBytes = C * (int)sizeof(TA);
   static constexpr int kStageRows = STEP * kRowBytes;
   static constexpr int kStage = kStageRows + STEP * (4 + (int)sizeof(TA));
   static constexpr int kWarpBytes = S * kStage;
 };
 
-template <typename TA, int C, int U, int S, class Load>
+template <typename TA, int C, int U, int S, class Load, int VF = 0>
 __global__ void __launch_bounds__(kThreads)
 k_segsum_async(const FeDev d, const ReduceItem* __restrict__ items, int64_t n_items, Load ld,
                TA* __restrict__ Sout, SplitArgs sa) {
-  using Sh = Shape<TA, C>;
-  constexpr int VEC = Sh::VEC, CL = Sh::CL, G = Sh::G;
-  using L = AsyncSegLayout<TA, C, U, S>;
+  using L = AsyncSegLayout<TA, C, U, S, VF>;
+  constexpr int VEC = L::VEC, CL = C / VEC, G = L::G;
+  static_assert(CL * G == 32, "lane groups fill the warp");
   constexpr int STEP = L::STEP;
   constexpr int NI = STEP >= 32 ? STEP / 32 : 1;
   static_assert(STEP <= 32 || STEP % 32 == 0, "a step's indices fill whole index registers");
   constexpr int CHUNK = VEC * (int)sizeof(TA);  // bytes a lane copies per row
+  constexpr int CP = CHUNK > 16 ? 16 : CHUNK;   // bytes per cp.async
   extern __shared__ __align__(16) unsigned char dyn_smem[];
   __shared__ double smt[kWarps][32];
   const int lane = threadIdx.x & 31;
@@ -1883,7 +1888,10 @@ k_segsum_async(const FeDev d, const ReduceItem* __restrict__ items, int64_t n_it
         const int row = u * G + g;
         const int64_t p = it.pb + step * STEP + row;
         if (i >= 0) {
-          cp_async<CHUNK>(st + row * L::kRowBytes + jl * CHUNK, in + (int64_t)i * C + jl * VEC);
+#pragma unroll
+          for (int q = 0; q < CHUNK / CP; ++q)
+            cp_async<CP>(st + row * L::kRowBytes + jl * CHUNK + q * CP,
+                         reinterpret_cast<const char*>(in + (int64_t)i * C + jl * VEC) + q * CP);
           if (jl == 0) {
             cp_async_bytes4(skey + row, key + p);
             if (cwp) cp_async<(int)sizeof(TA)>(scw + row, cwp + p);

@@ -802,19 +802,24 @@ static int launch_expand_demean(Ctx& c, Tab tab, T* rows, const char* name, doub
   return exdm_u<T, C, 2>(c, tab, rows);
 }
 
+// FP64 rows of 32-column tiles: 4 elements per lane (4 rows per warp
+// instruction, half the per-row work of 2 elements per lane), with half the
+// row slots per lane group so that a stage holds the same rows
 template <typename TA, int C, int U, int S, class Load>
 static int launch_segsum_async(Ctx& c, Load ld, TA* out, const ReduceItem* items, int64_t n,
                                unsigned grid) {
-  using L = AsyncSegLayout<TA, C, U, S>;
+  constexpr int VF = (std::is_same<TA, double>::value && C == 32) ? 4 : 0;
+  constexpr int UE = VF ? (U > 1 ? U / 2 : 1) : U;
+  using L = AsyncSegLayout<TA, C, UE, S, VF>;
   const int smem = kWarps * L::kWarpBytes;
   static bool attr_set = false;  // per instantiation (set once per process)
   if (!attr_set) {
-    FE_CK(cudaFuncSetAttribute(k_segsum_async<TA, C, U, S, Load>,
+    FE_CK(cudaFuncSetAttribute(k_segsum_async<TA, C, UE, S, Load, VF>,
                                cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     attr_set = true;
   }
-  k_segsum_async<TA, C, U, S, Load><<<grid, kThreads, smem, c.s>>>(c.d, items, n, ld, out,
-                                                                    c.seg_split());
+  k_segsum_async<TA, C, UE, S, Load, VF><<<grid, kThreads, smem, c.s>>>(c.d, items, n, ld, out,
+                                                                         c.seg_split());
   return 0;
 }
 
