@@ -802,13 +802,14 @@ static int launch_expand_demean(Ctx& c, Tab tab, T* rows, const char* name, doub
   return exdm_u<T, C, 2>(c, tab, rows);
 }
 
-// FP64 rows of 32-column tiles: 4 elements per lane (4 rows per warp
-// instruction, half the per-row work of 2 elements per lane), with half the
-// row slots per lane group so that a stage holds the same rows
+// Rows of 32-column tiles: 32 bytes per lane (FP64: 4 elements, 4 rows per
+// warp instruction; FP32: 8 elements, 8 rows), half the per-row work of
+// 16-byte lanes, with half the row slots per lane group so that a stage
+// holds the same rows
 template <typename TA, int C, int U, int S, class Load>
 static int launch_segsum_async(Ctx& c, Load ld, TA* out, const ReduceItem* items, int64_t n,
                                unsigned grid) {
-  constexpr int VF = (std::is_same<TA, double>::value && C == 32) ? 4 : 0;
+  constexpr int VF = C == 32 ? 32 / (int)sizeof(TA) : 0;
   constexpr int UE = VF ? (U > 1 ? U / 2 : 1) : U;
   using L = AsyncSegLayout<TA, C, UE, S, VF>;
   const int smem = kWarps * L::kWarpBytes;
