@@ -1289,6 +1289,140 @@ k_demean(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_items, c
 }
 
 // ---------------------------------------------------------------------------
+// k_demean_narrow: the projection of the absorbed-primary mode (as k_demean)
+// for tiles of C < 32 columns.  One warp per demean item.  An item's rows are
+// contiguous C-element rows, so its element e = lane + 32 k lies in row e / C
+// and column e % C = lane % C (32 is a multiple of C): every lane keeps one
+// column.  A short item (at most kDemeanRows rows) is read in KC chunks of 32
+// elements; in each chunk the level sums of cw x are scanned over the rows of
+// each column (lanes C apart; the levels are contiguous rows, so a lane adds
+// the partial d rows back only within its own level), the open level's partial
+// carries into the next chunk, and each level's total is kept at its last row
+// in shared memory; then u = x - cw scale_l^2 z_l.  A long item (one level) is
+// summed per lane and reduced over the lanes of each column, then projected
+// in a second pass over memory.  ||u||^2 per column goes to the CTA's norm
+// slot.  `in` is the source (== rows for the in-place projection); rows
+// (optional) and rows32 (optional FP32 copy) receive u.
+// ---------------------------------------------------------------------------
+template <typename T, int C, bool W>
+__global__ void __launch_bounds__(kThreads)
+k_demean_narrow(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_items,
+                const T* in, T* rows, float* __restrict__ rows32, double* __restrict__ part,
+                int64_t S) {
+  static_assert(C < 32 && 32 % C == 0, "tiles narrower than a warp");
+  constexpr int RC = (int)kDemeanRows;
+  static_assert(RC == 32, "one item row per lane for the keys");
+  constexpr int KC = RC * C / 32;  // chunks of 32 elements in a short item
+  constexpr int RPC = 32 / C;      // rows per chunk
+  __shared__ T zs[kWarps][RC * C];  // level sums z (level, column)
+  __shared__ double sm[kWarps][32];
+  if (d.active_pre && *d.active_pre == 0) return;  // the whole CTA
+  const int lane = threadIdx.x & 31;
+  const int wib = threadIdx.x >> 5;
+  const int col = lane % C;
+  const int kp = d.primary;
+  const int32_t* __restrict__ refp = d.refs[kp];
+  const T* __restrict__ cwp = cw_of<T>(d, kp);
+  const T* __restrict__ scp = scale_of<T>(d, kp);
+  T* zb = zs[wib];
+  double nrm = 0.0;
+  const int64_t wstride = (int64_t)gridDim.x * kWarps;
+  for (int64_t wi = (int64_t)blockIdx.x * kWarps + wib; wi < n_items; wi += wstride) {
+    const ExpandItem it = items[wi];
+    const int64_t ib = it.ib;
+    if (it.ie <= ib) continue;
+    if (it.ie - ib <= RC) {
+      const int n = (int)(it.ie - ib);
+      const bool okl = lane < n;
+      const int kpr = okl ? __ldg(refp + ib + lane) : kSentinel;
+      const T cwv = (W && okl && cwp) ? __ldg(cwp + ib + lane) : T(1);
+      T f = T(0);  // cw scale^2 of row `lane`
+      if (okl) {
+        const T sl = __ldg(scp + kpr);
+        f = sl * sl * cwv;
+      }
+      const int kn = __shfl_down_sync(FE_FULL, kpr, 1);
+      // level ends after row r: a key change, or the item's last row
+      const uint32_t ends = __ballot_sync(FE_FULL, okl && (lane + 1 == n || kn != kpr));
+      const T* src = in + ib * C;
+      T x[KC];
+#pragma unroll
+      for (int k = 0; k < KC; ++k) {
+        const int e = lane + 32 * k;
+        x[k] = e < n * C ? src[e] : T(0);
+      }
+      T carry = T(0);   // the partial of the level open at the previous chunk's end
+      int carry_lv = -1;
+#pragma unroll
+      for (int k = 0; k < KC; ++k) {
+        if (RPC * k >= n) break;  // warp-uniform
+        const int r = (lane + 32 * k) / C;
+        const int lv = __popc(ends & ((1u << r) - 1u));
+        const T cr = W ? __shfl_sync(FE_FULL, cwv, r) : T(1);
+        T v = W ? cr * x[k] : x[k];
+#pragma unroll
+        for (int dd = C; dd < 32; dd <<= 1) {
+          const T o = __shfl_up_sync(FE_FULL, v, dd);
+          const int lo = __shfl_up_sync(FE_FULL, lv, dd);
+          if (lane >= dd && lo == lv) v += o;
+        }
+        if (lv == carry_lv) v += carry;
+        if (r < n && ((ends >> r) & 1u)) zb[lv * C + col] = v;
+        carry = __shfl_sync(FE_FULL, v, 32 - C + col);
+        carry_lv = __shfl_sync(FE_FULL, lv, 32 - C + col);
+      }
+      __syncwarp();
+#pragma unroll
+      for (int k = 0; k < KC; ++k) {
+        const int e = lane + 32 * k;
+        const int r = e / C;  // < 32
+        const T fr = __shfl_sync(FE_FULL, f, r);
+        if (e < n * C) {
+          const int lv = __popc(ends & ((1u << r) - 1u));
+          const T u = x[k] - fr * zb[lv * C + col];
+          if (rows) rows[ib * C + e] = u;
+          if (rows32) rows32[ib * C + e] = (float)u;
+          nrm += (double)u * (double)u;
+        }
+      }
+      __syncwarp();  // zb is rewritten by the next item
+      continue;
+    }
+    // one level longer than RC rows: z per column over the whole level
+    const T sl = __ldg(scp + __ldg(refp + ib));
+    const int64_t ne = (it.ie - ib) * C;
+    T acc = T(0);
+    for (int64_t e = lane; e < ne; e += 32) {
+      const T v = in[ib * C + e];
+      acc += (W && cwp) ? __ldg(cwp + ib + e / C) * v : v;
+    }
+#pragma unroll
+    for (int o = C; o < 32; o <<= 1) acc += __shfl_xor_sync(FE_FULL, acc, o);
+    for (int64_t e = lane; e < ne; e += 32) {
+      const T cr = (W && cwp) ? __ldg(cwp + ib + e / C) : T(1);
+      const T u = in[ib * C + e] - sl * sl * cr * acc;
+      if (rows) rows[ib * C + e] = u;
+      if (rows32) rows32[ib * C + e] = (float)u;
+      nrm += (double)u * (double)u;
+    }
+  }
+  // ||u||^2 per column: the lanes of a column, then warps in order -> the
+  // CTA's slot (slots beyond the grid hold 0)
+#pragma unroll
+  for (int o = C; o < 32; o <<= 1) nrm += __shfl_xor_sync(FE_FULL, nrm, o);
+  if (lane < C) sm[wib][lane] = nrm;
+  __syncthreads();
+  if (part != nullptr && threadIdx.x < C) {
+    double t = 0.0;
+#pragma unroll
+    for (int w = 0; w < kWarps; ++w) t += sm[w][threadIdx.x];
+    part[(int64_t)threadIdx.x * S + blockIdx.x] = t;
+    for (int64_t sl = (int64_t)blockIdx.x + gridDim.x; sl < S; sl += gridDim.x)
+      part[(int64_t)threadIdx.x * S + sl] = 0.0;
+  }
+}
+
+// ---------------------------------------------------------------------------
 // k_expand_demean: the expand and the demean of the absorbed-primary mode in
 // one pass over the rows (32-column tiles).  Per demean item (whole primary
 // levels, at most kDemeanRows rows):

@@ -706,11 +706,11 @@ int plan_items(fe_plan* pl, int C, ItemSet** out) {
       if (cur_b >= 0) dst.push_back({cur_b, cur_e, k, p, -1, 0});
     }
   }
-  // demean items (absorbed-primary mode: 32-column tiles, one problem, 2+ FEs):
-  // whole primary levels packed up to kDemeanRows rows; a longer level is one
-  // item of its own (the pass walks each item twice, so short items keep the
-  // second read in cache)
-  if (C == 32 && nprob == 1 && K >= 2) {
+  // demean items (absorbed-primary mode: one problem, 2+ FEs): whole primary
+  // levels packed up to kDemeanRows rows; a longer level is one item of its
+  // own (the pass walks each item twice, so short items keep the second read
+  // in cache)
+  if (nprob == 1 && K >= 2) {
     const std::vector<int64_t>& off = pl->seg_off[kp];
     const int64_t nl = pl->nlev[kp];
     int64_t cur_b = -1, cur_e = -1;

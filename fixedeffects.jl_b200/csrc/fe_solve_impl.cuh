@@ -36,52 +36,57 @@ namespace fe {
 // load / unload / coefficient kernels
 // ---------------------------------------------------------------------------
 // B[q][j] = y[i][col0 + j] * sqrt(w_i) with q the sorted position of i
-// (src/AbstractFixedEffectSolver.jl:50-55).  A CTA stages kLoadRows
-// observations x C columns in shared memory: the reads are coalesced along
-// observations (column-major input), the writes are whole contiguous rows.
-// Every thread issues all its loads (kLoadPer, independent) before the first
-// shared-memory store, so 16 KB per CTA are in flight at C = 32.  C is a
-// compile-time power of two (index splits are shifts) and W says whether there
-// are weights (without, no multiply or divide by sqrt(w) = 1).
-constexpr int kLoadRows = 64;
-template <int C> constexpr int load_per() { return kLoadRows * C >= 256 ? kLoadRows * C / 256 : 1; }
+// (src/AbstractFixedEffectSolver.jl:50-55).  A CTA stages load_rows<C>()
+// observations x C columns (2048 elements, 8 per thread, for every tile
+// width) in shared memory: the reads are coalesced along observations
+// (column-major input), the writes are whole contiguous rows.  Every thread
+// issues all its loads before the first shared-memory store, so 16 KB per CTA
+// are in flight.  C is a compile-time power of two (index splits are shifts)
+// and W says whether there are weights (without, no multiply or divide by
+// sqrt(w) = 1).
+constexpr int kLoadElems = 2048;  // elements per CTA
+constexpr int kLoadPer = kLoadElems / 256;
+template <int C> constexpr int load_rows() { return kLoadElems / C; }
+// the row padding of the staged tile (none for one column, whose accesses
+// run along rows in both phases)
+template <int C> constexpr int load_pad() { return C == 1 ? 0 : 1; }
 template <typename TY, int C, bool W>
 __global__ void __launch_bounds__(256) k_load(const TY* __restrict__ Y, int64_t ld, int64_t col0,
                                               int ncols, const int32_t* __restrict__ dst,
                                               const double* __restrict__ sw,
                                               double* __restrict__ B, int64_t N) {
-  constexpr int PER = load_per<C>();
-  constexpr int JS = 256 / kLoadRows;  // column stride between a thread's loads
-  __shared__ double tile[kLoadRows][C + 1];
-  __shared__ int32_t rows[kLoadRows];
-  const int64_t i0 = (int64_t)blockIdx.x * kLoadRows;
-  // load phase: thread t reads row t % kLoadRows of columns t / kLoadRows + JS u
-  const int r = threadIdx.x % kLoadRows, j0 = threadIdx.x / kLoadRows;
-  const int64_t i = i0 + r;
-  const bool in = i < N;
-  double v[PER];
+  constexpr int R = load_rows<C>();
+  __shared__ double tile[R][C + load_pad<C>()];
+  __shared__ int32_t rows[R];
+  const int64_t i0 = (int64_t)blockIdx.x * R;
+  // load phase: element e = t + 256 u in column-major order (column e / R,
+  // row e % R)
+  double v[kLoadPer];
 #pragma unroll
-  for (int u = 0; u < PER; ++u) {
-    const int j = j0 + u * JS;
-    v[u] = (in && j < ncols) ? (double)Y[i + (col0 + j) * ld] : 0.0;
+  for (int u = 0; u < kLoadPer; ++u) {
+    const int e = threadIdx.x + u * 256;
+    const int j = e / R, r = e % R;
+    const int64_t i = i0 + r;
+    double x = 0.0;
+    if (i < N && j < ncols) {
+      x = (double)Y[i + (col0 + j) * ld];
+      if (W) x *= sw[i];
+    }
+    v[u] = x;
   }
-  if (threadIdx.x < kLoadRows)
-    rows[threadIdx.x] = (i0 + threadIdx.x < N) ? dst[i0 + threadIdx.x] : -1;
-  const double s = (W && in) ? sw[i] : 1.0;
+  for (int r = threadIdx.x; r < R; r += 256) rows[r] = (i0 + r < N) ? dst[i0 + r] : -1;
 #pragma unroll
-  for (int u = 0; u < PER; ++u) {
-    const int j = j0 + u * JS;
-    if (j < C) tile[r][j] = W ? v[u] * s : v[u];
+  for (int u = 0; u < kLoadPer; ++u) {
+    const int e = threadIdx.x + u * 256;
+    tile[e % R][e / R] = v[u];
   }
   __syncthreads();
 #pragma unroll
-  for (int u = 0; u < PER; ++u) {
+  for (int u = 0; u < kLoadPer; ++u) {
     const int e = threadIdx.x + u * 256;
     const int rr = e / C, j = e % C;
-    if (e < kLoadRows * C) {
-      const int32_t q = rows[rr];
-      if (q >= 0) B[(int64_t)q * C + j] = tile[rr][j];
-    }
+    const int32_t q = rows[rr];
+    if (q >= 0) B[(int64_t)q * C + j] = tile[rr][j];
   }
 }
 
@@ -89,38 +94,37 @@ __global__ void __launch_bounds__(256) k_load(const TY* __restrict__ Y, int64_t 
 // whole rows in (all of a thread's row loads issued before the first
 // shared-memory store), coalesced columns out.
 template <typename TY, int C, bool W>
-__global__ void __launch_bounds__(256) k_unload(const double* __restrict__ R, int64_t ld,
+__global__ void __launch_bounds__(256) k_unload(const double* __restrict__ Rw, int64_t ld,
                                                 int64_t col0, int ncols,
                                                 const int32_t* __restrict__ dst,
                                                 const double* __restrict__ sw,
                                                 TY* __restrict__ Y, int64_t N) {
-  constexpr int PER = load_per<C>();
-  constexpr int JS = 256 / kLoadRows;
-  __shared__ double tile[kLoadRows][C + 1];
-  const int64_t i0 = (int64_t)blockIdx.x * kLoadRows;
-  double v[PER];
+  constexpr int R = load_rows<C>();
+  __shared__ double tile[R][C + load_pad<C>()];
+  const int64_t i0 = (int64_t)blockIdx.x * R;
+  double v[kLoadPer];
 #pragma unroll
-  for (int u = 0; u < PER; ++u) {
+  for (int u = 0; u < kLoadPer; ++u) {
     const int e = threadIdx.x + u * 256;
     const int rr = e / C, j = e % C;
     const int64_t i = i0 + rr;
-    v[u] = (e < kLoadRows * C && i < N) ? R[(int64_t)dst[i] * C + j] : 0.0;
+    v[u] = i < N ? Rw[(int64_t)dst[i] * C + j] : 0.0;
   }
 #pragma unroll
-  for (int u = 0; u < PER; ++u) {
+  for (int u = 0; u < kLoadPer; ++u) {
     const int e = threadIdx.x + u * 256;
-    const int rr = e / C, j = e % C;
-    if (e < kLoadRows * C) tile[rr][j] = v[u];
+    tile[e / C][e % C] = v[u];
   }
   __syncthreads();
-  const int r = threadIdx.x % kLoadRows, j0 = threadIdx.x / kLoadRows;
-  const int64_t i = i0 + r;
-  if (i >= N) return;
-  const double s = W ? sw[i] : 1.0;
 #pragma unroll
-  for (int u = 0; u < PER; ++u) {
-    const int j = j0 + u * JS;
-    if (j < ncols) Y[i + (col0 + j) * ld] = (TY)(W ? tile[r][j] / s : tile[r][j]);
+  for (int u = 0; u < kLoadPer; ++u) {
+    const int e = threadIdx.x + u * 256;
+    const int j = e / R, r = e % R;
+    const int64_t i = i0 + r;
+    if (i < N && j < ncols) {
+      const double x = tile[r][j];
+      Y[i + (col0 + j) * ld] = (TY)(W ? x / sw[i] : x);
+    }
   }
 }
 
@@ -486,6 +490,23 @@ static int demean_launch(Ctx& c, const T* in, T* rows, float* rows32, T* out,
       FE_CK(cudaGetLastError());
     }
     return 0;
+  } else if constexpr (NS == 0 && NG == 0 && C < 32) {
+    // narrow tiles (no small FEs, the residual computed apart)
+    (void)out;
+    (void)xs;
+    const int64_t n = (int64_t)c.its->dm.size();
+    static int occ = 0;  // resident CTAs per SM, per instantiation
+    if (occ == 0) {
+      int o = 0;
+      FE_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, k_demean_narrow<T, C, W>, kThreads, 0));
+      occ = std::max(o, 1);
+    }
+    const int64_t grid =
+        std::max<int64_t>(1, std::min<int64_t>(c.its->Se, (int64_t)occ * c.its->sms));
+    k_demean_narrow<T, C, W><<<(unsigned)grid, kThreads, 0, c.s>>>(
+        c.d, c.its->d_dm.as<ExpandItem>(), n, in, rows, rows32, c.part_e, c.its->Se);
+    FE_CK(cudaGetLastError());
+    return 0;
   } else {
     (void)c;
     (void)in;
@@ -493,7 +514,7 @@ static int demean_launch(Ctx& c, const T* in, T* rows, float* rows32, T* out,
     (void)rows32;
     (void)out;
     (void)xs;
-    set_error_cstr("demean pass requested for a tile narrower than 32 columns");
+    set_error_cstr("demean pass with small fixed effects requested for a narrow tile");
     return 1;
   }
 }
@@ -950,7 +971,8 @@ static bool use_rowsum(const fe_plan* pl, int C) {
 // a_l the unit columns of the primary FE (contiguous row segments).  LSMR then
 // iterates over the other FEs' levels only, on a better-conditioned operator.
 static bool use_absorb(const fe_plan* pl, const ItemSet* its, int C) {
-  return pl->opt_absorb != 0 && C == 32 && pl->nprob == 1 && pl->K >= 2 && !its->dm.empty();
+  (void)C;  // tiles of every width: k_demean (32 columns) or k_demean_narrow
+  return pl->opt_absorb != 0 && pl->nprob == 1 && pl->K >= 2 && !its->dm.empty();
 }
 
 // algorithmic bytes per launch (the roofline numerators): every index vector
@@ -1123,13 +1145,13 @@ static int prepare(fe_plan* pl, int C, int sT, bool mixed, Ctx& c) {
 
 template <int C, typename TY, bool W>
 static void launch_load(const fe_plan* pl, Ctx& c, const SolveReq& rq, int64_t col0, int ncols) {
-  k_load<TY, C, W><<<grid1(pl->N, kLoadRows), 256, 0, c.s>>>(
+  k_load<TY, C, W><<<grid1(pl->N, load_rows<C>()), 256, 0, c.s>>>(
       (const TY*)rq.Y, rq.ld, col0, ncols, pl->d_obs_dst.as<int32_t>(),
       W ? pl->d_sw_orig.as<double>() : nullptr, pl->ws.B64.as<double>(), pl->N);
 }
 template <int C, typename TY, bool W>
 static void launch_unload(const fe_plan* pl, Ctx& c, const SolveReq& rq, int64_t col0, int ncols) {
-  k_unload<TY, C, W><<<grid1(pl->N, kLoadRows), 256, 0, c.s>>>(
+  k_unload<TY, C, W><<<grid1(pl->N, load_rows<C>()), 256, 0, c.s>>>(
       pl->ws.R64.as<double>(), rq.ld, col0, ncols, pl->d_obs_dst.as<int32_t>(),
       W ? pl->d_sw_orig.as<double>() : nullptr, (TY*)rq.Y, pl->N);
 }
@@ -1666,7 +1688,9 @@ static int solve_mixed_tile(fe_plan* pl, const SolveReq& rq, int64_t col0, int n
   pg.inst = c.inst;
   // the fused absorbed loop gathers scale * v, kept beside v by both P-side
   // updates
-  float* VS = (absorb && pl->opt_exdm) ? w.VS.as<float>() : nullptr;
+  // (32-column tiles; narrower tiles run the expand, then the projection)
+  const bool exdm = absorb && pl->opt_exdm && C == 32;
+  float* VS = exdm ? w.VS.as<float>() : nullptr;
   pe.VS = VS;
   pg.VS32 = VS;
   const int64_t cap = std::max<int64_t>(rq.maxiter, 1) + 2;
@@ -1682,9 +1706,10 @@ static int solve_mixed_tile(fe_plan* pl, const SolveReq& rq, int64_t col0, int n
     // absorbed rounds after the first, FE_OPT_FUSED_RESID: the residual and
     // its projection in one pass, by the demean kernel (2, and the default
     // where it fits) or by the staged fused kernel (1)
-    const int fres = pl->opt_fused_resid < 0 ? (resid_demean_fits(pl) ? 2 : 0)
-                                             : (pl->opt_fused_resid == 2 && !resid_demean_fits(pl)
-                                                    ? 0 : pl->opt_fused_resid);
+    const int fres = C != 32 ? 0
+                     : pl->opt_fused_resid < 0 ? (resid_demean_fits(pl) ? 2 : 0)
+                                               : (pl->opt_fused_resid == 2 && !resid_demean_fits(pl)
+                                                      ? 0 : pl->opt_fused_resid);
     const bool fused_r = absorb && !from_b && fres != 0;
     if ((st = zero_slab(c, S64, 8))) return st;
     if (!from_b && (st = launch_prescale64(c, X64, X, w.XS64.as<double>(), absorb,
@@ -1738,7 +1763,7 @@ static int solve_mixed_tile(fe_plan* pl, const SolveReq& rq, int64_t col0, int n
               FE_CK(cudaMemsetAsync(S32 + (size_t)pl->lev_base[k] * C, 0,
                                     (size_t)(pl->nlev[k] + 1) * C * 4, c.s));
         }
-        if (pl->opt_exdm) {
+        if (exdm) {
           if ((e = launch_expand_demean<float, C>(c, TabOne<float, float, vec_of<float, C>()>{VS}, U,
                                                   "expand_demean", by.expand_demean)))
             return e;

@@ -454,6 +454,40 @@ def test_absorbed_primary_matches_oracle(fe, oracle, case):
     assert np.array_equal(out[i_def], out[i_sep]) and np.array_equal(out[i_two], out[i_sep])
 
 
+@pytest.mark.parametrize("ncols,weighted", [(1, False), (1, True), (3, True), (8, False), (8, True)])
+def test_absorbed_narrow_tiles(fe, oracle, ncols, weighted):
+    # mixed residual solves of tiles narrower than 32 columns with the primary
+    # FE projected out (k_demean_narrow), with one primary level longer than a
+    # demean item: against the oracle, the full-LSMR path (FE_OPT_ABSORB = 0)
+    # and bitwise across two calls
+    rng = np.random.default_rng(29)
+    N = 50_000
+    r1 = rng.integers(1, 5001, N)
+    r1[rng.random(N) < 0.1] = 7  # one long primary level
+    r2 = rng.integers(1, 601, N)
+    r3 = rng.integers(1, 31, N)
+    inter = [None, None, rng.uniform(0.5, 1.5, N) if weighted else None]
+    w = rng.uniform(0.5, 1.5, N) if weighted else None
+    refs = [r1, r2, r3]
+    Y = np.asfortranarray(rng.standard_normal((N, ncols)) + (r1 % 11)[:, None] * 0.3)
+    R_o, _, _ = oracle.solve_residuals_cols(Y, refs, None, inter, w, tol=1e-8)
+    fes = [fe.FixedEffect(r, interaction=a) for r, a in zip(refs, inter)]
+    out = []
+    for absorb in (1, 0):
+        feM = fe.AbstractFixedEffectSolver(fes, w, "CUDA", np.float64, precision="mixed")
+        feM.set_option(fe._lib.FE_OPT_ABSORB, absorb)
+        R, its, cvs = feM.solve_residuals(Y.copy(), tol=1e-8)
+        R2, its2, _ = feM.solve_residuals(Y.copy(), tol=1e-8)
+        feM.close()
+        assert cvs.all(), (absorb, its)
+        assert np.array_equal(R, R2) and np.array_equal(its, its2)
+        err = max(rel_err(R[:, j], R_o[:, j]) for j in range(ncols))
+        assert err < REL, (absorb, err)
+        out.append((R, its))
+    # the projected problem needs fewer LSMR iterations
+    assert np.sum(out[0][1]) < np.sum(out[1][1]), (out[0][1], out[1][1])
+
+
 def test_absorbed_column_stopping_at_round0(fe):
     # a zero column stops at refinement round 0 (||r0|| = 0): its residual is
     # r0 = M b = 0.  The plan first solves a nonzero column in the same slot,
