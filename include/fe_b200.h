@@ -74,9 +74,9 @@ extern "C" {
                                 convergence checks from a captured CUDA graph */
 #define FE_OPT_ROWSUM_VARIANT 12 /* row-sum pass: -1 default, 0 rows staged in shared
                                     memory (cp.async ring), 1 rows in registers */
-#define FE_OPT_ABSORB 14     /* 1 (default): FE_PREC_MIXED residual solves of 32-column
-                                tiles of single-problem plans with 2+ FEs project the
-                                primary FE out of the least-squares problem and run
+#define FE_OPT_ABSORB 14     /* 1 (default): FE_PREC_MIXED residual solves (tiles of
+                                every width) of single-problem plans with 2+ FEs project
+                                the primary FE out of the least-squares problem and run
                                 LSMR over the other FEs' levels (same residuals, fewer
                                 and cheaper iterations); 0: LSMR over all FEs */
 #define FE_OPT_FUSED_DEMEAN 15 /* 1 (default): the absorbed loop computes and projects
