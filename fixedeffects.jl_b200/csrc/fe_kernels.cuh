@@ -1326,30 +1326,71 @@ k_demean_narrow(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_i
   const T* __restrict__ scp = scale_of<T>(d, kp);
   T* zb = zs[wib];
   double nrm = 0.0;
-  const int64_t wstride = (int64_t)gridDim.x * kWarps;
-  for (int64_t wi = (int64_t)blockIdx.x * kWarps + wib; wi < n_items; wi += wstride) {
+  // Items are walked with the next one's loads in flight: its descriptor,
+  // row keys, weights and scales, and (at most 32 bytes per lane, where the
+  // registers do not cost occupancy) its rows.
+  constexpr bool PFX = KC * (int)sizeof(T) <= 32;
+  struct Pre {
+    int64_t ib, ne;  // first row; rows (0: none)
+    int kpr;
+    T cwv, sl;
+    T x[PFX ? KC : 1];
+  };
+  auto fetch = [&](int64_t wi, Pre& p) {
+    p.ib = 0;
+    p.ne = 0;
+    p.kpr = kSentinel;
+    p.cwv = T(1);
+    p.sl = T(0);
+    if (wi >= n_items) return;
     const ExpandItem it = items[wi];
-    const int64_t ib = it.ib;
-    if (it.ie <= ib) continue;
-    if (it.ie - ib <= RC) {
-      const int n = (int)(it.ie - ib);
-      const bool okl = lane < n;
-      const int kpr = okl ? __ldg(refp + ib + lane) : kSentinel;
-      const T cwv = (W && okl && cwp) ? __ldg(cwp + ib + lane) : T(1);
-      T f = T(0);  // cw scale^2 of row `lane`
-      if (okl) {
-        const T sl = __ldg(scp + kpr);
-        f = sl * sl * cwv;
-      }
-      const int kn = __shfl_down_sync(FE_FULL, kpr, 1);
-      // level ends after row r: a key change, or the item's last row
-      const uint32_t ends = __ballot_sync(FE_FULL, okl && (lane + 1 == n || kn != kpr));
-      const T* src = in + ib * C;
-      T x[KC];
+    p.ib = it.ib;
+    p.ne = it.ie > it.ib ? it.ie - it.ib : 0;
+    if (p.ne == 0 || p.ne > RC) return;
+    const int n = (int)p.ne;
+    if (lane < n) {
+      p.kpr = __ldg(refp + p.ib + lane);
+      if (W && cwp) p.cwv = __ldg(cwp + p.ib + lane);
+      p.sl = __ldg(scp + p.kpr);
+    }
+    if constexpr (PFX) {
 #pragma unroll
       for (int k = 0; k < KC; ++k) {
         const int e = lane + 32 * k;
-        x[k] = e < n * C ? src[e] : T(0);
+        p.x[k] = e < n * C ? in[p.ib * C + e] : T(0);
+      }
+    }
+  };
+  const int64_t wstride = (int64_t)gridDim.x * kWarps;
+  Pre cur, nxt;
+  int64_t wi = (int64_t)blockIdx.x * kWarps + wib;
+  fetch(wi, cur);
+  for (; wi < n_items; wi += wstride) {
+    fetch(wi + wstride, nxt);
+    const int64_t ib = cur.ib;
+    const int64_t ne = cur.ne;
+    if (ne == 0) {
+      cur = nxt;
+      continue;
+    }
+    if (ne <= RC) {
+      const int n = (int)ne;
+      const bool okl = lane < n;
+      const int kpr = cur.kpr;
+      const T cwv = cur.cwv;
+      const T f = okl ? cur.sl * cur.sl * cwv : T(0);  // cw scale^2 of row `lane`
+      const int kn = __shfl_down_sync(FE_FULL, kpr, 1);
+      // level ends after row r: a key change, or the item's last row
+      const uint32_t ends = __ballot_sync(FE_FULL, okl && (lane + 1 == n || kn != kpr));
+      T x[KC];
+#pragma unroll
+      for (int k = 0; k < KC; ++k) {
+        if constexpr (PFX) {
+          x[k] = cur.x[k];
+        } else {
+          const int e = lane + 32 * k;
+          x[k] = e < n * C ? in[ib * C + e] : T(0);
+        }
       }
       T carry = T(0);   // the partial of the level open at the previous chunk's end
       int carry_lv = -1;
@@ -1386,25 +1427,27 @@ k_demean_narrow(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_i
         }
       }
       __syncwarp();  // zb is rewritten by the next item
+      cur = nxt;
       continue;
     }
     // one level longer than RC rows: z per column over the whole level
     const T sl = __ldg(scp + __ldg(refp + ib));
-    const int64_t ne = (it.ie - ib) * C;
+    const int64_t nel = ne * C;
     T acc = T(0);
-    for (int64_t e = lane; e < ne; e += 32) {
+    for (int64_t e = lane; e < nel; e += 32) {
       const T v = in[ib * C + e];
       acc += (W && cwp) ? __ldg(cwp + ib + e / C) * v : v;
     }
 #pragma unroll
     for (int o = C; o < 32; o <<= 1) acc += __shfl_xor_sync(FE_FULL, acc, o);
-    for (int64_t e = lane; e < ne; e += 32) {
+    for (int64_t e = lane; e < nel; e += 32) {
       const T cr = (W && cwp) ? __ldg(cwp + ib + e / C) : T(1);
       const T u = in[ib * C + e] - sl * sl * cr * acc;
       if (rows) rows[ib * C + e] = u;
       if (rows32) rows32[ib * C + e] = (float)u;
       nrm += (double)u * (double)u;
     }
+    cur = nxt;
   }
   // ||u||^2 per column: the lanes of a column, then warps in order -> the
   // CTA's slot (slots beyond the grid hold 0)
