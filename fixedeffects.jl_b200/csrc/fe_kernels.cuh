@@ -1314,7 +1314,15 @@ k_demean_narrow(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_i
   static_assert(RC == 32, "one item row per lane for the keys");
   constexpr int KC = RC * C / 32;  // chunks of 32 elements in a short item
   constexpr int RPC = 32 / C;      // rows per chunk
-  __shared__ T zs[kWarps][RC * C];  // level sums z (level, column)
+  // FP32 with C >= 4 (TASKS): the item's rows, their weights and the level
+  // sums z in shared memory; each lane sums the rows of one (level, column)
+  // pair (measured at 8 columns: 2.69 -> 2.13 ms per launch on 100M rows).
+  // Otherwise z from per-column segmented scans over the lanes (at 1 column
+  // the pairs are too few to occupy the warp: 93 us against 115 us).
+  constexpr bool TASKS = sizeof(T) == 4 && C >= 4;
+  constexpr int WSH = TASKS ? 2 * RC * C + RC : RC * C;  // elements per warp
+  __shared__ T wsh[kWarps][WSH];
+  __shared__ int lends[kWarps][TASKS ? RC : 1];  // last row of each level
   __shared__ double sm[kWarps][32];
   if (d.active_pre && *d.active_pre == 0) return;  // the whole CTA
   const int lane = threadIdx.x & 31;
@@ -1324,7 +1332,9 @@ k_demean_narrow(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_i
   const int32_t* __restrict__ refp = d.refs[kp];
   const T* __restrict__ cwp = cw_of<T>(d, kp);
   const T* __restrict__ scp = scale_of<T>(d, kp);
-  T* zb = zs[wib];
+  T* zb = wsh[wib];                          // z (level, column)
+  T* bx = TASKS ? wsh[wib] + RC * C : nullptr;   // staged rows
+  T* cws = TASKS ? wsh[wib] + 2 * RC * C : nullptr;  // staged row weights
   double nrm = 0.0;
   // Items are walked with the next one's loads in flight: its descriptor,
   // row keys, weights and scales, and (at most 32 bytes per lane, where the
@@ -1392,11 +1402,29 @@ k_demean_narrow(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_i
           x[k] = e < n * C ? in[ib * C + e] : T(0);
         }
       }
+      if constexpr (TASKS) {
+        // level sums: lane t takes (level t / C, column t % C) and sums the
+        // level's rows of its column in row order
+#pragma unroll
+        for (int k = 0; k < KC; ++k) bx[lane + 32 * k] = x[k];
+        if (W) cws[lane] = cwv;
+        const int nlev = __popc(ends);
+        if (okl && ((ends >> lane) & 1u)) lends[wib][__popc(ends & ((1u << lane) - 1u))] = lane;
+        __syncwarp();
+        for (int t = lane; t < nlev * C; t += 32) {
+          const int j = t / C, c = t - j * C;
+          const int r1 = lends[wib][j];
+          T acc = T(0);
+          for (int r = j > 0 ? lends[wib][j - 1] + 1 : 0; r <= r1; ++r)
+            acc += W ? cws[r] * bx[r * C + c] : bx[r * C + c];
+          zb[j * C + c] = acc;
+        }
+      }
       T carry = T(0);   // the partial of the level open at the previous chunk's end
       int carry_lv = -1;
 #pragma unroll
       for (int k = 0; k < KC; ++k) {
-        if (RPC * k >= n) break;  // warp-uniform
+        if (TASKS || RPC * k >= n) break;  // warp-uniform
         const int r = (lane + 32 * k) / C;
         const int lv = __popc(ends & ((1u << r) - 1u));
         const T cr = W ? __shfl_sync(FE_FULL, cwv, r) : T(1);
