@@ -90,6 +90,29 @@ __global__ void __launch_bounds__(256) k_load(const TY* __restrict__ Y, int64_t 
   }
 }
 
+// The same for tiles of 1 or 2 columns, whose sorted rows are shorter than a
+// 32-byte sector: gathered through the inverse permutation (src: sorted
+// position -> observation; sw_sorted: sqrt(w) in sorted order), so the rows
+// are written whole and in order and the random reads of y fall in L2,
+// instead of scattering partial-sector writes.
+template <typename TY, int C, bool W>
+__global__ void __launch_bounds__(256) k_load_gather(const TY* __restrict__ Y, int64_t ld,
+                                                     int64_t col0, int ncols,
+                                                     const int32_t* __restrict__ src,
+                                                     const double* __restrict__ sw_sorted,
+                                                     double* __restrict__ B, int64_t N) {
+  static_assert(C <= 2, "narrow rows");
+  const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= N) return;
+  const int64_t i = src[q];
+  const double s = W ? sw_sorted[q] : 1.0;
+#pragma unroll
+  for (int j = 0; j < C; ++j) {
+    const double x = j < ncols ? (double)Y[i + (col0 + j) * ld] : 0.0;
+    B[q * C + j] = W ? x * s : x;
+  }
+}
+
 // y[i][col0 + j] = R[q][j] / sqrt(w_i)  (src/AbstractFixedEffectSolver.jl:62-66):
 // whole rows in (all of a thread's row loads issued before the first
 // shared-memory store), coalesced columns out.
@@ -1145,6 +1168,12 @@ static int prepare(fe_plan* pl, int C, int sT, bool mixed, Ctx& c) {
 
 template <int C, typename TY, bool W>
 static void launch_load(const fe_plan* pl, Ctx& c, const SolveReq& rq, int64_t col0, int ncols) {
+  if constexpr (C <= 2) {
+    k_load_gather<TY, C, W><<<grid1(pl->N), 256, 0, c.s>>>(
+        (const TY*)rq.Y, rq.ld, col0, ncols, pl->d_obs_src.as<int32_t>(),
+        W ? pl->d_sw_sorted.as<double>() : nullptr, pl->ws.B64.as<double>(), pl->N);
+    return;
+  }
   k_load<TY, C, W><<<grid1(pl->N, load_rows<C>()), 256, 0, c.s>>>(
       (const TY*)rq.Y, rq.ld, col0, ncols, pl->d_obs_dst.as<int32_t>(),
       W ? pl->d_sw_orig.as<double>() : nullptr, pl->ws.B64.as<double>(), pl->N);
