@@ -1303,12 +1303,16 @@ k_demean(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_items, c
 // in a second pass over memory.  ||u||^2 per column goes to the CTA's norm
 // slot.  `in` is the source (== rows for the in-place projection); rows
 // (optional) and rows32 (optional FP32 copy) receive u.
+// ipc == 0: the CTAs walk all items grid-stride (one problem).  ipc > 0 (batch
+// plans): CTA b takes items [b ipc, (b+1) ipc), all of one problem, and skips
+// the items of a problem none of whose columns is active (act_mode 1: the
+// inner loop's flag, 2: the refinement's); its rows are left as they are.
 // ---------------------------------------------------------------------------
 template <typename T, int C, bool W>
 __global__ void __launch_bounds__(kThreads)
 k_demean_narrow(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_items,
                 const T* in, T* rows, float* __restrict__ rows32, double* __restrict__ part,
-                int64_t S) {
+                int64_t S, int64_t ipc, const Inst* __restrict__ inst, int act_mode) {
   static_assert(C < 32 && 32 % C == 0, "tiles narrower than a warp");
   constexpr int RC = (int)kDemeanRows;
   static_assert(RC == 32, "one item row per lane for the keys");
@@ -1346,16 +1350,24 @@ k_demean_narrow(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_i
     T cwv, sl;
     T x[PFX ? KC : 1];
   };
+  const int64_t wstride = ipc > 0 ? (int64_t)kWarps : (int64_t)gridDim.x * kWarps;
+  int64_t wi = ipc > 0 ? (int64_t)blockIdx.x * ipc + wib : (int64_t)blockIdx.x * kWarps + wib;
+  const int64_t cta_end = ((int64_t)blockIdx.x + 1) * ipc;
+  const int64_t wend = (ipc > 0 && cta_end < n_items) ? cta_end : n_items;
   auto fetch = [&](int64_t wi, Pre& p) {
     p.ib = 0;
     p.ne = 0;
     p.kpr = kSentinel;
     p.cwv = T(1);
     p.sl = T(0);
-    if (wi >= n_items) return;
+    if (wi >= wend) return;
     const ExpandItem it = items[wi];
     p.ib = it.ib;
     p.ne = it.ie > it.ib ? it.ie - it.ib : 0;
+    if (inst != nullptr && p.ne > 0) {
+      const Inst& s = inst[(int64_t)it.prob * C + col];
+      if (!__any_sync(FE_FULL, (act_mode == 1 ? s.active : s.outer_active) != 0)) p.ne = 0;
+    }
     if (p.ne == 0 || p.ne > RC) return;
     const int n = (int)p.ne;
     if (lane < n) {
@@ -1371,11 +1383,9 @@ k_demean_narrow(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_i
       }
     }
   };
-  const int64_t wstride = (int64_t)gridDim.x * kWarps;
   Pre cur, nxt;
-  int64_t wi = (int64_t)blockIdx.x * kWarps + wib;
   fetch(wi, cur);
-  for (; wi < n_items; wi += wstride) {
+  for (; wi < wend; wi += wstride) {
     fetch(wi + wstride, nxt);
     const int64_t ib = cur.ib;
     const int64_t ne = cur.ne;

@@ -314,6 +314,11 @@ int plan_build(fe_plan* pl, int32_t nprob, const int64_t* n_obs, int32_t K,
   pl->primary = 0;
   for (int k = 1; k < K; ++k)
     if (pl->nlev[k] > pl->nlev[pl->primary]) pl->primary = k;
+  pl->absorbable = K >= 2;
+  if (nprob > 1)
+    for (int p = 0; p < nprob && pl->absorbable; ++p)
+      if (n_obs[p] > 0 && (n_levels[(int64_t)p * K + pl->primary] == 0 || pl->prob_nfe[p] < 2))
+        pl->absorbable = false;
 
   FE_CK(cudaSetDevice(device));
   if (!pl->stream) {
@@ -457,10 +462,11 @@ int plan_update_weights(fe_plan* pl, const double* weights) {
                                                            epi, nullptr, nullptr, 0);
     FE_CK(cudaGetLastError());
   }
-  // the absorbed operator's column scales (single-problem plans, 2+ FEs)
+  // the absorbed operator's column scales (plans whose primary FE can be
+  // projected out; a batch's levels belong to one problem each)
   pl->d_abs_scale_d.resize(K);
   pl->d_abs_scale_f.resize(K);
-  if (pl->nprob == 1 && K >= 2 && N > 0) {
+  if (pl->absorbable && N > 0) {
     const int kp = pl->primary;
     DevBuf pcs, first;
     std::vector<AbsPiece> hp;
@@ -551,13 +557,13 @@ int plan_items(fe_plan* pl, int C, ItemSet** out) {
   const int64_t Tp = item_size(total_rows);
   // the non-primary FEs' levels alone (the absorbed loop's P side) are sized
   // on their own count, so that their items fill the GPU in whole waves
-  const int64_t Tp_np =
-      item_size(total_rows - (pl->nprob == 1 ? pl->nlev[pl->primary] : 0));
+  const int64_t Tp_np = item_size(total_rows - (pl->absorbable ? pl->nlev[pl->primary] : 0));
 
   const int nprob = pl->nprob;
   const int K = pl->K;
   its->ex_slot_off.assign((size_t)nprob + 1, 0);
   its->pu_slot_off.assign((size_t)nprob + 1, 0);
+  its->pu_abs_slot_off.assign(1, 0);
   std::vector<ReduceItem> rd_prim, rd_small;
   const int kp = pl->primary;
   its->sms = sms;
@@ -653,6 +659,20 @@ int plan_items(fe_plan* pl, int C, ItemSet** out) {
       pu_fe(kp, Tp);
     } else {
       for (int k = 0; k < K; ++k) pu_fe(k, Tp);
+      if (pl->absorbable && C < 32) {
+        // the absorbed loop's P side: the problem's non-primary levels
+        const size_t a0 = its->pu_abs.size();
+        for (int k = 0; k < K; ++k) {
+          if (k == kp) continue;
+          const int64_t rb = pl->lev_base[k] + pl->prob_lev_off[(size_t)p * K + k];
+          const int64_t re = pl->lev_base[k] + pl->prob_lev_off[(size_t)(p + 1) * K + k];
+          for (int64_t b = rb; b < re; b += Tp_np) its->pu_abs.push_back({b, std::min(re, b + Tp_np), k, p});
+        }
+        while ((its->pu_abs.size() - a0) % kWarps) its->pu_abs.push_back({0, 0, 0, p});
+        if (its->pu_abs.size() == a0)
+          for (int w = 0; w < kWarps; ++w) its->pu_abs.push_back({0, 0, 0, p});
+        its->pu_abs_slot_off.push_back((int64_t)(its->pu_abs.size() / kWarps));
+      }
     }
     while ((its->pu.size() - q0) % kWarps) its->pu.push_back({0, 0, 0, p});
     if (its->pu.size() == q0)
@@ -725,6 +745,39 @@ int plan_items(fe_plan* pl, int C, ItemSet** out) {
       cur_e = e;
     }
     if (cur_b >= 0) its->dm.push_back({cur_b, cur_e, 0, -1, 0, 0});
+  } else if (pl->absorbable && C < 32) {
+    // batch plans: each problem's primary levels (its rows are one contiguous
+    // range, in level order) packed alike, padded to whole CTAs of kDemeanIpc
+    // items, so that each CTA's norm slot belongs to one problem
+    its->dm_ipc = kDemeanIpc;
+    its->dm_slot_off.assign((size_t)nprob + 1, 0);
+    const std::vector<int64_t>& off = pl->seg_off[kp];
+    for (int p = 0; p < nprob; ++p) {
+      const size_t d0 = its->dm.size();
+      const int64_t o0 = pl->prob_obs_off[p], o1 = pl->prob_obs_off[p + 1];
+      const int64_t plb = pl->prob_lev_off[(size_t)p * K + kp];
+      const int64_t ple = pl->prob_lev_off[(size_t)(p + 1) * K + kp];
+      if (o1 > o0 && ple > plb) {
+        const int64_t base = o0 - off[(size_t)plb];  // sorted row of level-order position
+        int64_t cur_b = -1, cur_e = -1;
+        for (int64_t l = plb; l < ple; ++l) {
+          const int64_t b = off[(size_t)l] + base, e = off[(size_t)l + 1] + base;
+          if (e == b) continue;
+          if (cur_b >= 0 && e - cur_b > kDemeanRows) {
+            its->dm.push_back({cur_b, cur_e, p, -1, 0, 0});
+            cur_b = -1;
+          }
+          if (cur_b < 0) cur_b = b;
+          cur_e = e;
+        }
+        if (cur_b >= 0) its->dm.push_back({cur_b, cur_e, p, -1, 0, 0});
+      }
+      while ((its->dm.size() - d0) % kDemeanIpc) its->dm.push_back({o1, o1, p, -1, 0, 0});
+      if (its->dm.size() == d0)
+        for (int64_t q = 0; q < kDemeanIpc; ++q) its->dm.push_back({o1, o1, p, -1, 0, 0});
+      its->dm_slot_off[(size_t)p + 1] = (int64_t)(its->dm.size() / kDemeanIpc);
+    }
+    its->Sdm = its->dm_slot_off[(size_t)nprob];
   }
   its->rd_large = (int64_t)its->rd.size();
   its->rd.insert(its->rd.end(), rd_small.begin(), rd_small.end());
@@ -744,9 +797,19 @@ int plan_items(fe_plan* pl, int C, ItemSet** out) {
   if (!st) st = upload(its->d_pu, its->pu.data(), its->pu.size(), s);
   if (!st) st = upload(its->d_ex_off, its->ex_slot_off.data(), its->ex_slot_off.size(), s);
   if (!st) st = upload(its->d_pu_off, its->pu_slot_off.data(), its->pu_slot_off.size(), s);
-  its->Sp_np = its->pu_np / kWarps;
-  const int64_t off_np[2] = {0, its->Sp_np};
-  if (!st) st = upload(its->d_pu_off_np, off_np, 2, s);
+  if (its->dm_ipc == 0) {
+    // single problem: the absorbed loop's P side is the leading items
+    its->Sp_np = its->pu_np / kWarps;
+    const int64_t off_np[2] = {0, its->Sp_np};
+    if (!st) st = upload(its->d_pu_off_np, off_np, 2, s);
+  } else {
+    // batch plans: its own list, per-problem P-side and demean slots
+    its->pu_np = (int64_t)its->pu_abs.size();
+    its->Sp_np = its->pu_np / kWarps;
+    if (!st) st = upload(its->d_pu_abs, its->pu_abs.data(), its->pu_abs.size(), s);
+    if (!st) st = upload(its->d_pu_off_np, its->pu_abs_slot_off.data(), its->pu_abs_slot_off.size(), s);
+    if (!st) st = upload(its->d_dm_off, its->dm_slot_off.data(), its->dm_slot_off.size(), s);
+  }
   if (!st) st = upload(its->d_dm, its->dm.data(), its->dm.size(), s);
   if (!st) st = upload(its->d_ex_splits, its->ex_splits.data(), its->ex_splits.size(), s);
   const size_t nsc = std::max<size_t>(its->splits.size(), 1) * 4;

@@ -107,6 +107,14 @@ struct ItemSet {
   int64_t pu_np = 0;                   // leading P-side items of the non-primary FEs
   int64_t Sp_np = 0;                   // their norm slots
   std::vector<ExpandItem> dm;          // demean items (absorbed-primary mode)
+  // batch plans (absorbed mode on narrow tiles): demean items padded per
+  // problem to whole CTAs of dm_ipc items, one norm slot per CTA; the P-side
+  // items of the non-primary FEs as a list of their own, padded likewise
+  int64_t dm_ipc = 0;                  // 0: single problem, grid-stride walk
+  int64_t Sdm = 0;                     // demean norm slots (batch plans)
+  std::vector<int64_t> dm_slot_off;    // per problem (batch plans)
+  std::vector<PItem> pu_abs;           // batch plans' non-primary P-side items
+  std::vector<int64_t> pu_abs_slot_off;
   std::vector<int64_t> ex_slot_off;       // per problem, expand norm slots (CTAs)
   std::vector<int64_t> pu_slot_off;       // per problem, P-side norm slots (CTAs)
   int64_t n_pieces = 0, n_blocks = 0;
@@ -115,6 +123,7 @@ struct ItemSet {
   DevBuf d_ex, d_rd, d_splits, d_pu, d_ex_off, d_pu_off, d_split_cnt, d_block_cnt;
   DevBuf d_ex_splits, d_ex_split_cnt, d_ex_block_cnt;
   DevBuf d_pu_off_np, d_dm;
+  DevBuf d_dm_off, d_pu_abs;
 };
 
 struct Workspace {
@@ -156,6 +165,9 @@ struct fe_plan {
   int32_t K = 0;
   int32_t nprob = 1;
   int32_t primary = 0;
+  // the primary FE can be projected out of every problem: one problem with
+  // 2+ FEs, or a batch whose problems all hold the primary FE and another
+  bool absorbable = false;
   bool weighted = false;
   std::vector<bool> interacted;
   std::vector<int64_t> nlev;           // per FE: total levels over problems

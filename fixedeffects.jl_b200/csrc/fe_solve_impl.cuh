@@ -524,10 +524,22 @@ static int demean_launch(Ctx& c, const T* in, T* rows, float* rows32, T* out,
       FE_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, k_demean_narrow<T, C, W>, kThreads, 0));
       occ = std::max(o, 1);
     }
+    if (c.its->dm_ipc > 0) {
+      // batch plans: one CTA per kDemeanIpc items of one problem, one norm slot
+      // each; the problems whose columns have stopped are skipped (the inner
+      // loop's FP32 pass: its flag; the refinement's FP64 pass: the outer flag)
+      const int act_mode = sizeof(T) == 4 ? 1 : 2;
+      k_demean_narrow<T, C, W><<<(unsigned)c.its->Sdm, kThreads, 0, c.s>>>(
+          c.d, c.its->d_dm.as<ExpandItem>(), n, in, rows, rows32, c.part_e, c.its->Sdm,
+          c.its->dm_ipc, c.inst, act_mode);
+      FE_CK(cudaGetLastError());
+      return 0;
+    }
     const int64_t grid =
         std::max<int64_t>(1, std::min<int64_t>(c.its->Se, (int64_t)occ * c.its->sms));
     k_demean_narrow<T, C, W><<<(unsigned)grid, kThreads, 0, c.s>>>(
-        c.d, c.its->d_dm.as<ExpandItem>(), n, in, rows, rows32, c.part_e, c.its->Se);
+        c.d, c.its->d_dm.as<ExpandItem>(), n, in, rows, rows32, c.part_e, c.its->Se, 0, nullptr,
+        0);
     FE_CK(cudaGetLastError());
     return 0;
   } else {
@@ -923,10 +935,13 @@ static int launch_pupdate(Ctx& c, const typename Epi::TS* S, Epi epi, double* pa
                           const char* name, double bytes) {
   ProfScope ps(c.pl, name, bytes);
   // absorbed-primary mode: the non-primary levels only (the leading items)
+  // (batch plans: a list of their own, per problem)
   const int64_t n = c.absorb ? c.its->pu_np : (int64_t)c.its->pu.size();
   const unsigned grid = (unsigned)(n / kWarps);
+  const PItem* items = (c.absorb && c.its->dm_ipc > 0) ? c.its->d_pu_abs.as<PItem>()
+                                                       : c.its->d_pu.as<PItem>();
   k_pupdate<C, Tune<C>::kPU, Epi><<<grid, kThreads, 0, c.s>>>(
-      c.d, c.its->d_pu.as<PItem>(), n, S, epi, pa, pb, c.absorb ? c.its->Sp_np : c.its->Sp);
+      c.d, items, n, S, epi, pa, pb, c.absorb ? c.its->Sp_np : c.its->Sp);
   FE_CK(cudaGetLastError());
   return 0;
 }
@@ -940,8 +955,11 @@ static int launch_scalar_phase(Ctx& c, int phase, int init_mode) {
   a.phase = phase;
   a.init_mode = init_mode;
   a.counters = c.counters;
-  a.off0 = c.its->d_ex_off.as<int64_t>();
-  a.S0 = c.its->Se;
+  // the absorbed mode's norms of u come from the demean pass: per-problem
+  // slots of their own in batch plans
+  const bool dm_slots = c.absorb && c.its->dm_ipc > 0;
+  a.off0 = dm_slots ? c.its->d_dm_off.as<int64_t>() : c.its->d_ex_off.as<int64_t>();
+  a.S0 = dm_slots ? c.its->Sdm : c.its->Se;
   a.off1 = c.absorb ? c.its->d_pu_off_np.as<int64_t>() : c.its->d_pu_off.as<int64_t>();
   a.S1 = c.absorb ? c.its->Sp_np : c.its->Sp;
   switch (phase) {
@@ -987,15 +1005,18 @@ static bool use_rowsum(const fe_plan* pl, int C) {
   return pl->opt_fuse != 0 && C == 32 && pl->nprob == 1;
 }
 
-// Absorbed-primary mode of the mixed-precision residual solve (32-column
-// tiles of single-problem plans with 2+ FEs): the least-squares residual is
+// Absorbed-primary mode of the mixed-precision residual solve (plans with 2+
+// FEs, and batches whose problems all hold the primary FE and another): the
+// least-squares residual is
 // that of the problem with the primary FE projected out,
 //   min || M (b - A_r x_r) ||,  M u = u - sum_l a_l (a_l' u),
 // a_l the unit columns of the primary FE (contiguous row segments).  LSMR then
 // iterates over the other FEs' levels only, on a better-conditioned operator.
 static bool use_absorb(const fe_plan* pl, const ItemSet* its, int C) {
-  (void)C;  // tiles of every width: k_demean (32 columns) or k_demean_narrow
-  return pl->opt_absorb != 0 && pl->nprob == 1 && pl->K >= 2 && !its->dm.empty();
+  // tiles of every width: k_demean (32 columns) or k_demean_narrow; batch
+  // plans have demean items on narrow tiles only
+  (void)C;
+  return pl->opt_absorb != 0 && pl->absorbable && !its->dm.empty();
 }
 
 // algorithmic bytes per launch (the roofline numerators): every index vector
@@ -1108,9 +1129,12 @@ static int prepare(fe_plan* pl, int C, int sT, bool mixed, Ctx& c) {
   if ((st = w.X.ensure(P * nC * (size_t)sT))) return st;
   if (mixed && (st = w.X64.ensure(P * nC * 8))) return st;
   if (mixed && (st = w.XS64.ensure(P * nC * 8))) return st;
-  if ((st = w.part_e.ensure((size_t)std::max<int64_t>(its->Se, 1) * nC * 8))) return st;
-  if ((st = w.part_a.ensure((size_t)std::max<int64_t>(its->Sp, 1) * nC * 8))) return st;
-  if ((st = w.part_b.ensure((size_t)std::max<int64_t>(its->Sp, 1) * nC * 8))) return st;
+  if ((st = w.part_e.ensure((size_t)std::max<int64_t>(std::max(its->Se, its->Sdm), 1) * nC * 8)))
+    return st;
+  // (a batch plan's absorbed P-side list can hold more slots than the full one)
+  const int64_t sp = std::max<int64_t>(std::max(its->Sp, its->Sp_np), 1);
+  if ((st = w.part_a.ensure((size_t)sp * nC * 8))) return st;
+  if ((st = w.part_b.ensure((size_t)sp * nC * 8))) return st;
   if ((st = w.S.ensure(P * nC * 8))) return st;
   if ((st = w.piece_part.ensure((size_t)std::max<int64_t>(its->n_pieces, 1) * nC * 8))) return st;
   if ((st = w.ex_piece_part.ensure((size_t)std::max<int64_t>(its->ex_n_pieces, 1) * nC * 8))) return st;

@@ -75,10 +75,12 @@ extern "C" {
 #define FE_OPT_ROWSUM_VARIANT 12 /* row-sum pass: -1 default, 0 rows staged in shared
                                     memory (cp.async ring), 1 rows in registers */
 #define FE_OPT_ABSORB 14     /* 1 (default): FE_PREC_MIXED residual solves (tiles of
-                                every width) of single-problem plans with 2+ FEs project
-                                the primary FE out of the least-squares problem and run
-                                LSMR over the other FEs' levels (same residuals, fewer
-                                and cheaper iterations); 0: LSMR over all FEs */
+                                every width) of single-problem plans with 2+ FEs, and of
+                                batch plans whose problems all hold the primary FE and
+                                another (tiles narrower than 32 columns), project the
+                                primary FE out of the least-squares problem and run LSMR
+                                over the other FEs' levels (same residuals, fewer and
+                                cheaper iterations); 0: LSMR over all FEs */
 #define FE_OPT_FUSED_DEMEAN 15 /* 1 (default): the absorbed loop computes and projects
                                   the rows in one kernel; 0: expand, then demean */
 #define FE_OPT_ABSORB_SCALE 16 /* 1 (default): the absorbed LSMR scales the other FEs'

@@ -488,6 +488,80 @@ def test_absorbed_narrow_tiles(fe, oracle, ncols, weighted):
     assert np.sum(out[0][1]) < np.sum(out[1][1]), (out[0][1], out[1][1])
 
 
+@pytest.mark.parametrize("weighted", [False, True])
+def test_batch_absorbed_vs_oracle(fe, oracle, weighted):
+    # batch plans project each problem's primary FE out (demean items and norm
+    # slots per problem, k_demean_narrow): against the oracle, against the
+    # full-LSMR batch (FE_OPT_ABSORB = 0) and bitwise across two calls.  The
+    # problems stop at different iterations, so the passes skip stopped
+    # problems, whose rows must stay as they were.
+    rng = np.random.default_rng(37 + int(weighted))
+    probs = []
+    for p in range(10):
+        n = int(rng.integers(300, 20_000))
+        r1 = rng.integers(1, max(3, n // 8) + 1, n)
+        if p == 3:
+            r1[rng.random(n) < 0.2] = 1  # a primary level longer than a demean item
+        raw = [r1, rng.integers(1, 41, n)]
+        inter = [None, None]
+        if p % 2:
+            raw.append(rng.integers(1, 301, n))
+            inter.append(rng.uniform(0.5, 1.5, n) if weighted else None)
+        refs = [np.unique(r, return_inverse=True)[1].astype(np.int64) + 1 for r in raw]
+        w = rng.uniform(0.5, 1.5, n) if weighted else None
+        y = rng.standard_normal(n) + (r1 % 7) * 0.4 + (raw[1] % 5) * 0.3
+        probs.append((refs, inter, w, y))
+    ref = [oracle.solve_residuals(y, refs, None, inter, w, tol=1e-8)[0] for refs, inter, w, y in probs]
+    fes_list = [[fe.FixedEffect(r, interaction=a) for r, a in zip(refs, inter)]
+                for refs, inter, _, _ in probs]
+    ws = [w for _, _, w, _ in probs] if weighted else None
+    iters = []
+    for absorb in (1, 0):
+        bs = fe.BatchSolver(fes_list, ws, precision="mixed")
+        bs.set_option(fe._lib.FE_OPT_ABSORB, absorb)
+        bs.set_option(fe._lib.FE_OPT_PROFILE, 1)
+        outs, its, cvs = bs.solve_residuals([y for *_, y in probs], tol=1e-8, maxiter=10000)
+        ran_demean = "demean" in bs.kernel_stats()
+        bs.set_option(fe._lib.FE_OPT_PROFILE, 0)
+        outs2, its2, _ = bs.solve_residuals([y for *_, y in probs], tol=1e-8, maxiter=10000)
+        bs.close()
+        assert ran_demean == (absorb == 1)
+        assert cvs.all(), (absorb, its)
+        assert np.array_equal(its, its2)
+        for r, r2 in zip(outs, outs2):
+            assert np.array_equal(r, r2)
+        for (refs, inter, w, y), r, ro in zip(probs, outs, ref):
+            err = np.linalg.norm(r - ro)
+            assert err <= REL * np.linalg.norm(ro) + REL * np.linalg.norm(y), (absorb, err)
+        iters.append(np.asarray(its))
+    # the projected problems need fewer LSMR iterations in all
+    assert iters[0].sum() < iters[1].sum(), iters
+
+
+def test_batch_without_primary_everywhere_is_not_absorbed(fe, oracle):
+    # slot 1 has the most levels (the primary FE); problem 2 holds only slot 0,
+    # so its rows have no primary level to project out and the whole batch
+    # keeps the full LSMR
+    rng = np.random.default_rng(43)
+    probs = []
+    for p in range(4):
+        n = int(rng.integers(2_000, 6_000))
+        r0 = rng.integers(1, 31, n)
+        refs = [r0] if p == 2 else [r0, rng.integers(1, n // 5 + 1, n)]
+        refs = [np.unique(r, return_inverse=True)[1].astype(np.int64) + 1 for r in refs]
+        probs.append((refs, rng.standard_normal(n) + (r0 % 3)))
+    fes_list = [[fe.FixedEffect(r) for r in refs] for refs, _ in probs]
+    bs = fe.BatchSolver(fes_list, precision="mixed")
+    bs.set_option(fe._lib.FE_OPT_PROFILE, 1)
+    outs, its, cvs = bs.solve_residuals([y for _, y in probs], tol=1e-8, maxiter=10000)
+    assert "demean" not in bs.kernel_stats()
+    bs.close()
+    assert cvs.all()
+    for (refs, y), r in zip(probs, outs):
+        ro = oracle.solve_residuals(y, refs, None, None, None, tol=1e-8)[0]
+        assert np.linalg.norm(r - ro) <= REL * np.linalg.norm(ro) + REL * np.linalg.norm(y)
+
+
 def test_absorbed_column_stopping_at_round0(fe):
     # a zero column stops at refinement round 0 (||r0|| = 0): its residual is
     # r0 = M b = 0.  The plan first solves a nonzero column in the same slot,
