@@ -1303,12 +1303,14 @@ k_demean(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_items, c
 // in a second pass over memory.  ||u||^2 per column goes to the CTA's norm
 // slot.  `in` is the source (== rows for the in-place projection); rows
 // (optional) and rows32 (optional FP32 copy) receive u.
-// ipc == 0: the CTAs walk all items grid-stride (one problem).  ipc > 0 (batch
-// plans): CTA b takes items [b ipc, (b+1) ipc), all of one problem, and skips
-// the items of a problem none of whose columns is active (act_mode 1: the
-// inner loop's flag, 2: the refinement's); its rows are left as they are.
+// BATCH = false: the CTAs walk all items grid-stride (one problem).  BATCH
+// (batch plans): CTA b takes items [b ipc, (b+1) ipc), all of one problem, and
+// skips the items of a problem none of whose columns is active (act_mode 1:
+// the inner loop's flag, 2: the refinement's); its rows are left as they are.
+// (A compile-time switch: the batch walk costs the single-problem form
+// registers, 64 -> 116 for FP64 8-column tiles.)
 // ---------------------------------------------------------------------------
-template <typename T, int C, bool W>
+template <typename T, int C, bool W, bool BATCH = false>
 __global__ void __launch_bounds__(kThreads)
 k_demean_narrow(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_items,
                 const T* in, T* rows, float* __restrict__ rows32, double* __restrict__ part,
@@ -1350,10 +1352,10 @@ k_demean_narrow(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_i
     T cwv, sl;
     T x[PFX ? KC : 1];
   };
-  const int64_t wstride = ipc > 0 ? (int64_t)kWarps : (int64_t)gridDim.x * kWarps;
-  int64_t wi = ipc > 0 ? (int64_t)blockIdx.x * ipc + wib : (int64_t)blockIdx.x * kWarps + wib;
+  const int64_t wstride = BATCH ? (int64_t)kWarps : (int64_t)gridDim.x * kWarps;
+  int64_t wi = BATCH ? (int64_t)blockIdx.x * ipc + wib : (int64_t)blockIdx.x * kWarps + wib;
   const int64_t cta_end = ((int64_t)blockIdx.x + 1) * ipc;
-  const int64_t wend = (ipc > 0 && cta_end < n_items) ? cta_end : n_items;
+  const int64_t wend = (BATCH && cta_end < n_items) ? cta_end : n_items;
   auto fetch = [&](int64_t wi, Pre& p) {
     p.ib = 0;
     p.ne = 0;
@@ -1364,7 +1366,7 @@ k_demean_narrow(const FeDev d, const ExpandItem* __restrict__ items, int64_t n_i
     const ExpandItem it = items[wi];
     p.ib = it.ib;
     p.ne = it.ie > it.ib ? it.ie - it.ib : 0;
-    if (inst != nullptr && p.ne > 0) {
+    if (BATCH && p.ne > 0) {
       const Inst& s = inst[(int64_t)it.prob * C + col];
       if (!__any_sync(FE_FULL, (act_mode == 1 ? s.active : s.outer_active) != 0)) p.ne = 0;
     }

@@ -518,22 +518,22 @@ static int demean_launch(Ctx& c, const T* in, T* rows, float* rows32, T* out,
     (void)out;
     (void)xs;
     const int64_t n = (int64_t)c.its->dm.size();
-    static int occ = 0;  // resident CTAs per SM, per instantiation
-    if (occ == 0) {
-      int o = 0;
-      FE_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, k_demean_narrow<T, C, W>, kThreads, 0));
-      occ = std::max(o, 1);
-    }
     if (c.its->dm_ipc > 0) {
       // batch plans: one CTA per kDemeanIpc items of one problem, one norm slot
       // each; the problems whose columns have stopped are skipped (the inner
       // loop's FP32 pass: its flag; the refinement's FP64 pass: the outer flag)
       const int act_mode = sizeof(T) == 4 ? 1 : 2;
-      k_demean_narrow<T, C, W><<<(unsigned)c.its->Sdm, kThreads, 0, c.s>>>(
+      k_demean_narrow<T, C, W, true><<<(unsigned)c.its->Sdm, kThreads, 0, c.s>>>(
           c.d, c.its->d_dm.as<ExpandItem>(), n, in, rows, rows32, c.part_e, c.its->Sdm,
           c.its->dm_ipc, c.inst, act_mode);
       FE_CK(cudaGetLastError());
       return 0;
+    }
+    static int occ = 0;  // resident CTAs per SM, per instantiation
+    if (occ == 0) {
+      int o = 0;
+      FE_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, k_demean_narrow<T, C, W>, kThreads, 0));
+      occ = std::max(o, 1);
     }
     const int64_t grid =
         std::max<int64_t>(1, std::min<int64_t>(c.its->Se, (int64_t)occ * c.its->sms));
