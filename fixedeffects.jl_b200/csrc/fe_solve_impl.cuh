@@ -1025,6 +1025,7 @@ struct Bytes {
   double expand, segsum, pupdate, resid64, segsum64, grad64, rowsum, rowsum64;
   // absorbed-primary mode
   double expand_abs, resid64_abs, demean, demean64, pupdate_np, grad64_np, expand_demean;
+  double segsum_abs, segsum64_abs;  // the gathered (neither primary nor small) FEs only
   double prescale64, prescale64_abs, resid_demean64, resid_dm64;
 };
 static Bytes alg_bytes(const fe_plan* pl, const ItemSet* its, int C, int sT) {
@@ -1109,6 +1110,24 @@ static Bytes alg_bytes(const fe_plan* pl, const ItemSet* its, int C, int sT) {
   b.prescale64 = P * (C * 20.0 + 8.0);
   b.segsum64 = posmeta + cwp64 + pos * C * 8.0 + (P - Pf) * C * 8.0;
   b.grad64 = P * C * (8.0 + 4.0 + 8.0 + 4.0 + 8.0);
+  {
+    // the absorbed loop's segmented sums cover the FEs that are neither the
+    // primary nor small (the same figures as above where the row-sum pass runs)
+    double posA = 0, metaA = 0, cwA = 0, cwA64 = 0, PA = 0;
+    for (int k = 0; k < pl->K; ++k) {
+      if (k == pl->primary || ((its->small_mask >> k) & 1u)) continue;
+      const double sl = (double)pl->seg_len[k];
+      posA += sl;
+      metaA += sl * (4.0 + (pl->perm_identity[k] ? 0.0 : 4.0));
+      if (pl->weighted || pl->interacted[k]) {
+        cwA += sl * sT;
+        cwA64 += sl * 8.0;
+      }
+      PA += (double)pl->nlev[k];
+    }
+    b.segsum_abs = metaA + cwA + posA * C * sT + PA * C * sT;
+    b.segsum64_abs = metaA + cwA64 + posA * C * 8.0 + PA * C * 8.0;
+  }
   return b;
 }
 
@@ -1788,7 +1807,7 @@ static int solve_mixed_tile(fe_plan* pl, const SolveReq& rq, int64_t col0, int n
         return st;
       }
       if ((st = launch_segsum<double, C>(c, LoadIn<double, double, vec_of<double, C>()>{R64}, S64,
-                                         "segsum64", by.segsum64, true, "", 0.0, true)))
+                                         "segsum64", by.segsum64_abs, true, "", 0.0, true)))
         return st;
     } else if ((st = launch_segsum<double, C>(c, LoadIn<double, double, vec_of<double, C>()>{R64}, S64,
                                               "segsum64", by.segsum64, fuse, "rowsum64", by.rowsum64))) {
@@ -1830,7 +1849,7 @@ static int solve_mixed_tile(fe_plan* pl, const SolveReq& rq, int64_t col0, int n
         if ((e = launch_scalar_phase(c, PH_BETA, 0))) return e;
         if (!c.firm_atomic &&
             (e = launch_segsum<float, C>(c, LoadIn<float, float, vec_of<float, C>()>{U}, S32, "segsum",
-                                         by.segsum, true, "", 0.0, true)))
+                                         by.segsum_abs, true, "", 0.0, true)))
           return e;
         if ((e = xchg_slab(c, S32, 4))) return e;
         if ((e = launch_pupdate<C>(c, S32, pe, c.part_a, c.part_b, "pupdate", by.pupdate_np))) return e;
