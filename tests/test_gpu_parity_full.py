@@ -101,7 +101,7 @@ def _compare_columns(name, Y, R, its, cvs, info, oracle_out, cols, prec):
     }
     if prec == "mixed":
         entry["iterations_note"] = ("mixed: LSMR iterations of all refined inner solves + 1 "
-                                    "(absorbed primary FE on 32-column tiles); no oracle counterpart")
+                                    "(absorbed primary FE); no oracle counterpart")
     _record(name, entry)
     assert all(bool(cvs[j]) for j in range(Y.shape[1])), name
     assert all(o[2] for o in oracle_out), name
