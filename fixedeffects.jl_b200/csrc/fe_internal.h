@@ -26,7 +26,7 @@ constexpr int kSentinel = 0x7fffffff;  // "no level" key
 constexpr int kSmallRows = 32;         // rows of the row-sum pass's small-FE tables
 constexpr int kRowSumSmallFE = 2;      // small FEs the row-sum pass reduces
 constexpr int64_t kDemeanRows = 32;    // rows per demean item (whole primary levels)
-constexpr int64_t kDemeanIpc = 32;     // demean items per CTA of a batch plan (4 per warp)
+constexpr int64_t kDemeanIpc = 128;    // demean items per CTA of a batch plan (16 per warp)
 
 // A contiguous range of observations (sorted order) processed by one warp.
 // Items hold whole levels of the primary FE (the FE that orders the
