@@ -15,6 +15,15 @@ configurations; the reference publishes no dataset):
   large_zipf_100m_8col                  100M obs, 10M uniform x Zipf(1.3) over 10k,
                                         weighted; 8 Float32 columns per step
 
+The reference's own benchmark problems (benchmark/run.jl:6-28), same shapes,
+numpy draws:
+
+  simple_10m                            10M obs, 100k x 100 uniform; 1 Float64 column
+  hard_800k                             800k obs, worker 400k x firm 50k, each
+                                        worker's firm near worker / 8; 1 Float64 column
+  hard_800k_interacted                  800k obs, worker and worker x U(0, 1);
+                                        1 Float64 column, maxiter 300 as there
+
 One step = one batched solve of the step's columns (or problems) to the FP64
 1e-8 stopping test in mixed precision (FP32 bulk, FP64 scalars, FP64
 iterative refinement).
@@ -63,6 +72,10 @@ WORKLOADS = {
     "three_fe_interacted_10m": 1,
     "uneven_256_problems": 3,
     "large_zipf_100m_8col": 4,
+    # the reference's own benchmark problems (benchmark/run.jl:6-28)
+    "simple_10m": 5,
+    "hard_800k": 6,
+    "hard_800k_interacted": 7,
 }
 DEFAULT_WORKLOAD = "worker_firm_year_10m_32col"
 TOL = 1e-8
@@ -228,7 +241,8 @@ def _perturb(Y, rank):
 
 
 class Columns:
-    """One problem, `ncols` columns per step (configs 0, 1, 2, 4)."""
+    """One problem, `ncols` columns per step (configs 0, 1, 2, 4 and the
+    reference's benchmark problems)."""
 
     batch = False
 
@@ -247,6 +261,7 @@ class Columns:
         self.ncols = pb.Y.shape[1]
         self.solves = self.ncols
         self.nlev = [int(n) for n in pb.nlev]
+        self.maxiter = int(pb.meta.get("maxiter") or MAXITER)
 
     def fes(self, fe):
         pb = self.pb
@@ -262,7 +277,7 @@ class Columns:
         return Y0, Yw
 
     def solve_device(self, feM, Yw):
-        _, its, cvs = feM.solve_residuals(Yw, tol=TOL, maxiter=MAXITER)
+        _, its, cvs = feM.solve_residuals(Yw, tol=TOL, maxiter=self.maxiter)
         return its, cvs
 
     def host_buffers(self, torch, pinned):
@@ -280,7 +295,7 @@ class Columns:
         A[...] = self.pb.Y
 
     def solve_host(self, feM, A):
-        feM.solve_residuals(A, tol=TOL, maxiter=MAXITER)
+        feM.solve_residuals(A, tol=TOL, maxiter=self.maxiter)
 
     def io_bytes(self):
         return self.N * self.ncols * self.pb.Y.dtype.itemsize
@@ -297,8 +312,8 @@ class Columns:
         pb = self.pb
         t = time.perf_counter()
         R, its, _ = O.solve_residuals_cols(pb.Y[:, :1].astype(np.float64), pb.refs, pb.nlev,
-                                           pb.interaction, pb.weights, tol=TOL, maxiter=MAXITER,
-                                           nthreads=nthreads)
+                                           pb.interaction, pb.weights, tol=TOL,
+                                           maxiter=self.maxiter, nthreads=nthreads)
         dt = time.perf_counter() - t
         return {"solves": 1, "seconds": dt, "iterations": [int(x) for x in its],
                 "sample": f"1 of {self.ncols} columns at full N={self.N} ({dt:.1f} s; serial "
@@ -312,7 +327,8 @@ class Columns:
         return {"workload": self.name, "N": self.N, "fixed_effects": self.nlev,
                 "weighted": self.pb.weights is not None,
                 "interacted": [a is not None for a in self.pb.interaction],
-                "columns_per_gpu": self.ncols, "input_dtype": str(self.pb.Y.dtype)}
+                "columns_per_gpu": self.ncols, "input_dtype": str(self.pb.Y.dtype),
+                "maxiter": self.maxiter}
 
 
 class Problems:

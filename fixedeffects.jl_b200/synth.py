@@ -1,4 +1,5 @@
-"""Seeded synthetic workloads with the shapes of the five solver configurations.
+"""Seeded synthetic workloads with the shapes of the five solver configurations
+and of the reference's own benchmark problems (benchmark/run.jl).
 
 The reference publishes no dataset for this path, so every workload here is
 generated: numpy PCG64, seed 0 for the CPU-runnable two-FE case and the
@@ -24,6 +25,11 @@ WORKLOADS = {
     3: "uneven_256_problems: 256 problems, N log-uniform [1e3,1e6], 2-3 FEs, weighted",
     4: "large_zipf_100m_8col: N=1e8, FEs 1e7 uniform x Zipf(1.3) over 1e4, weighted, "
        "8 Float32 columns",
+    5: "simple_10m: N=1e7, FEs 1e5 x 1e2 uniform, 1 column (the reference's benchmark)",
+    6: "hard_800k: N=8e5, worker 4e5 x firm 5e4 linked locally, 1 column (the reference's "
+       "benchmark)",
+    7: "hard_800k_interacted: N=8e5, worker and worker x uniform, 1 column, maxiter 300 "
+       "(the reference's benchmark)",
 }
 
 
@@ -160,5 +166,60 @@ def config4(scale: float = 1.0, seed: int = 4, ncols: int = 8) -> Problem:
     return Problem(list(refs), list(nlev), [None, None], w, Y, {"config": 4})
 
 
+# The reference's own benchmark problems (benchmark/run.jl:6-28), with its
+# shapes and value distributions drawn from numpy instead of Julia's RNG:
+# uniform level ids, columns uniform on [0, 1).  `maxiter` is the iteration
+# cap that benchmark/run.jl gives the solve (None: the default 10000).
+def simple_10m(scale: float = 1.0, seed: int = 5) -> Problem:
+    """N = 1e7, FEs of N/100 and 100 uniform levels (benchmark/run.jl:9-15)."""
+    rng = np.random.default_rng(seed)
+    N = _scaled(10_000_000, scale, 10)
+    K = 100
+    r1 = rng.integers(1, max(2, N // K) + 1, N)
+    r2 = rng.integers(1, K + 1, N)
+    x = rng.random(N)
+    refs, nlev = zip(*(compact(r) for r in (r1, r2)))
+    return Problem(list(refs), list(nlev), [None, None], None,
+                   np.asfortranarray(x[:, None]), {"config": 5, "maxiter": None})
+
+
+def _worker_firm_800k(rng, scale):
+    """pid uniform over M = 4e5 workers; each worker's firm is drawn from the
+    21 firms around pid / 8, clipped to 1..5e4 (benchmark/run.jl:18-25)."""
+    N = _scaled(800_000, scale, 10)
+    M = _scaled(400_000, scale)
+    O = _scaled(50_000, scale)
+    pid = rng.integers(1, M + 1, N)
+    lo = np.maximum(1, pid // 8 - 10)
+    hi = np.minimum(O, pid // 8 + 10)
+    hi = np.maximum(hi, lo)
+    fid = lo + np.floor(rng.random(N) * (hi - lo + 1)).astype(np.int64)
+    return N, pid, fid
+
+
+def hard_800k(scale: float = 1.0, seed: int = 6) -> Problem:
+    """Worker-firm FEs (4e5 x 5e4 levels, linked locally), one column
+    (benchmark/run.jl:17-25, solved at the default maxiter as :39-42)."""
+    rng = np.random.default_rng(seed)
+    N, pid, fid = _worker_firm_800k(rng, scale)
+    x = rng.random(N)
+    refs, nlev = zip(*(compact(r) for r in (pid, fid)))
+    return Problem(list(refs), list(nlev), [None, None], None,
+                   np.asfortranarray(x[:, None]), {"config": 6, "maxiter": None})
+
+
+def hard_800k_interacted(scale: float = 1.0, seed: int = 7) -> Problem:
+    """The worker FE and the worker FE interacted with a uniform variable
+    (benchmark/run.jl:26-27), maxiter = 300 as :49-52."""
+    rng = np.random.default_rng(seed)
+    N, pid, _ = _worker_firm_800k(rng, scale)
+    x = rng.random(N)
+    y = rng.random(N)
+    ref, n = compact(pid)
+    return Problem([ref, ref.copy()], [n, n], [None, y], None,
+                   np.asfortranarray(x[:, None]), {"config": 7, "maxiter": 300})
+
+
 def make(config: int, scale: float = 1.0, **kw):
-    return {0: config0, 1: config1, 2: config2, 3: config3, 4: config4}[config](scale=scale, **kw)
+    return {0: config0, 1: config1, 2: config2, 3: config3, 4: config4, 5: simple_10m,
+            6: hard_800k, 7: hard_800k_interacted}[config](scale=scale, **kw)

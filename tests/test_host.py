@@ -145,6 +145,24 @@ def test_synth_shapes(synth):
     assert p4.weights is not None and p4.Y.shape[1] == 2
 
 
+def test_reference_benchmark_shapes(synth):
+    """The problems of the reference's benchmark/run.jl:6-28: 100 levels per
+    simple-FE level on average, firms within 10 of worker / 8, and the
+    interacted case's two FEs on the same worker ids."""
+    ps = synth.simple_10m(scale=0.01)
+    assert ps.N == 100_000 and ps.nlev[1] == 100 and ps.Y.dtype == np.float64
+    assert 0.0 <= ps.Y.min() and ps.Y.max() < 1.0
+    rng = np.random.default_rng(0)
+    N, pid, fid = synth._worker_firm_800k(rng, 1.0)
+    assert N == 800_000 and pid.max() <= 400_000 and fid.min() >= 1 and fid.max() <= 50_000
+    assert np.all(np.abs(fid - pid // 8) <= 10 + 1)  # +1: clipping at firm 1
+    ph = synth.hard_800k(scale=0.01)
+    assert len(ph.refs) == 2 and ph.meta["maxiter"] is None
+    pi = synth.hard_800k_interacted(scale=0.01)
+    assert np.array_equal(pi.refs[0], pi.refs[1]) and pi.interaction[0] is None
+    assert pi.interaction[1] is not None and pi.meta["maxiter"] == 300
+
+
 def test_synth_deterministic(synth):
     a = synth.config1(scale=0.0005)
     b = synth.config1(scale=0.0005)
