@@ -217,6 +217,27 @@ def test_bench_throughput_figures():
     assert abs(t["alg_GBps"] - 8e9 / 0.01 / 1e9) < 1e-9
 
 
+@pytest.mark.parametrize("workload,maxiter", [("simple_10m", 10000), ("hard_800k_interacted", 300)])
+def test_reference_arm_line_on_the_reference_benchmark_problems(workload, maxiter):
+    """bench.py --impl reference prints one JSON line with the arm's fields on
+    the reference's benchmark problems (shrunk 100x), with the problem's own
+    iteration cap in its config."""
+    import json
+    import subprocess
+    import sys
+    r = subprocess.run([sys.executable, str(ROOT / "bench.py"), "--impl", "reference",
+                        "--workload", workload, "--scale", "0.01", "--steps", "1", "--warmup", "1"],
+                       capture_output=True, text=True, timeout=300, cwd=ROOT)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [x for x in r.stdout.splitlines() if x.startswith("{")]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    assert d["impl"] == "reference" and d["unit"] == "solves/s" and d["value"] > 0
+    assert d["config"]["workload"] == workload and d["config"]["maxiter"] == maxiter
+    assert d["cpu_baseline"]["kind"] == "port" and d["cpu_baseline"]["value"] == d["value"]
+    assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["e2e"]["d2h_bytes_per_step"] == 0
+
+
 def _entry_point_bodies():
     """(name, body) of every extern "C" entry point in the library sources."""
     csrc = Path(__file__).resolve().parent.parent / "fixedeffects.jl_b200" / "csrc"
