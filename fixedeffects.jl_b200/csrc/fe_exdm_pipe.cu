@@ -12,14 +12,22 @@ namespace {
 template <int NL, int NS, bool W, int STG, bool PG, bool ATOM = false, int WARPS = kWarps>
 int launch_one(const ExdmLaunch& a) {
   auto kern = k_exdm_pipe<NL, NS, W, STG, PG, ATOM, WARPS>;
-  static size_t attr_smem = 0;  // per instantiation: the opt-in size set so far
-  if (a.smem > attr_smem) {
-    FE_CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)a.smem));
-    // the largest shared-memory carve-out, so that the CTAs the grid counts
-    // on (up to three of 4 warps) are resident together
-    FE_CK(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
-                               (int)cudaSharedmemCarveoutMaxShared));
-    attr_smem = a.smem;
+  // per instantiation and device: the opt-in size set so far (0: none).  The
+  // size only grows; the mutex keeps two threads from setting it out of order.
+  static std::atomic<size_t> attr_smem[kDeviceSlots];
+  static std::mutex attr_mu;
+  const int dev = current_device();
+  const bool slot = dev >= 0 && dev < kDeviceSlots;
+  if (!slot || a.smem > attr_smem[dev].load(std::memory_order_acquire)) {
+    std::lock_guard<std::mutex> lock(attr_mu);
+    if (!slot || a.smem > attr_smem[dev].load(std::memory_order_acquire)) {
+      FE_CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)a.smem));
+      // the largest shared-memory carve-out, so that the CTAs the grid counts
+      // on (up to three of 4 warps) are resident together
+      FE_CK(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 (int)cudaSharedmemCarveoutMaxShared));
+      if (slot) attr_smem[dev].store(a.smem, std::memory_order_release);
+    }
   }
   kern<<<(unsigned)a.grid, WARPS * 32, a.smem, a.stream>>>(a.d, a.items, a.n_items, a.tab,
                                                           a.rows, a.inst, a.rs, a.sr, a.lf,

@@ -13,10 +13,40 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <atomic>
+#include <mutex>
 #include <string>
 #include <vector>
 
 namespace fe {
+
+// cudaFuncSetAttribute applies to the device that is current when it is
+// called, so a kernel's one-time attribute settings are recorded per device:
+// one bit per device index below kDeviceSlots (higher indices make the
+// setting on every launch).  Two threads may both make the same setting,
+// which is harmless.
+constexpr int kDeviceSlots = 64;
+struct PerDeviceOnce {
+  std::atomic<uint64_t> bits{0};
+  bool needed(int dev) const {
+    return dev < 0 || dev >= kDeviceSlots ||
+           !((bits.load(std::memory_order_acquire) >> dev) & 1u);
+  }
+  void done(int dev) {
+    if (dev >= 0 && dev < kDeviceSlots)
+      bits.fetch_or(uint64_t(1) << dev, std::memory_order_acq_rel);
+  }
+};
+
+// The device current on the calling host thread (0 if it cannot be read).
+inline int current_device() {
+  int d = 0;
+  if (cudaGetDevice(&d) != cudaSuccess) {
+    (void)cudaGetLastError();
+    d = 0;
+  }
+  return d;
+}
 
 constexpr int kMaxFE = 8;          // fixed effects per plan
 constexpr int kWarps = 8;          // warps per CTA in the expand/reduce kernels

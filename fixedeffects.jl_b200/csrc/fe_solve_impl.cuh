@@ -394,16 +394,16 @@ static int rowsum_launch(Ctx& c, const TA* src, TA* out) {
     auto kern = regs ? k_rowsum_reg<TA, C, W, NS> : k_rowsum<TA, C, W, NS>;
     const int RING = regs ? 0 : RowSumStep<TA>::value * RowSumStep<TA>::NBUF;
     const size_t smem = (size_t)kWarps * (RING + c.its->small_rows) * C * sizeof(TA);
-    // per instantiation: the opt-in shared-memory limit (set once) and the
-    // resident CTAs per SM for the last shared-memory size seen
-    static bool attr_set[2] = {false, false};
+    // per instantiation: the opt-in shared-memory limit (set once per
+    // device) and the resident CTAs per SM for the last shared-memory size seen
+    static PerDeviceOnce attr_set[2];
     static size_t occ_smem[2] = {(size_t)-1, (size_t)-1};
     static int occ[2] = {1, 1};
     const int vi = regs ? 1 : 0;
-    if (!attr_set[vi]) {
+    if (attr_set[vi].needed(c.pl->device)) {
       FE_CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)(kWarps * (RING + kSmallRows) * C * sizeof(TA))));
-      attr_set[vi] = true;
+      attr_set[vi].done(c.pl->device);
     }
     if (occ_smem[vi] != smem) {
       int o = 0;
@@ -474,13 +474,13 @@ static int demean_launch(Ctx& c, const T* in, T* rows, float* rows32, T* out,
   if constexpr (C == 32) {
     auto kern = k_demean<T, C, W, NS, NG>;
     const size_t smem = (size_t)kWarps * (kDemeanRows + c.its->small_rows) * C * sizeof(T);
-    static bool attr_set = false;  // per instantiation
+    static PerDeviceOnce attr_set;  // per instantiation
     static size_t occ_smem = (size_t)-1;
     static int occ = 1;
-    if (!attr_set) {
+    if (attr_set.needed(c.pl->device)) {
       FE_CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)(kWarps * (kDemeanRows + kSmallRows) * C * sizeof(T))));
-      attr_set = true;
+      attr_set.done(c.pl->device);
     }
     if (occ_smem != smem) {
       int o = 0;
@@ -610,14 +610,14 @@ static int exdm_launch(Ctx& c, Tab tab, T* rows, const double* B = nullptr,
     auto kern = k_expand_demean<T, C, U, KB, RESID, W, NS, Tab, true>;
     const size_t smem =
         (size_t)kWarps * ((2 * kDemeanRows + c.its->small_rows) * C * sizeof(T) + 32 * sizeof(int));
-    static bool attr_set = false;  // per instantiation
+    static PerDeviceOnce attr_set;  // per instantiation
     static size_t occ_smem = (size_t)-1;
     static int occ = 1;
-    if (!attr_set) {
+    if (attr_set.needed(c.pl->device)) {
       FE_CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)(kWarps * ((2 * kDemeanRows + kSmallRows) * C * sizeof(T) +
                                                  32 * sizeof(int)))));
-      attr_set = true;
+      attr_set.done(c.pl->device);
     }
     if (occ_smem != smem) {
       int o = 0;
@@ -869,11 +869,11 @@ static int launch_segsum_async(Ctx& c, Load ld, TA* out, const ReduceItem* items
   constexpr int UE = VF ? (U > 1 ? U / 2 : 1) : U;
   using L = AsyncSegLayout<TA, C, UE, S, VF>;
   const int smem = kWarps * L::kWarpBytes;
-  static bool attr_set = false;  // per instantiation (set once per process)
-  if (!attr_set) {
+  static PerDeviceOnce attr_set;  // per instantiation (set once per device)
+  if (attr_set.needed(c.pl->device)) {
     FE_CK(cudaFuncSetAttribute(k_segsum_async<TA, C, UE, S, Load, VF>,
                                cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    attr_set = true;
+    attr_set.done(c.pl->device);
   }
   k_segsum_async<TA, C, UE, S, Load, VF><<<grid, kThreads, smem, c.s>>>(c.d, items, n, ld, out,
                                                                          c.seg_split());

@@ -268,6 +268,24 @@ def test_every_entry_point_restores_the_callers_device():
         assert "DeviceRestore" in body.split("\n", 2)[1], (name, fname)
 
 
+def test_kernel_attributes_are_set_per_device():
+    """cudaFuncSetAttribute applies to the current device only, so every
+    setting of a kernel attribute sits behind a per-device record (a plan on a
+    second GPU of the same process must set it again), never a process-wide
+    flag."""
+    csrc = Path(__file__).resolve().parent.parent / "fixedeffects.jl_b200" / "csrc"
+    sites = 0
+    for f in sorted(list(csrc.glob("*.cu")) + list(csrc.glob("*.cuh"))):
+        lines = re.sub(r"//[^\n]*", "", f.read_text()).splitlines()
+        assert not any(re.search(r"static bool attr_set", ln) for ln in lines), f.name
+        for i, ln in enumerate(lines):
+            if "cudaFuncSetAttribute(" in ln:
+                sites += 1
+                window = "\n".join(lines[max(0, i - 12):i])
+                assert ("needed(" in window) or ("attr_smem[dev]" in window), (f.name, i + 1)
+    assert sites >= 6
+
+
 def test_noalloc_entry_point_calls_no_allocator():
     """fe_plan_scales_noalloc's translation unit never allocates device memory
     (no cudaMalloc / cudaFree / plan buffer growth)."""
