@@ -727,12 +727,10 @@ static int exdm_choose(const Ctx& c, ExdmChoice* ch) {
   *ch = ExdmChoice{};
   const fe_plan* pl = c.pl;
   if (pl->opt_exdm_pipe == 0) return 0;
-  static int smem_max = -1;  // opt-in shared memory per block of the device
-  if (smem_max < 0) {
-    int v = 0;
-    FE_CK(cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, pl->device));
-    smem_max = v;
-  }
+  // opt-in shared memory per block of the plan's device (a host query, read
+  // per call so that every device of the process answers for itself)
+  int smem_max = 0;
+  FE_CK(cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, pl->device));
   for (int k = 0; k < pl->K; ++k) {
     const bool small = ((c.its->small_mask >> k) & 1u) != 0;
     if (pl->weighted || pl->interacted[k]) ch->w = true;
@@ -819,14 +817,10 @@ static int try_exdm_pipe(Ctx& c, const float* tab, float* rows, int* launched) {
   // to three of 4 warps); the norm slots are the expand's, so the grid must
   // not exceed their count
   a.smem = exdm_pipe_smem(nl, nsr, kc.stages, kc.per_group, kc.warps, kc.vsm);
-  static int smem_sm = -1, smem_res = 0;  // shared memory per SM, reserved per CTA
-  if (smem_sm < 0) {
-    int v = 0, r = 0;
-    FE_CK(cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerMultiprocessor, c.pl->device));
-    FE_CK(cudaDeviceGetAttribute(&r, cudaDevAttrReservedSharedMemoryPerBlock, c.pl->device));
-    smem_sm = v;
-    smem_res = r;
-  }
+  // shared memory per SM and reserved per CTA on the plan's device
+  int smem_sm = 0, smem_res = 0;
+  FE_CK(cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, c.pl->device));
+  FE_CK(cudaDeviceGetAttribute(&smem_res, cudaDevAttrReservedSharedMemoryPerBlock, c.pl->device));
   const size_t per_cta = a.smem + (size_t)smem_res;  // no static shared memory
   const int per_sm = std::max(1, std::min(kc.warps < kWarps ? 3 : 1, (int)(smem_sm / per_cta)));
   a.grid = std::max<int64_t>(1, std::min<int64_t>(c.its->Se, (int64_t)per_sm * c.its->sms));
