@@ -95,6 +95,24 @@ def test_lsmr_matches_scipy(oracle, seed):
     assert np.max(np.abs(fit_o - A_fit)) < 1e-9
 
 
+def test_same_refs_twice_one_interacted_matches_scipy(oracle, synth):
+    """The reference benchmark's interacted problem (benchmark/run.jl:26-27):
+    the worker FE and the same worker ids interacted with a variable, a
+    slow-converging, ill-conditioned pair.  At a tight tolerance the oracle's
+    residual is scipy's projection, and it is orthogonal to every column."""
+    p = synth.hard_800k_interacted(scale=0.005)
+    y = p.Y[:, 0].astype(np.float64)
+    A, _ = _sparse_A(p.refs, p.nlev, p.interaction, None, oracle)
+    x, istop = spl.lsmr(A, y, atol=1e-13, btol=1e-13, conlim=1e12, maxiter=100000)[:2]
+    R, _, cv = oracle.solve_residuals_cols(np.asfortranarray(y[:, None]), p.refs, p.nlev,
+                                           p.interaction, None, tol=1e-13, maxiter=100000,
+                                           nthreads=4)
+    assert istop in (1, 2) and bool(cv[0])
+    r_s = y - A @ x
+    assert np.linalg.norm(R[:, 0] - r_s) <= 1e-8 * np.linalg.norm(r_s)
+    assert np.abs(A.T @ R[:, 0]).max() <= 1e-10 * np.linalg.norm(y)
+
+
 def test_scale_zero_guard(oracle):
     # issue #97 of the reference: a level whose interaction is all zero gets scale 0
     refs = np.array([1, 1, 2, 2, 3])
