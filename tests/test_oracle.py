@@ -95,12 +95,14 @@ def test_lsmr_matches_scipy(oracle, seed):
     assert np.max(np.abs(fit_o - A_fit)) < 1e-9
 
 
-def test_same_refs_twice_one_interacted_matches_scipy(oracle, synth):
-    """The reference benchmark's interacted problem (benchmark/run.jl:26-27):
-    the worker FE and the same worker ids interacted with a variable, a
-    slow-converging, ill-conditioned pair.  At a tight tolerance the oracle's
-    residual is scipy's projection, and it is orthogonal to every column."""
-    p = synth.hard_800k_interacted(scale=0.005)
+@pytest.mark.parametrize("problem", ["hard_800k", "hard_800k_interacted"])
+def test_reference_benchmark_problems_match_scipy(oracle, synth, problem):
+    """The reference benchmark's worker-firm problems (benchmark/run.jl:17-27)
+    at 1/200 of their size: workers linked to nearby firms, and the worker FE
+    next to the same worker ids interacted with a variable (a slow-converging,
+    ill-conditioned pair).  At a tight tolerance the oracle's residual is
+    scipy's projection, and it is orthogonal to every column."""
+    p = getattr(synth, problem)(scale=0.005)
     y = p.Y[:, 0].astype(np.float64)
     A, _ = _sparse_A(p.refs, p.nlev, p.interaction, None, oracle)
     x, istop = spl.lsmr(A, y, atol=1e-13, btol=1e-13, conlim=1e12, maxiter=100000)[:2]
